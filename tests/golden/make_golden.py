@@ -1,0 +1,413 @@
+"""Generate the golden vectors under tests/golden/ from the reference itself.
+
+Run in a container that has the reference checkout:
+
+    python tests/golden/make_golden.py /path/to/roxy-dcc
+
+The reference's Python is imported with the import-only stand-ins in
+`_refshim/` (taichi, pygame, moderngl).  Its `@ti.func` bodies then run as
+plain float32 Python, so every golden number below is produced by the
+reference's own source:
+
+  bvh_build.npz   GPUBVHBuilder.build              (rendering/taichi/bvh_builder.py:315-544)
+  traversal.npz   bvh_intersect / bvh_occluded     (rendering/taichi/intersect.py:81-219)
+  prims.npz       Sphere/Plane/Cube/Triangle.taichi_intersect (scene/primitives.py:90-215,
+                  scene/mesh.py:133-157)
+  trace_scene.npz extract_scene output, scene_intersect and trace() with a scripted
+                  random stream                    (rendering/taichi/extractor.py,
+                                                    intersect.py:249-309, trace.py:139-236)
+  denoise.npz     edge_aware_denoise               (rendering/denoise.py:23-104)
+  sampling.npz    pixel_sample_offset              (rendering/sampling.py:17-23)
+
+Nothing at test time reads the reference; the tests read these fixtures.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _setup(ref_root):
+    sys.path.insert(0, os.path.join(HERE, "_refshim"))
+    sys.path.insert(1, ref_root)
+    sys.path.insert(2, HERE)
+    sys.setrecursionlimit(100000)
+
+
+def _ns():
+    import core
+    import scene
+    from scene.materials import Emissive, Glossy
+
+    class NS:
+        pass
+
+    ns = NS()
+    for name in ("Vec3", "Color"):
+        setattr(ns, name, getattr(core, name))
+    for name in ("World", "Camera", "SceneObject", "Sphere", "Plane", "Cube", "Mesh", "Triangle",
+                 "IndexedMesh", "Diffuse", "Metal", "Dielectric", "Shape"):
+        setattr(ns, name, getattr(scene, name))
+    ns.Emissive = Emissive
+    ns.Glossy = Glossy
+    return ns
+
+
+def _tri_dict(x):
+    return {'v0': [x, 0, 0], 'v1': [x + 1, 0, 0], 'v2': [x, 1, 0],
+            'n0': [0, 0, 1], 'n1': [0, 0, 1], 'n2': [0, 0, 1],
+            'mat_type': 0, 'albedo': [1, 1, 1], 'roughness': 0.0, 'ior': 1.0, 'emission': 0.0}
+
+
+def _nodes_arrays(builder):
+    nodes = builder.nodes
+    n = len(nodes)
+    out = {
+        "node_min": np.array([nd['aabb_min'] for nd in nodes], dtype=np.float32).reshape(n, 3),
+        "node_max": np.array([nd['aabb_max'] for nd in nodes], dtype=np.float32).reshape(n, 3),
+        "left": np.array([nd['left'] for nd in nodes], dtype=np.int32),
+        "right": np.array([nd['right'] for nd in nodes], dtype=np.int32),
+        "start": np.array([nd['tri_start'] for nd in nodes], dtype=np.int32),
+        "count": np.array([nd['tri_count'] for nd in nodes], dtype=np.int32),
+        "order": np.asarray(builder.ordered_tris, dtype=np.int32),
+    }
+    return out
+
+
+def make_bvh(out_dir):
+    from rendering.taichi.bvh_builder import GPUBVHBuilder, TriangleBatch
+    import golden_scenes as gs
+
+    cases = {}
+
+    def add(name, v0, v1, v2, leaf):
+        n = len(v0)
+        batch = TriangleBatch(v0, v1, v2,
+                              np.tile([0, 0, 1], (n, 1)), np.tile([0, 0, 1], (n, 1)), np.tile([0, 0, 1], (n, 1)),
+                              np.zeros(n, np.int32), np.ones((n, 3), np.float32), np.zeros(n, np.float32),
+                              np.ones(n, np.float32), np.zeros(n, np.float32))
+        b = GPUBVHBuilder()
+        b.MAX_LEAF_SIZE = leaf
+        b.build([batch])
+        arr = _nodes_arrays(b)
+        cases[name] = dict(v0=np.asarray(v0, np.float32), v1=np.asarray(v1, np.float32),
+                           v2=np.asarray(v2, np.float32), leaf=np.int32(leaf), **arr)
+
+    for name, xs, leaf in (("legacy_perm_leaf1", [7, 1, 6, 0, 5, 2, 4, 3], 1),
+                           ("legacy_range_leaf4", list(range(8)), 4),
+                           ("legacy_two_leaf8", [0, 2], 8)):
+        d = [_tri_dict(x) for x in xs]
+        add(name, [t['v0'] for t in d], [t['v1'] for t in d], [t['v2'] for t in d], leaf)
+    for n, leaf, seed in ((1, 8, 1), (2, 8, 2), (9, 8, 3), (100, 8, 4), (1000, 8, 5), (5000, 8, 6),
+                          (3000, 4, 7), (777, 1, 8), (4096, 2, 9)):
+        v0, v1, v2 = gs.soup_triangles(n, seed)
+        add(f"soup{n}_leaf{leaf}", v0, v1, v2, leaf)
+    pos, f = gs.icosphere(3)
+    add("ico3_leaf8", pos[f[:, 0]].astype(np.float32), pos[f[:, 1]].astype(np.float32),
+        pos[f[:, 2]].astype(np.float32), 8)
+    # flat in z: zero centroid extent on one axis
+    v0, v1, v2 = gs.soup_triangles(300, 10)
+    for v in (v0, v1, v2):
+        v[:, 2] = 0.25
+    add("flat300_leaf8", v0, v1, v2, 8)
+    # duplicated triangles: equal Morton codes, order decided by the stable sort
+    v0, v1, v2 = gs.soup_triangles(40, 11)
+    add("dup200_leaf3", np.repeat(v0, 5, 0), np.repeat(v1, 5, 0), np.repeat(v2, 5, 0), 3)
+
+    flat = {}
+    for name, d in cases.items():
+        for k, v in d.items():
+            flat[f"{name}/{k}"] = v
+    flat["case_names"] = np.array(sorted(cases))
+    np.savez_compressed(os.path.join(out_dir, "bvh_build.npz"), **flat)
+
+    # palette / material dedupe behaviour (bvh_builder.py:370-410)
+    batch = TriangleBatch.from_dicts([_tri_dict(0), dict(_tri_dict(2), albedo=[0.5, 0.5, 0.5]),
+                                      dict(_tri_dict(4), mat_type=1, roughness=0.25), _tri_dict(6)])
+    b = GPUBVHBuilder().build([batch])
+    np.savez_compressed(os.path.join(out_dir, "bvh_palette.npz"),
+                        ordered_mat_idx=b._ordered_mat_idx.astype(np.int32),
+                        palette_type=np.array([m['type'] for m in b.mat_palette], np.int32),
+                        palette_albedo=np.array([m['albedo'] for m in b.mat_palette], np.float32),
+                        palette_roughness=np.array([m['roughness'] for m in b.mat_palette], np.float32))
+    print("bvh_build.npz:", len(cases), "cases")
+
+
+def _load_reference_bvh(batch, leaf):
+    from rendering.taichi.bvh_builder import GPUBVHBuilder
+    b = GPUBVHBuilder()
+    b.MAX_LEAF_SIZE = leaf
+    b.build([batch])
+    b.upload()
+    return b
+
+
+def make_traversal(out_dir):
+    import taichi as ti
+    from rendering.taichi.bvh_builder import TriangleBatch
+    import rendering.taichi.intersect as isect
+    import rendering.taichi.fields as fields
+    import golden_scenes as gs
+
+    out = {}
+    for case, (v0, v1, v2), leaf, (ro, rd) in (
+        ("soup2000", gs.soup_triangles(2000, 21), 8, gs.random_rays(400, 22)),
+        ("ico3", tuple(np.asarray(x, np.float32) for x in _ico_tris(3)), 4, gs.random_rays(300, 23, spread=2.0)),
+    ):
+        n = len(v0)
+        batch = TriangleBatch(v0, v1, v2, np.tile([0, 0, 1], (n, 1)), np.tile([0, 0, 1], (n, 1)),
+                              np.tile([0, 0, 1], (n, 1)), np.zeros(n, np.int32), np.ones((n, 3)),
+                              np.zeros(n), np.ones(n), np.zeros(n))
+        b = _load_reference_bvh(batch, leaf)
+        fields._bvh_n_tris[None] = b.triangle_count
+        ts, ids, us, vs, occ = [], [], [], [], []
+        rng = np.random.default_rng(99)
+        max_t = rng.uniform(0.05, 3.0, size=len(ro)).astype(np.float32)
+        for i in range(len(ro)):
+            t, idx, u, v = isect.bvh_intersect(ti.Vector(ro[i]), ti.Vector(rd[i]))
+            ts.append(np.float32(t)); ids.append(int(idx)); us.append(np.float32(u)); vs.append(np.float32(v))
+            occ.append(int(isect.bvh_occluded(ti.Vector(ro[i]), ti.Vector(rd[i]), max_t[i])))
+        arr = _nodes_arrays(b)
+        out.update({f"{case}/v0": v0, f"{case}/v1": v1, f"{case}/v2": v2, f"{case}/leaf": np.int32(leaf),
+                    f"{case}/ro": ro, f"{case}/rd": rd, f"{case}/max_t": max_t,
+                    f"{case}/t": np.array(ts, np.float32), f"{case}/idx": np.array(ids, np.int32),
+                    f"{case}/u": np.array(us, np.float32), f"{case}/v": np.array(vs, np.float32),
+                    f"{case}/occluded": np.array(occ, np.int32)})
+        out.update({f"{case}/{k}": v for k, v in arr.items()})
+        print(f"traversal {case}: {len(ro)} rays, hits={int(np.sum(np.array(ids) >= 0))}")
+    out["case_names"] = np.array(["soup2000", "ico3"])
+    np.savez_compressed(os.path.join(out_dir, "traversal.npz"), **out)
+
+
+def _ico_tris(subdiv):
+    import golden_scenes as gs
+    pos, f = gs.icosphere(subdiv)
+    pos = pos * 0.9
+    return pos[f[:, 0]], pos[f[:, 1]], pos[f[:, 2]]
+
+
+def make_prims(out_dir):
+    import taichi as ti
+    from scene.primitives import Sphere, Plane, Cube
+    from scene.mesh import Triangle
+    import golden_scenes as gs
+
+    ro, rd = gs.random_rays(300, 31, spread=1.2)
+    rng = np.random.default_rng(32)
+    cen = rng.uniform(-0.5, 0.5, size=(300, 3)).astype(np.float32)
+    rad = rng.uniform(0.1, 0.9, size=300).astype(np.float32)
+    nrm = rng.normal(size=(300, 3))
+    nrm = (nrm / np.linalg.norm(nrm, axis=1, keepdims=True)).astype(np.float32)
+    off = rng.uniform(-1, 1, size=300).astype(np.float32)
+    he = rng.uniform(0.1, 0.6, size=(300, 3)).astype(np.float32)
+    v0, v1, v2 = gs.soup_triangles(300, 33)
+    v1 = (v0 + (v1 - v0) * 8).astype(np.float32)
+    v2 = (v0 + (v2 - v0) * 8).astype(np.float32)
+    ts = {"sphere": [], "plane": [], "cube": [], "tri": [], "cube_normal": []}
+    for i in range(300):
+        o, d = ti.Vector(ro[i]), ti.Vector(rd[i])
+        ts["sphere"].append(np.float32(Sphere.taichi_intersect(o, d, ti.Vector(cen[i]), rad[i])))
+        ts["plane"].append(np.float32(Plane.taichi_intersect(o, d, ti.Vector(nrm[i]), off[i])))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tc = Cube.taichi_intersect(o, d, ti.Vector(cen[i]), ti.Vector(he[i]))
+        ts["cube"].append(np.float32(tc))
+        hp = o + d * np.float32(tc if tc > 0 else 1.0)
+        ts["cube_normal"].append(Cube.taichi_normal(hp, ti.Vector(cen[i]), ti.Vector(he[i])).to_list())
+        ts["tri"].append(np.float32(Triangle.taichi_intersect(o, d, ti.Vector(v0[i]), ti.Vector(v1[i]), ti.Vector(v2[i]))))
+    np.savez_compressed(os.path.join(out_dir, "prims.npz"), ro=ro, rd=rd, center=cen, radius=rad, normal=nrm,
+                        offset=off, half=he, v0=v0, v1=v1, v2=v2,
+                        **{f"t_{k}": np.array(v, np.float32) for k, v in ts.items()})
+    print("prims.npz written")
+
+
+def _dump_field(fld, n, width=None, dtype=np.float32):
+    out = np.zeros((n, width) if width else (n,), dtype=dtype)
+    for i in range(n):
+        v = fld[i]
+        out[i] = v.e if hasattr(v, "e") else v
+    return out
+
+
+def make_trace_scene(out_dir):
+    import taichi as ti
+    import rendering.taichi.fields as F
+    import rendering.taichi.trace  # noqa: F401 (the package re-exports a function of the same name)
+    trace_mod = sys.modules["rendering.taichi.trace"]
+    import rendering.taichi.intersect as isect
+    from rendering.taichi.extractor import extract_scene
+    import golden_scenes as gs
+
+    world = gs.build_trace_scene(_ns())
+    stats = extract_scene(world)
+    n_obj = int(F._n_objects[None])
+    n_nodes = int(F._bvh_n_nodes[None])
+    n_tris = int(F._bvh_n_tris[None])
+    n_mats = int(F._mat_n_mats[None])
+    n_lights = int(F._n_lights[None])
+    out = {
+        "stats": np.array([stats['primitive_count'], stats['bvh_nodes'], stats['bvh_triangles'],
+                           stats['bvh_materials'], stats['bvh_leaf_size']], np.int32),
+        "obj_type": _dump_field(F._obj_type, n_obj, dtype=np.int32),
+        "obj_center": _dump_field(F._obj_center, n_obj, 3),
+        "obj_radius": _dump_field(F._obj_radius, n_obj),
+        "obj_normal": _dump_field(F._obj_normal, n_obj, 3),
+        "obj_offset": _dump_field(F._obj_offset, n_obj),
+        "obj_extra": _dump_field(F._obj_extra, n_obj, 3),
+        "obj_v0": _dump_field(F._obj_v0, n_obj, 3),
+        "obj_v1": _dump_field(F._obj_v1, n_obj, 3),
+        "obj_v2": _dump_field(F._obj_v2, n_obj, 3),
+        "obj_mat_type": _dump_field(F._obj_mat_type, n_obj, dtype=np.int32),
+        "obj_albedo": _dump_field(F._obj_albedo, n_obj, 3),
+        "obj_roughness": _dump_field(F._obj_roughness, n_obj),
+        "obj_ior": _dump_field(F._obj_ior, n_obj),
+        "obj_emission": _dump_field(F._obj_emission, n_obj),
+        "light_center": _dump_field(F._light_center, n_lights, 3),
+        "light_radius": _dump_field(F._light_radius, n_lights),
+        "light_albedo": _dump_field(F._light_albedo, n_lights, 3),
+        "light_emission": _dump_field(F._light_emission, n_lights),
+        "node_min": _dump_field(F._bvh_aabb_min, n_nodes, 3),
+        "node_max": _dump_field(F._bvh_aabb_max, n_nodes, 3),
+        "left": _dump_field(F._bvh_left, n_nodes, dtype=np.int32),
+        "right": _dump_field(F._bvh_right, n_nodes, dtype=np.int32),
+        "start": _dump_field(F._bvh_tri_start, n_nodes, dtype=np.int32),
+        "count": _dump_field(F._bvh_tri_count, n_nodes, dtype=np.int32),
+        "v0": _dump_field(F._bvh_v0, n_tris, 3), "v1": _dump_field(F._bvh_v1, n_tris, 3),
+        "v2": _dump_field(F._bvh_v2, n_tris, 3),
+        "n0": _dump_field(F._bvh_n0, n_tris, 3), "n1": _dump_field(F._bvh_n1, n_tris, 3),
+        "n2": _dump_field(F._bvh_n2, n_tris, 3),
+        "tri_mat": _dump_field(F._bvh_mat_idx, n_tris, dtype=np.int32),
+        "mat_type": _dump_field(F._mat_type, n_mats, dtype=np.int32),
+        "mat_albedo": _dump_field(F._mat_albedo, n_mats, 3),
+        "mat_roughness": _dump_field(F._mat_roughness, n_mats),
+        "mat_ior": _dump_field(F._mat_ior, n_mats),
+        "mat_emission": _dump_field(F._mat_emission, n_mats),
+    }
+    # scene_intersect on camera-like rays
+    ro, rd = gs.trace_rays(300, seed=41)
+    si = {"t": [], "idx": [], "is_bvh": [], "u": [], "v": [], "normal": []}
+    for i in range(len(ro)):
+        t, nrm, idx, is_bvh, _mat, u, v = isect.scene_intersect(ti.Vector(ro[i]), ti.Vector(rd[i]))
+        si["t"].append(np.float32(t)); si["idx"].append(int(idx)); si["is_bvh"].append(int(is_bvh))
+        si["u"].append(np.float32(u)); si["v"].append(np.float32(v)); si["normal"].append(nrm.to_list())
+    out.update({"si_ro": ro, "si_rd": rd})
+    out.update({f"si_{k}": np.array(v, np.float32 if k in ("t", "u", "v", "normal") else np.int32)
+                for k, v in si.items()})
+
+    # trace() with scripted random streams
+    counter = ti.CounterField()
+    trace_mod._ray_count = counter
+    tro, trd = gs.trace_rays(96, seed=42)
+    rng = np.random.default_rng(43)
+    configs = [
+        # (max_depth, use_sky, direct_light_mode, direct_light_max_depth)
+        (6, 0, 0, 1), (6, 0, 1, 3), (8, 1, 0, 8), (1, 0, 0, 0),
+    ]
+    recs = {k: [] for k in ("color", "normal", "albedo", "depth", "consumed", "rays", "cfg")}
+    streams = []
+    bg = ti.Vector([0.05, 0.05, 0.08])
+    for ci, (md, sky, mode, dlmd) in enumerate(configs):
+        for i in range(len(tro)):
+            stream = rng.random(512).astype(np.float32)
+            ti.set_random_stream(stream)
+            counter.value = 0
+            color, nrm, alb, dep = trace_mod.trace(ti.Vector(tro[i]), ti.Vector(trd[i]), md, sky, bg,
+                                                   mode, dlmd, 1)
+            recs["color"].append(color.to_list()); recs["normal"].append(nrm.to_list())
+            recs["albedo"].append(alb.to_list()); recs["depth"].append(float(dep))
+            recs["consumed"].append(ti.consumed()); recs["rays"].append(counter.value)
+            recs["cfg"].append(ci)
+            streams.append(stream)
+    out.update({"tr_ro": np.tile(tro, (len(configs), 1)), "tr_rd": np.tile(trd, (len(configs), 1)),
+                "tr_stream": np.array(streams, np.float32),
+                "tr_configs": np.array(configs, np.int32),
+                "tr_bg": np.array([0.05, 0.05, 0.08], np.float32)})
+    for k, v in recs.items():
+        out[f"tr_{k}"] = np.array(v, np.float32 if k in ("color", "normal", "albedo", "depth") else np.int32)
+    np.savez_compressed(os.path.join(out_dir, "trace_scene.npz"), **out)
+
+    # IndexedMesh flattening (scene/mesh.py:397-430 via extractor.py:174-191)
+    obj = gs.build_indexed_object(_ns())
+    geo = obj.shapes[0].geometry
+    arrs = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+    np.savez_compressed(os.path.join(out_dir, "indexed_arrays.npz"),
+                        **{k: np.asarray(v) for k, v in arrs.items() if k != "groups"},
+                        world_matrix=np.array(obj.world_matrix.rows, np.float64),
+                        world_inverse=np.array(obj.world_inverse_matrix.rows, np.float64))
+    print(f"trace_scene.npz: objects={n_obj} nodes={n_nodes} tris={n_tris} mats={n_mats} lights={n_lights}")
+
+
+def make_denoise(out_dir):
+    from rendering.denoise import edge_aware_denoise, linear_to_display
+    rng = np.random.default_rng(51)
+    out = {}
+    cases = [
+        ("small_color_only", (5, 5), 1, 0.2, 0.8, None),
+        ("legacy_none", (4, 5), 1, 0.25, 0.6, None),
+        ("r1_all_guides", (37, 53), 1, 0.08, 0.8, ("normal", "albedo", "depth")),
+        ("r2_all_guides", (40, 31), 2, 0.3, 1.0, ("normal", "albedo", "depth")),
+        ("r1_normal_only", (33, 33), 1, 0.5, 0.7, ("normal",)),
+        ("r3_albedo_depth", (29, 45), 3, 0.15, 0.9, ("albedo", "depth")),
+        ("r1_hdr", (64, 48), 1, 0.08, 0.8, ("normal", "albedo", "depth")),
+    ]
+    names = []
+    for name, (h, w), r, sc, amt, guides in cases:
+        px = rng.random((h, w, 3), dtype=np.float32)
+        if name == "r1_hdr":
+            px = (px * 12.0).astype(np.float32)
+        kw = {}
+        if guides:
+            if "normal" in guides:
+                nrm = rng.normal(size=(h, w, 3)).astype(np.float32)
+                nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
+                nrm[: h // 2] = [0, 1, 0]
+                kw["normal"] = nrm.astype(np.float32)
+            if "albedo" in guides:
+                alb = rng.random((h, w, 3), dtype=np.float32)
+                alb[:, : w // 3] = 0.5
+                kw["albedo"] = alb
+            if "depth" in guides:
+                kw["depth"] = (rng.random((h, w), dtype=np.float32) * 4.0 + 1.0).astype(np.float32)
+        res = edge_aware_denoise(px, radius=r, sigma_color=sc, amount=amt, **kw)
+        out[f"{name}/pixels"] = px
+        for k, v in kw.items():
+            out[f"{name}/{k}"] = v
+        out[f"{name}/params"] = np.array([r, sc, amt], np.float64)
+        out[f"{name}/out"] = np.asarray(res, np.float32)
+        names.append(name)
+    lin = rng.normal(0.5, 0.6, size=(16, 16, 3)).astype(np.float32)
+    out["display/in"] = lin
+    out["display/out"] = linear_to_display(lin)
+    out["case_names"] = np.array(names)
+    np.savez_compressed(os.path.join(out_dir, "denoise.npz"), **out)
+    print("denoise.npz:", len(names), "cases")
+
+
+def make_sampling(out_dir):
+    from rendering.sampling import pixel_sample_offset
+    vals = np.zeros((16, 16, 8, 2), np.float64)
+    for y in range(16):
+        for x in range(16):
+            for f in range(8):
+                vals[y, x, f] = pixel_sample_offset(x, y, f)
+    np.savez_compressed(os.path.join(out_dir, "sampling.npz"), offsets=vals)
+    print("sampling.npz written")
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ROXY_REFERENCE")
+    if not ref_root or not os.path.isdir(ref_root):
+        raise SystemExit("usage: make_golden.py <reference checkout>")
+    _setup(ref_root)
+    np.seterr(all="ignore")
+    make_bvh(HERE)
+    make_denoise(HERE)
+    make_sampling(HERE)
+    make_prims(HERE)
+    make_traversal(HERE)
+    make_trace_scene(HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+/*
+ * roxy.h — C ABI of libroxy_cuda.so, the B200 (sm_100a) path-tracing hot path.
+ *
+ * Plain C: opaque handles, host pointers and sizes, int status codes.  Every
+ * call returns RX_OK (0) or an RX_ERR_* code; rx_last_error() gives the text.
+ * Host arrays passed in are copied before the call returns; the library never
+ * keeps a host pointer.  Calls on one context are serialised by its mutex.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the roxy-dcc project root).
+ */
+#ifndef ROXY_H
+#define ROXY_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  RX_OK = 0,
+  RX_ERR_ARG = 1,       /* invalid argument (the reference raises ValueError) */
+  RX_ERR_CAPACITY = 2,  /* size beyond a limit (the reference asserts)        */
+  RX_ERR_CUDA = 3,      /* CUDA runtime error                                 */
+  RX_ERR_STATE = 4,     /* call out of order (e.g. render before a BVH)       */
+  RX_ERR_DEVICE = 5     /* a kernel reported an internal error flag           */
+};
+
+enum { RX_BVH_REFERENCE = 0, RX_BVH_LBVH_SAH = 1 };
+
+enum {
+  RX_ACC_RADIANCE = 0, /* running-mean linear radiance (H,W,3)  */
+  RX_ACC_NORMAL = 1,   /* first-hit normal running mean (H,W,3) */
+  RX_ACC_ALBEDO = 2,   /* first-hit albedo running mean (H,W,3) */
+  RX_ACC_DEPTH = 3,    /* first-hit depth running mean (H,W)    */
+  RX_ACC_DISPLAY = 4   /* sqrt(min(radiance, 1)) (H,W,3)        */
+};
+
+typedef struct rx_ctx rx_ctx;
+typedef struct rx_scene rx_scene;
+typedef struct rx_accum rx_accum;
+
+/* Arguments of one render call: the reference's render_kernel parameters
+ * (rendering/taichi/trace.py:239-254) plus the sampling options. */
+typedef struct {
+  int width, height;
+  float fov_tan, aspect;
+  float cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];
+  int max_depth;               /* bounce loop length (trace.py:149)            */
+  int use_sky;                 /* sky gradient, else bg (trace.py:154-159)     */
+  float bg[3];
+  int direct_light_mode;       /* 0 one light, 1 all lights (trace.py:60-93)   */
+  int direct_light_max_depth;  /* NEE at depth < this (trace.py:199,210)       */
+  float sample_clamp;          /* clamp each sample to [0, c] if c > 0          */
+  int reference_compat;        /* 1: sphere-light NEE only, emission counted
+                                  again on BSDF hits, as trace.py does          */
+  uint32_t seed;               /* counter-based RNG key                         */
+  int wave_paths;              /* paths per wavefront (0 = automatic)           */
+} rx_render_params;
+
+/* Edge-aware filter (rendering/denoise.py:23-104) and its a-trous extension:
+ * pass i filters the previous pass with taps spaced 2^i apart; passes = 1 is
+ * exactly edge_aware_denoise. */
+typedef struct {
+  int radius;
+  int passes;
+  float sigma_color, sigma_normal, sigma_albedo, sigma_depth;
+  float amount;
+  int use_normal, use_albedo, use_depth; /* guides used by rx_accum_denoise */
+  int to_display;                        /* apply linear_to_display (denoise.py:107) */
+} rx_denoise_params;
+
+int rx_version(void);
+int rx_device_count(int* out);
+
+/* Context: device, stream, error text.  Replaces ti.init
+ * (rendering/taichi/__init__.py:4-5). */
+int rx_ctx_create(int device, rx_ctx** out);
+int rx_ctx_destroy(rx_ctx* ctx);
+const char* rx_last_error(const rx_ctx* ctx);
+int rx_ctx_sync(rx_ctx* ctx);
+void* rx_ctx_stream(rx_ctx* ctx); /* the cudaStream_t the library launches on */
+
+/* Scene state.  Replaces the module-global fields written by extract_scene
+ * and GPUBVHBuilder.upload (rendering/taichi/fields.py:22-79,
+ * rendering/taichi/extractor.py:19-50, rendering/taichi/bvh_builder.py:560-655). */
+int rx_scene_create(rx_ctx* ctx, rx_scene** out);
+int rx_scene_destroy(rx_scene* scene);
+/* Triangles in caller order, float32 xyz triples, palette index per triangle
+ * (TriangleBatch, bvh_builder.py:8-272). */
+int rx_scene_set_triangles(rx_scene* scene, int n, const float* v0, const float* v1, const float* v2,
+                           const float* n0, const float* n1, const float* n2, const int* mat_idx);
+/* Material palette (fields.py:73-78). */
+int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float* albedo,
+                           const float* roughness, const float* ior, const float* emission);
+/* Primitive slots (extractor.py:19-33 _write_slot): type 0 sphere, 1 plane,
+ * 2 cube, 4 triangle, each with its own material. */
+int rx_scene_set_objects(rx_scene* scene, int n, const int* type, const float* center, const float* radius,
+                         const float* normal, const float* offset, const float* extra, const float* v0,
+                         const float* v1, const float* v2, const int* mat_type, const float* albedo,
+                         const float* roughness, const float* ior, const float* emission);
+/* Explicit lights (extractor.py:36-50 plus emissive triangles): kind 0 sphere
+ * (p0 centre, p1[0] radius), kind 1 triangle (p0, p1, p2); alias table over
+ * pick_pdf for the one-light mode. */
+int rx_scene_set_lights(rx_scene* scene, int n, const int* kind, const float* p0, const float* p1,
+                        const float* p2, const float* albedo, const float* emission, const float* area,
+                        const float* pick_pdf, const float* alias_prob, const int* alias_idx);
+
+/* BVH build on the device.  RX_BVH_REFERENCE reproduces GPUBVHBuilder.build's
+ * Morton method (bvh_builder.py:315-478) node for node; RX_BVH_LBVH_SAH builds
+ * a Karras LBVH with SAH leaf collapse (core/bvh.py's role for the GPU path),
+ * optionally with the sphere slots as BVH primitives. */
+int rx_bvh_build(rx_scene* scene, int method, int max_leaf, int spheres_in_bvh);
+/* Upload a tree already in the reference's node format (GPUBVHBuilder.upload,
+ * bvh_builder.py:560-655); triangles must be set first, `order` maps leaf
+ * order to caller order. */
+int rx_bvh_set_reference(rx_scene* scene, int n_nodes, const float* node_min, const float* node_max,
+                         const int* left, const int* right, const int* tri_start, const int* tri_count,
+                         const int* order);
+/* Node count, primitive count, method, leaf size, depth (levels). */
+int rx_bvh_info(rx_scene* scene, int* n_nodes, int* n_prims, int* method, int* leaf_size, int* depth);
+/* Reference-format export (GPUBVHBuilder.nodes / ordered_tris) of a tree built
+ * with RX_BVH_REFERENCE or uploaded; arrays sized n_nodes (order: n_tris). */
+int rx_bvh_export_reference(rx_scene* scene, float* node_min, float* node_max, int* left, int* right,
+                            int* tri_start, int* tri_count, int* order);
+
+/* Traversal-layout export for structural checks: n_nodes x 16 floats (the
+ * 64-byte node records) and the leaf-order -> caller-order primitive map
+ * (triangles < n_tris, spheres after them). */
+int rx_bvh_export_layout(rx_scene* scene, float* nodes, int* order);
+
+/* Closest hit over the BVH for n rays (bvh_intersect, intersect.py:81-152):
+ * t (1e9 on miss), id = caller triangle index (-1 miss; spheres in the BVH
+ * report -(slot + 2)), barycentrics u, v.  Host pointers. */
+int rx_trace_closest(rx_scene* scene, long n, const float* ro, const float* rd, float* t, int* id, float* u,
+                     float* v);
+/* Any hit before tmax (bvh_occluded / scene_occluded, intersect.py:155-246). */
+int rx_trace_any(rx_scene* scene, long n, const float* ro, const float* rd, const float* tmax, int* occluded);
+/* Full scene query (scene_intersect, intersect.py:249-309): kind 0 miss,
+ * 1 BVH triangle, 2 sphere in the BVH, 3 object slot; id = triangle index or
+ * slot; normal is the un-flipped surface normal. */
+int rx_scene_intersect(rx_scene* scene, long n, const float* ro, const float* rd, float* t, int* kind, int* id,
+                       float* u, float* v, float* normal);
+/* Device-pointer variants for callers that keep rays resident in HBM. */
+int rx_trace_closest_device(rx_scene* scene, long n, const float* d_ro, const float* d_rd, float* d_t, int* d_id,
+                            float* d_u, float* d_v);
+
+/* Progressive accumulation buffers and the wavefront render.  Replaces
+ * render_kernel and the TaichiRenderer frame loop (trace.py:239-283,
+ * rendering/taichi_renderer.py:87-161). */
+int rx_accum_create(rx_ctx* ctx, int width, int height, rx_accum** out);
+int rx_accum_destroy(rx_accum* acc);
+int rx_accum_reset(rx_accum* acc);
+int rx_render(rx_scene* scene, rx_accum* acc, const rx_render_params* params, int frames);
+int rx_accum_read(rx_accum* acc, int which, float* host_out);
+/* frames accumulated and rays cast so far (rays counted as trace.py:150-151
+ * and :78-79 count them: one per bounce including the primary, one per
+ * shadow ray) */
+int rx_accum_info(rx_accum* acc, int* width, int* height, int* frames, long long* rays);
+/* Denoise the resident accumulators (taichi_renderer.py:67-79) into host_out (H,W,3). */
+int rx_accum_denoise(rx_accum* acc, const rx_denoise_params* params, float* host_out);
+/* Per-kernel CUDA-event timing of the next render calls (for profiling). */
+int rx_accum_set_timing(rx_accum* acc, int on);
+/* ms of the last render, ms per kernel class (extend, shade, connect, other)
+ * and the number of kernel launches it made. */
+int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
+
+/* edge_aware_denoise / a-trous on caller host buffers (denoise.py:23-104):
+ * color (H,W,3); normal, albedo (H,W,3) and depth (H,W) may be NULL. */
+int rx_denoise(rx_ctx* ctx, int height, int width, const float* color, const float* normal, const float* albedo,
+               const float* depth, const rx_denoise_params* params, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROXY_H */

@@ -711,7 +711,7 @@ inline PathOut trace(const orc_scene& s, const orc_params& p, Rng& rng, V3 ro, V
         V3 d = p.reference_compat ? direct_light_compat(s, p, rng, b, hit_p, n, alb, cnt)
                                   : direct_light_full(s, p, rng, b, hit_p, n, alb, cnt);
         color = color + thr * d;
-        nee_here = true;
+        nee_here = s.n_lights > 0;
       }
       float r1 = rng.get(b, SLOT_BSDF_U1);
       float r2 = rng.get(b, SLOT_BSDF_U2);
@@ -728,7 +728,7 @@ inline PathOut trace(const orc_scene& s, const orc_params& p, Rng& rng, V3 ro, V
         V3 d = p.reference_compat ? direct_light_compat(s, p, rng, b, hit_p, n, alb, cnt)
                                   : direct_light_full(s, p, rng, b, hit_p, n, alb, cnt);
         color = color + (thr * d) * rough;
-        did = true;
+        did = s.n_lights > 0;
       }
       float lobe = rng.get(b, SLOT_LOBE);
       if (lobe < rough) {

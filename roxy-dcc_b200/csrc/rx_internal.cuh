@@ -1,0 +1,511 @@
+// Internal device-side definitions shared by the roxy CUDA translation units.
+//
+// The library is compiled with -fmad=false: every float expression rounds
+// like a sequence of IEEE single operations, which is what lets the hit
+// distances and barycentrics match the float32 restatement of the
+// reference's Moller-Trumbore bit for bit.  Where a fused multiply-add is
+// wanted (slab tests on padded boxes, where rounding cannot change a
+// result) it is written explicitly with __fmaf_rn.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "../../include/roxy.h"
+
+namespace rx {
+
+__host__ __device__ __forceinline__ float int_bits_as_float(int i) {
+  float f;
+  memcpy(&f, &i, sizeof(f));
+  return f;
+}
+
+// ---------------------------------------------------------------- float3 ops
+__host__ __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__host__ __device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+__host__ __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+__host__ __device__ __forceinline__ float3 operator*(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__host__ __device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__host__ __device__ __forceinline__ float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+// left-to-right sum of products, as the reference's vector dot
+__host__ __device__ __forceinline__ float dot(float3 a, float3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__host__ __device__ __forceinline__ float3 cross(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+// v * (1 / |v|), the reference's normalized()
+__device__ __forceinline__ float3 normalized(float3 a) {
+  float inv = 1.0f / sqrtf(dot(a, a));
+  return inv * a;
+}
+__host__ __device__ __forceinline__ float3 vmin(float3 a, float3 b) { return f3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+__host__ __device__ __forceinline__ float3 vmax(float3 a, float3 b) { return f3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+__host__ __device__ __forceinline__ float maxc(float3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+
+// ------------------------------------------------------------------- layout
+// BVH node (64 B, four float4): both children's boxes live in the parent, so
+// one coalesced 64-byte fetch decides which children to visit.
+//   n[0] = (L.min.x, L.max.x, L.min.y, L.max.y)
+//   n[1] = (L.min.z, L.max.z, R.min.x, R.max.x)
+//   n[2] = (R.min.y, R.max.y, R.min.z, R.max.z)
+//   n[3] = (left word, right word, left count, right count) as int bits
+// child word >= 0: internal node index; < 0: leaf, first primitive = ~word,
+// primitive count in the matching count slot (0 = empty leaf).
+struct Node4 {
+  float4 a, b, c, d;
+};
+
+// Primitives in leaf order, three float4 each (48 B):
+//   triangle: a = (v0, kind = 0), b = (v1 - v0, 0), c = (v2 - v0, 0)
+//   sphere:   a = (centre, kind = 1), b = (radius, 0, 0, 0), c = 0
+enum PrimKind { PRIM_TRI = 0, PRIM_SPHERE = 1 };
+
+// Shading record per primitive in leaf order (three float4):
+//   s0 = (n0, material index bits), s1 = (n1, source id bits), s2 = (n2, 0)
+// source id: triangle index in the caller's order, or the object slot for
+// spheres.
+
+// Linear primitive slot, scanned before the BVH exactly like the reference's
+// _obj_* fields (rendering/taichi/intersect.py:259-287).
+struct ObjSlot {
+  int type;        // 0 sphere, 1 plane, 2 cube, 4 triangle
+  int mat;         // palette index
+  float radius, offset;
+  float3 center, normal, extra, v0, v1, v2;
+};  // 88 B
+
+// Explicit light (emissive sphere or emissive triangle).
+struct Light {
+  int kind;        // 0 sphere, 1 triangle
+  float area;
+  float pick_pdf;
+  float emission;  // intensity; radiance = albedo * intensity
+  float3 p0, p1, p2;
+  float3 albedo;
+};
+
+struct DevScene {
+  const float4* nodes;     // n_nodes * 4
+  int n_nodes;
+  float3 root_min, root_max;
+  const float4* prims;     // n_prims * 3
+  const float4* shade;     // n_prims * 3
+  int n_prims;
+  const float4* mat_a;     // (albedo, type bits)
+  const float4* mat_b;     // (roughness, ior, emission, texture)
+  int n_mats;
+  const ObjSlot* objs;
+  int n_objs;
+  const Light* lights;
+  const float* alias_prob;
+  const int* alias_idx;
+  int n_lights;
+  int exact_slab;          // 1: slab test with the reference's operation order
+};
+
+// --------------------------------------------------------------------- RNG
+// Philox4x32-10 (Salmon et al., SC'11): counter = (pixel, sample, bounce,
+// block), key = (seed, constant).  Identical to the oracle's generator.
+__host__ __device__ __forceinline__ void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+    uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+    uint32_t n0 = hi1 ^ c1 ^ k0;
+    uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+__host__ __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+constexpr uint32_t kKeyHi = 0x5EEDC0DEu;
+
+enum {
+  SLOT_LIGHT_PICK = 0, SLOT_LIGHT_ACCEPT = 1, SLOT_LIGHT_U1 = 2, SLOT_LIGHT_U2 = 3,
+  SLOT_BSDF_U1 = 4, SLOT_BSDF_U2 = 5, SLOT_LOBE = 6, SLOT_RR = 7,
+  SLOT_FUZZ_U1 = 8, SLOT_FUZZ_U2 = 9,
+  SLOT_ALL_LIGHTS = 16
+};
+
+// device error bits (set by kernels, read by the host after a launch)
+enum {
+  ERR_STACK_OVERFLOW = 1,
+  ERR_QUEUE_OVERFLOW = 2,
+  ERR_SHADOW_OVERFLOW = 4,
+  ERR_BAD_NODE = 8
+};
+
+constexpr int kStack = 64;
+
+// ------------------------------------------------------------ intersection
+// rendering/taichi/intersect.py:17-25
+__device__ __forceinline__ float3 make_inv_dir(float3 d) {
+  return f3(fabsf(d.x) > 1e-10f ? 1.0f / d.x : 1e30f, fabsf(d.y) > 1e-10f ? 1.0f / d.y : 1e30f,
+            fabsf(d.z) > 1e-10f ? 1.0f / d.z : 1e30f);
+}
+
+// Moller-Trumbore with the reference's operation order and thresholds
+// (rendering/taichi/intersect.py:57-78).  v0 and the two edges are stored
+// precomputed; e = v - v0 rounds exactly as the reference computes it.
+__device__ __forceinline__ bool tri_hit(float3 o, float3 d, float4 a, float4 b, float4 c, float tmax, float& t,
+                                        float& u, float& v) {
+  float3 e1 = xyz(b), e2 = xyz(c);
+  float3 h = cross(d, e2);
+  float det = dot(e1, h);
+  if (!(fabsf(det) > 1e-8f)) return false;
+  float f = 1.0f / det;
+  float3 s = o - xyz(a);
+  float uu = f * dot(s, h);
+  if (!(uu >= 0.0f && uu <= 1.0f)) return false;
+  float3 q = cross(s, e1);
+  float vv = f * dot(d, q);
+  if (!(vv >= 0.0f && uu + vv <= 1.0f)) return false;
+  float tt = f * dot(e2, q);
+  if (!(tt > 0.001f && tt < tmax)) return false;
+  t = tt;
+  u = uu;
+  v = vv;
+  return true;
+}
+
+// scene/primitives.py:90-105 (assumes a unit direction)
+__device__ __forceinline__ float sphere_t(float3 o, float3 d, float3 c, float r) {
+  float3 oc = o - c;
+  float h = dot(d, oc);
+  float cc = dot(oc, oc) - r * r;
+  float disc = h * h - cc;
+  float t = -1.0f;
+  if (disc >= 0.0f) {
+    float sq = sqrtf(disc);
+    t = -h - sq;
+    if (t < 0.001f) t = -h + sq;
+    if (t < 0.001f) t = -1.0f;
+  }
+  return t;
+}
+
+// scene/primitives.py:145-154
+__device__ __forceinline__ float plane_t(float3 o, float3 d, float3 n, float off) {
+  float denom = dot(n, d);
+  float t = -1.0f;
+  if (fabsf(denom) >= 1e-6f) {
+    float tc = -(dot(n, o) + off) / denom;
+    if (tc >= 0.001f) t = tc;
+  }
+  return t;
+}
+
+// scene/primitives.py:187-201
+__device__ __forceinline__ float cube_t(float3 o, float3 d, float3 c, float3 he) {
+  float3 bmin = c - he, bmax = c + he;
+  float3 t0 = f3((bmin.x - o.x) / d.x, (bmin.y - o.y) / d.y, (bmin.z - o.z) / d.z);
+  float3 t1 = f3((bmax.x - o.x) / d.x, (bmax.y - o.y) / d.y, (bmax.z - o.z) / d.z);
+  float3 lo = vmin(t0, t1), hi = vmax(t0, t1);
+  float te = fmaxf(lo.x, fmaxf(lo.y, lo.z));
+  float tx = fminf(hi.x, fminf(hi.y, hi.z));
+  float t = -1.0f;
+  if (tx >= te && tx >= 0.001f) t = te >= 0.001f ? te : tx;
+  return t;
+}
+
+// scene/primitives.py:203-215
+__device__ __forceinline__ float3 cube_normal(float3 p, float3 c, float3 he) {
+  float3 dd = p - c;
+  dd = f3(dd.x / he.x, dd.y / he.y, dd.z / he.z);
+  float ax = fabsf(dd.x), ay = fabsf(dd.y), az = fabsf(dd.z);
+  if (ax >= ay && ax >= az) return f3(dd.x > 0.0f ? 1.0f : -1.0f, 0.0f, 0.0f);
+  if (ay >= az) return f3(0.0f, dd.y > 0.0f ? 1.0f : -1.0f, 0.0f);
+  return f3(0.0f, 0.0f, dd.z > 0.0f ? 1.0f : -1.0f);
+}
+
+// Linear scan of the object slots (intersect.py:259-287): closest t and slot.
+__device__ __forceinline__ float objs_closest(const DevScene& S, float3 o, float3 d, int& slot) {
+  float best = 1e9f;
+  slot = -1;
+  for (int i = 0; i < S.n_objs; ++i) {
+    const ObjSlot& ob = S.objs[i];
+    float t = -1.0f;
+    if (ob.type == 0) t = sphere_t(o, d, ob.center, ob.radius);
+    else if (ob.type == 1) t = plane_t(o, d, ob.normal, ob.offset);
+    else if (ob.type == 2) t = cube_t(o, d, ob.center, ob.extra);
+    else if (ob.type == 4) {
+      float uu, vv, tt;
+      float4 a = make_float4(ob.v0.x, ob.v0.y, ob.v0.z, 0.0f);
+      float4 b = make_float4(ob.v1.x - ob.v0.x, ob.v1.y - ob.v0.y, ob.v1.z - ob.v0.z, 0.0f);
+      float4 c = make_float4(ob.v2.x - ob.v0.x, ob.v2.y - ob.v0.y, ob.v2.z - ob.v0.z, 0.0f);
+      if (tri_hit(o, d, a, b, c, 3.0e38f, tt, uu, vv)) t = tt;
+    }
+    if (t > 0.001f && t < best) {
+      best = t;
+      slot = i;
+    }
+  }
+  return best;
+}
+
+__device__ __forceinline__ bool objs_any(const DevScene& S, float3 o, float3 d, float max_t) {
+  for (int i = 0; i < S.n_objs; ++i) {
+    const ObjSlot& ob = S.objs[i];
+    float t = -1.0f;
+    if (ob.type == 0) t = sphere_t(o, d, ob.center, ob.radius);
+    else if (ob.type == 1) t = plane_t(o, d, ob.normal, ob.offset);
+    else if (ob.type == 2) t = cube_t(o, d, ob.center, ob.extra);
+    else if (ob.type == 4) {
+      float uu, vv, tt;
+      float4 a = make_float4(ob.v0.x, ob.v0.y, ob.v0.z, 0.0f);
+      float4 b = make_float4(ob.v1.x - ob.v0.x, ob.v1.y - ob.v0.y, ob.v1.z - ob.v0.z, 0.0f);
+      float4 c = make_float4(ob.v2.x - ob.v0.x, ob.v2.y - ob.v0.y, ob.v2.z - ob.v0.z, 0.0f);
+      if (tri_hit(o, d, a, b, c, 3.0e38f, tt, uu, vv)) t = tt;
+    }
+    if (0.001f < t && t < max_t) return true;
+  }
+  return false;
+}
+
+// Slab test of both children of a node against [0.001, tmax].
+// exact = reference operation order (intersect.py:28-43); otherwise the
+// FMA form t = b * inv - o * inv, safe because every box is padded by 1e-4.
+template <bool EXACT>
+__device__ __forceinline__ void slab2(const float4 n0, const float4 n1, const float4 n2, float3 o, float3 inv,
+                                      float3 oinv, float tmax, bool& hl, bool& hr, float& tl, float& tr) {
+  float lx0, lx1, ly0, ly1, lz0, lz1, rx0, rx1, ry0, ry1, rz0, rz1;
+  if (EXACT) {
+    lx0 = (n0.x - o.x) * inv.x; lx1 = (n0.y - o.x) * inv.x;
+    ly0 = (n0.z - o.y) * inv.y; ly1 = (n0.w - o.y) * inv.y;
+    lz0 = (n1.x - o.z) * inv.z; lz1 = (n1.y - o.z) * inv.z;
+    rx0 = (n1.z - o.x) * inv.x; rx1 = (n1.w - o.x) * inv.x;
+    ry0 = (n2.x - o.y) * inv.y; ry1 = (n2.y - o.y) * inv.y;
+    rz0 = (n2.z - o.z) * inv.z; rz1 = (n2.w - o.z) * inv.z;
+  } else {
+    lx0 = __fmaf_rn(n0.x, inv.x, -oinv.x); lx1 = __fmaf_rn(n0.y, inv.x, -oinv.x);
+    ly0 = __fmaf_rn(n0.z, inv.y, -oinv.y); ly1 = __fmaf_rn(n0.w, inv.y, -oinv.y);
+    lz0 = __fmaf_rn(n1.x, inv.z, -oinv.z); lz1 = __fmaf_rn(n1.y, inv.z, -oinv.z);
+    rx0 = __fmaf_rn(n1.z, inv.x, -oinv.x); rx1 = __fmaf_rn(n1.w, inv.x, -oinv.x);
+    ry0 = __fmaf_rn(n2.x, inv.y, -oinv.y); ry1 = __fmaf_rn(n2.y, inv.y, -oinv.y);
+    rz0 = __fmaf_rn(n2.z, inv.z, -oinv.z); rz1 = __fmaf_rn(n2.w, inv.z, -oinv.z);
+  }
+  float lte = fmaxf(fminf(lx0, lx1), fmaxf(fminf(ly0, ly1), fminf(lz0, lz1)));
+  float ltx = fminf(fmaxf(lx0, lx1), fminf(fmaxf(ly0, ly1), fmaxf(lz0, lz1)));
+  float rte = fmaxf(fminf(rx0, rx1), fmaxf(fminf(ry0, ry1), fminf(rz0, rz1)));
+  float rtx = fminf(fmaxf(rx0, rx1), fminf(fmaxf(ry0, ry1), fmaxf(rz0, rz1)));
+  hl = ltx >= lte && ltx >= 0.001f && lte <= tmax;
+  hr = rtx >= rte && rtx >= 0.001f && rte <= tmax;
+  tl = lte;
+  tr = rte;
+}
+
+__device__ __forceinline__ bool slab1(float3 bmin, float3 bmax, float3 o, float3 inv, float tmax, float& te) {
+  float3 a = (bmin - o) * inv, b = (bmax - o) * inv;
+  float3 lo = vmin(a, b), hi = vmax(a, b);
+  te = fmaxf(lo.x, fmaxf(lo.y, lo.z));
+  float tx = fminf(hi.x, fminf(hi.y, hi.z));
+  return tx >= te && tx >= 0.001f && te <= tmax;
+}
+
+// Closest hit over the BVH with an explicit stack of (child word, count,
+// entry distance).  Visits nodes in the reference's order: nearer child
+// first, ties to the right child (intersect.py:128-150).  tmax in: current
+// best distance (from the linear scan), out: closest hit.  Returns the
+// leaf-order primitive index or -1.
+template <bool EXACT>
+__device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d, float& tmax, float& hu, float& hv,
+                                           int* err) {
+  int stk_w[kStack];
+  int stk_c[kStack];
+  float stk_t[kStack];
+  int sp = 0;
+  float3 inv = make_inv_dir(d);
+  float3 oinv = o * inv;
+  int hit = -1;
+  float te;
+  if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
+  int word = 0, cnt = 0;
+  float wt = te;
+  // a tree visits each record at most once per ray; the guard turns a
+  // malformed tree into an error flag instead of an endless loop
+  int guard = 4 * S.n_nodes + 64;
+  for (;;) {
+    if (--guard < 0) {
+      if (err) atomicOr(err, ERR_BAD_NODE);
+      break;
+    }
+    if (wt <= tmax) {
+      if (word >= S.n_nodes || (word < 0 && (~word + cnt > S.n_prims || cnt < 0))) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        break;
+      }
+      if (word >= 0) {
+        const float4* np = S.nodes + 4 * (size_t)word;
+        float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+        bool hl, hr;
+        float tl, tr;
+        slab2<EXACT>(n0, n1, n2, o, inv, oinv, tmax, hl, hr, tl, tr);
+        int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
+        int lc = __float_as_int(n3.z), rc = __float_as_int(n3.w);
+        if (hl && hr) {
+          bool left_first = tl < tr;
+          int fw = left_first ? rw : lw, fc = left_first ? rc : lc;
+          float ft = left_first ? tr : tl;
+          if (sp < kStack) {
+            stk_w[sp] = fw; stk_c[sp] = fc; stk_t[sp] = ft; ++sp;
+          } else if (err) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+          }
+          word = left_first ? lw : rw;
+          cnt = left_first ? lc : rc;
+          wt = left_first ? tl : tr;
+          continue;
+        } else if (hl) {
+          word = lw; cnt = lc; wt = tl;
+          continue;
+        } else if (hr) {
+          word = rw; cnt = rc; wt = tr;
+          continue;
+        }
+      } else {
+        int first = ~word;
+        for (int k = first; k < first + cnt; ++k) {
+          const float4* pp = S.prims + 3 * (size_t)k;
+          float4 a = __ldg(pp);
+          float t, u, v;
+          if (__float_as_int(a.w) == PRIM_TRI) {
+            float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
+            if (tri_hit(o, d, a, b, c, tmax, t, u, v)) {
+              tmax = t; hu = u; hv = v; hit = k;
+            }
+          } else {
+            float4 b = __ldg(pp + 1);
+            t = sphere_t(o, d, xyz(a), b.x);
+            if (t > 0.001f && t < tmax) {
+              tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
+            }
+          }
+        }
+      }
+    }
+    if (sp == 0) break;
+    --sp;
+    word = stk_w[sp]; cnt = stk_c[sp]; wt = stk_t[sp];
+  }
+  return hit;
+}
+
+// Any hit before max_t (intersect.py:155-219).
+template <bool EXACT>
+__device__ __forceinline__ bool bvh_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
+  int stk_w[kStack];
+  int stk_c[kStack];
+  int sp = 0;
+  float3 inv = make_inv_dir(d);
+  float3 oinv = o * inv;
+  float te;
+  if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, max_t, te)) return false;
+  int word = 0, cnt = 0;
+  int guard = 4 * S.n_nodes + 64;
+  for (;;) {
+    if (--guard < 0) {
+      if (err) atomicOr(err, ERR_BAD_NODE);
+      return false;
+    }
+    if (word >= S.n_nodes || (word < 0 && (~word + cnt > S.n_prims || cnt < 0))) {
+      if (err) atomicOr(err, ERR_BAD_NODE);
+      return false;
+    }
+    if (word >= 0) {
+      const float4* np = S.nodes + 4 * (size_t)word;
+      float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+      bool hl, hr;
+      float tl, tr;
+      slab2<EXACT>(n0, n1, n2, o, inv, oinv, max_t, hl, hr, tl, tr);
+      int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
+      int lc = __float_as_int(n3.z), rc = __float_as_int(n3.w);
+      if (hl && hr) {
+        bool left_first = tl < tr;
+        if (sp < kStack) {
+          stk_w[sp] = left_first ? rw : lw; stk_c[sp] = left_first ? rc : lc; ++sp;
+        } else if (err) {
+          atomicOr(err, ERR_STACK_OVERFLOW);
+        }
+        word = left_first ? lw : rw;
+        cnt = left_first ? lc : rc;
+        continue;
+      } else if (hl) {
+        word = lw; cnt = lc;
+        continue;
+      } else if (hr) {
+        word = rw; cnt = rc;
+        continue;
+      }
+    } else {
+      int first = ~word;
+      for (int k = first; k < first + cnt; ++k) {
+        const float4* pp = S.prims + 3 * (size_t)k;
+        float4 a = __ldg(pp);
+        float t, u, v;
+        if (__float_as_int(a.w) == PRIM_TRI) {
+          float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
+          if (tri_hit(o, d, a, b, c, max_t, t, u, v)) return true;
+        } else {
+          float4 b = __ldg(pp + 1);
+          t = sphere_t(o, d, xyz(a), b.x);
+          if (0.001f < t && t < max_t) return true;
+        }
+      }
+    }
+    if (sp == 0) break;
+    --sp;
+    word = stk_w[sp]; cnt = stk_c[sp];
+  }
+  return false;
+}
+
+// Hit record from the full scene query (intersect.py:249-309): the linear
+// object slots first, then the BVH, which wins only when strictly closer.
+struct SceneHit {
+  float t;
+  int prim;   // leaf-order primitive, or -1
+  int slot;   // object slot, or -1
+  float u, v;
+};
+
+template <bool EXACT>
+__device__ __forceinline__ SceneHit scene_closest(const DevScene& S, float3 o, float3 d, int* err) {
+  SceneHit h;
+  int slot;
+  float t = objs_closest(S, o, d, slot);
+  h.slot = slot;
+  h.prim = -1;
+  h.u = 0.0f;
+  h.v = 0.0f;
+  float u = 0.0f, v = 0.0f;
+  int p = bvh_closest<EXACT>(S, o, d, t, u, v, err);
+  if (p >= 0) {
+    h.prim = p;
+    h.slot = -1;
+    h.u = u;
+    h.v = v;
+  }
+  h.t = t;
+  return h;
+}
+
+template <bool EXACT>
+__device__ __forceinline__ bool scene_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
+  if (objs_any(S, o, d, max_t)) return true;
+  return bvh_any<EXACT>(S, o, d, max_t, err);
+}
+
+}  // namespace rx

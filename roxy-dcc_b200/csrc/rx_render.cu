@@ -1,0 +1,939 @@
+// Wavefront path tracer.
+//
+// The reference runs one megakernel thread per pixel per frame
+// (rendering/taichi/trace.py:239-283) that loops over bounces with five
+// material branches.  Here one wavefront holds `spf` frames x W x H paths
+// whose state lives in structure-of-arrays buffers in HBM; each bounce is
+//
+//   extend  (closest hit for the active queue)        rx_internal.cuh traversal
+//   shade   (materials, emission, NEE sample, scatter, Russian roulette;
+//            warp-aggregated pushes into the next queue and the shadow queue)
+//   connect (any-hit for the shadow queue, adds unoccluded contributions)
+//
+// followed by one accumulate pass that applies the sample clamp and folds
+// the frames into the running means exactly as the reference does.  The
+// per-wave launch sequence is captured once as a CUDA graph and replayed.
+//
+// Random numbers come from Philox4x32-10 keyed by (pixel, sample, bounce,
+// slot), so a path's numbers do not depend on scheduling.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "rx_internal.cuh"
+#include "rx_runtime.h"
+
+namespace rx {
+
+constexpr int kMaxBounce = 64;
+enum { C_Q = 0, C_FE = 64, C_FS = 128, C_S = 192, C_FC = 256, C_N = 320 };
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTwoPi = 6.283185307179586f;
+
+struct RenderK {
+  int W, H;
+  long long P;
+  int spf;
+  float fov_tan, aspect;
+  float3 cam_pos, cam_fwd, cam_right, cam_up;
+  int max_depth, use_sky;
+  float3 bg;
+  int mode, dlmd;
+  float clamp;
+  int compat;
+  uint32_t seed;
+  long long shadow_cap;
+  long long queue_cap;
+};
+
+__device__ __forceinline__ float fractf_(float x) { return x - floorf(x); }
+
+// camera.py:23-30 with a counter-based per-pixel phase in place of the
+// sin-hash: jitter = fract(phase + (frame + 1) * R2).
+__device__ __forceinline__ float3 camera_dir(const RenderK& K, int px, int py, int frame) {
+  uint32_t ph[4];
+  philox((uint32_t)((long long)py * K.W + px), 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, K.seed, kKeyHi, ph);
+  float i = (float)(frame + 1);
+  float jx = fractf_(u01(ph[0]) + i * 0.7548776662466927f);
+  float jy = fractf_(u01(ph[1]) + i * 0.5698402909980532f);
+  float u = ((float)px + jx) / (float)K.W * 2.0f - 1.0f;
+  float v = 1.0f - ((float)py + jy) / (float)K.H * 2.0f;
+  float ndx = u * K.aspect * K.fov_tan;
+  float ndy = v * K.fov_tan;
+  return normalized((K.cam_fwd + K.cam_right * ndx) + K.cam_up * ndy);
+}
+
+struct PathRng {
+  uint32_t pix, smp, bounce, seed;
+  uint32_t blk[3][4];
+  unsigned have;
+  __device__ void init(uint32_t p, uint32_t s, uint32_t b, uint32_t k) {
+    pix = p; smp = s; bounce = b; seed = k; have = 0;
+  }
+  __device__ float get(int slot) {
+    int bi = slot >> 2;
+    if (bi < 3) {
+      if (!(have & (1u << bi))) {
+        philox(pix, smp, bounce, (uint32_t)bi, seed, kKeyHi, blk[bi]);
+        have |= 1u << bi;
+      }
+      return u01(blk[bi][slot & 3]);
+    }
+    uint32_t o[4];
+    philox(pix, smp, bounce, (uint32_t)bi, seed, kKeyHi, o);
+    return u01(o[slot & 3]);
+  }
+};
+
+// ---------------------------------------------------------------- scattering
+// scatter.py:14-38
+__device__ __forceinline__ float3 diffuse_scatter(float3 n, float r1, float r2) {
+  float phi = kTwoPi * r1;
+  float r = sqrtf(r2);
+  float sp, cp;
+  sincosf(phi, &sp, &cp);
+  float lx = cp * r, ly = sp * r;
+  float lz = sqrtf(fmaxf(0.0f, 1.0f - r2));
+  float3 helper = fabsf(n.x) > 0.9f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
+  float3 bt = normalized(cross(n, helper));
+  float3 tg = cross(bt, n);
+  float3 s = normalized((tg * lx + bt * ly) + n * lz);
+  if (dot(s, s) < 1e-8f) s = n;
+  return normalized(s);
+}
+
+// scatter.py:6-11
+__device__ __forceinline__ float3 random_unit_vector(float r1, float r2) {
+  float theta = acosf(1.0f - 2.0f * r1);
+  float phi = kTwoPi * r2;
+  float st = sinf(theta);
+  float sp, cp;
+  sincosf(phi, &sp, &cp);
+  return f3(st * cp, st * sp, cosf(theta));
+}
+
+__device__ __forceinline__ float3 reflect(float3 d, float3 n) { return d - (2.0f * dot(d, n)) * n; }
+
+__device__ __forceinline__ float3 refract(float3 d, float3 n, float eta) {
+  float c = fminf(-dot(d, n), 1.0f);
+  float3 perp = eta * (d + c * n);
+  float3 par = -sqrtf(fabsf(1.0f - dot(perp, perp))) * n;
+  return perp + par;
+}
+
+__device__ __forceinline__ float schlick(float c, float eta) {
+  float r0 = powf((1.0f - eta) / (1.0f + eta), 2.0f);
+  return r0 + (1.0f - r0) * powf(1.0f - c, 5.0f);
+}
+
+// trace.py:23-57 cone sampling of a sphere light.
+__device__ __forceinline__ void sphere_light_sample(float3 hit_p, float3 center, float radius, float ru1, float ru2,
+                                                    float3& ldir, float& t_light, float& sop) {
+  float3 to_c = center - hit_p;
+  float dist2 = fmaxf(dot(to_c, to_c), 1e-6f);
+  float dist = sqrtf(dist2);
+  float3 axis = to_c / dist;
+  float sin2 = fminf(radius * radius / dist2, 1.0f);
+  float cos_max = sqrtf(fmaxf(0.0f, 1.0f - sin2));
+  float cos_t = 1.0f - ru1 * (1.0f - cos_max);
+  float sin_t = sqrtf(fmaxf(0.0f, 1.0f - cos_t * cos_t));
+  float phi = kTwoPi * ru2;
+  float3 helper = fabsf(axis.x) > 0.9f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
+  float3 bt = normalized(cross(axis, helper));
+  float3 tg = cross(bt, axis);
+  float sp, cp;
+  sincosf(phi, &sp, &cp);
+  ldir = normalized((tg * (cp * sin_t) + bt * (sp * sin_t)) + axis * cos_t);
+  float3 oc = hit_p - center;
+  float hb = dot(oc, ldir);
+  float c = dot(oc, oc) - radius * radius;
+  float disc = fmaxf(hb * hb - c, 0.0f);
+  t_light = -hb - sqrtf(disc);
+  sop = 2.0f * (1.0f - cos_max);
+}
+
+// One light sample without visibility: direction, shadow distance and the
+// contribution it adds if unoccluded (albedo * L * geometry * weight).
+__device__ __forceinline__ bool light_sample(const Light& L, float ru1, float ru2, float3 hit_p, float3 n, float3 alb,
+                                             float weight, float3& dir, float& max_t, float3& val) {
+  float3 base = (alb * L.albedo) * L.emission;
+  if (L.kind == 0) {
+    float3 ldir;
+    float tl, sop;
+    sphere_light_sample(hit_p, L.p0, L.p1.x, ru1, ru2, ldir, tl, sop);
+    float ndotl = dot(n, ldir);
+    if (!(ndotl > 0.0f)) return false;
+    max_t = tl * 0.999f;
+    if (!(max_t > 0.001f)) return false;
+    dir = ldir;
+    val = ((base * ndotl) * sop) * weight;
+    return true;
+  }
+  float su = sqrtf(ru1);
+  float b1 = su * (1.0f - ru2);
+  float b2 = su * ru2;
+  float3 e1 = L.p1 - L.p0, e2 = L.p2 - L.p0;
+  float3 y = (L.p0 + e1 * b1) + e2 * b2;
+  float3 to = y - hit_p;
+  float d2 = dot(to, to);
+  float d = sqrtf(d2);
+  float3 wi = to * (1.0f / d);
+  float ndotl = dot(n, wi);
+  if (!(ndotl > 0.0f)) return false;
+  float3 ln = normalized(cross(e1, e2));
+  float cos_l = fabsf(dot(ln, wi));
+  max_t = d * 0.999f;
+  if (!(max_t > 0.001f)) return false;
+  float g = (((ndotl * cos_l) * L.area) / (kPi * d2)) * weight;
+  dir = wi;
+  val = base * g;
+  return true;
+}
+
+// -------------------------------------------------------------------- kernels
+__global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4* __restrict__ ray_o,
+                           float4* __restrict__ ray_d, float4* __restrict__ thr, float4* __restrict__ rad,
+                           float4* __restrict__ gn, float4* __restrict__ ga, int* __restrict__ q0,
+                           int* __restrict__ counters) {
+  long long total = (long long)K.spf * K.P;
+  int fb = *frame_base;
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
+    int f = (int)(t / K.P);
+    long long s = t - (long long)f * K.P;
+    // 4-row strips walked column by column: a warp covers an 8 x 4 tile
+    long long strip = s / (4LL * K.W);
+    long long r = s - strip * 4LL * K.W;
+    int hs = min(4, K.H - (int)(4 * strip));
+    int px = (int)(r / hs);
+    int py = (int)(4 * strip + r % hs);
+    long long pix = (long long)py * K.W + px;
+    long long p = (long long)f * K.P + pix;
+    float3 d = camera_dir(K, px, py, fb + f);
+    ray_o[p] = make_float4(K.cam_pos.x, K.cam_pos.y, K.cam_pos.z, 1.0f);
+    ray_d[p] = make_float4(d.x, d.y, d.z, 0.0f);
+    thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    q0[t] = (int)p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)total;
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(128) k_extend(DevScene S, int b, const int* __restrict__ qin, int* counters,
+                                                const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
+                                                float4* __restrict__ hits, int* err) {
+  const int n = *(volatile int*)&counters[C_Q + b];
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&counters[C_FE + b], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    int i = base + lane;
+    if (i < n) {
+      int p = qin[i];
+      float4 o = ray_o[p], d = ray_d[p];
+      SceneHit h = scene_closest<EXACT>(S, xyz(o), xyz(d), err);
+      int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
+      hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
+    }
+  }
+}
+
+// warp-aggregated append: one atomic per warp, ranks by ballot / popc
+__device__ __forceinline__ int warp_append(bool want, int* counter) {
+  unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return -1;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, const int* __restrict__ qin,
+                                               int* __restrict__ qout, int* counters,
+                                               const int* __restrict__ frame_base, float4* __restrict__ ray_o,
+                                               float4* __restrict__ ray_d, float4* __restrict__ thr_b,
+                                               float4* __restrict__ rad_b, float4* __restrict__ gn,
+                                               float4* __restrict__ ga, const float4* __restrict__ hits,
+                                               float4* __restrict__ shadow, int* err) {
+  const int n = *(volatile int*)&counters[C_Q + b];
+  const int fb = *frame_base;
+  const int lane = threadIdx.x & 31;
+  const bool last_bounce = (b + 1) >= K.max_depth;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&counters[C_FS + b], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    int i = base + lane;
+    bool valid = i < n;
+    bool alive = false;
+    bool do_nee = false;
+    float nee_scale = 1.0f;
+    int p = 0;
+    float3 hit_p = f3(0, 0, 0), nrm = f3(0, 0, 1), alb = f3(0, 0, 0), thr_nee = f3(0, 0, 0);
+    PathRng rng;
+    if (valid) {
+      p = qin[i];
+      float4 h = hits[i];
+      float4 o4 = ray_o[p], d4 = ray_d[p], t4 = thr_b[p];
+      float3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
+      float cur_ior = o4.w;
+      bool prev_nee = d4.w != 0.0f;
+      int code = __float_as_int(h.y);
+      long long pl = p;
+      rng.init((uint32_t)(pl % K.P), (uint32_t)(fb + (int)(pl / K.P)), (uint32_t)b, K.seed);
+      float3 add = f3(0.0f, 0.0f, 0.0f);
+      bool has_add = false;
+      if (code == -1) {
+        // trace.py:154-159
+        float3 sky;
+        if (K.use_sky) {
+          float t = 0.5f * (d.y + 1.0f);
+          sky = f3(1.0f, 1.0f, 1.0f) * (1.0f - t) + f3(0.5f, 0.7f, 1.0f) * t;
+        } else {
+          sky = K.bg;
+        }
+        add = thr * sky;
+        has_add = true;
+      } else {
+        float t = h.x;
+        float3 nn;
+        int m;
+        bool listed;
+        if (code >= 0) {
+          const float4* sp = S.shade + 3 * (size_t)code;
+          float4 pa = __ldg(S.prims + 3 * (size_t)code);
+          float4 s0 = __ldg(sp);
+          m = __float_as_int(s0.w);
+          if (__float_as_int(pa.w) == PRIM_TRI) {
+            float w = 1.0f - h.z - h.w;
+            nn = normalized((xyz(s0) * w + xyz(__ldg(sp + 1)) * h.z) + xyz(__ldg(sp + 2)) * h.w);
+          } else {
+            nn = normalized((o + d * t) - xyz(pa));
+          }
+          listed = true;
+        } else {
+          const ObjSlot& ob = S.objs[-code - 2];
+          m = ob.mat;
+          if (ob.type == 0) nn = normalized((o + d * t) - ob.center);
+          else if (ob.type == 1) nn = ob.normal;
+          else if (ob.type == 2) nn = cube_normal(o + d * t, ob.center, ob.extra);
+          else nn = normalized(cross(ob.v1 - ob.v0, ob.v2 - ob.v0));
+          listed = ob.type == 0;
+        }
+        bool front = dot(nn, d) < 0.0f;
+        if (!front) nn = -nn;
+        hit_p = o + d * t;
+        float4 ma = __ldg(S.mat_a + m), mb = __ldg(S.mat_b + m);
+        int mt = __float_as_int(ma.w);
+        float3 albedo = xyz(ma);
+        float rough = mb.x, ior = mb.y, em = mb.z;
+        listed = listed && mt == 3 && em > 0.0f;
+        if (b == 0) {
+          gn[p] = make_float4(nn.x, nn.y, nn.z, t);
+          ga[p] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
+        }
+        if (mt == 3) {
+          // trace.py:194-196; with NEE on the previous diffuse vertex the
+          // default estimator already counted this emitter
+          if (!( !K.compat && prev_nee && listed)) {
+            add = (thr * albedo) * em;
+            has_add = true;
+          }
+        } else {
+          bool nee_here = false;
+          bool can_nee = b < K.dlmd && S.n_lights > 0;
+          float3 nd = d;
+          if (mt == 0) {
+            if (can_nee) {
+              do_nee = true;
+              nee_here = true;
+            }
+            nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
+          } else if (mt == 1) {
+            float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
+            nd = normalized(reflect(d, nn) + ru * rough);
+          } else if (mt == 4) {
+            if (can_nee) {
+              do_nee = true;
+              nee_scale = rough;
+            }
+            if (rng.get(SLOT_LOBE) < rough) {
+              nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
+              nee_here = do_nee;
+            } else {
+              float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
+              nd = normalized(reflect(d, nn) + ru * rough);
+            }
+          } else if (mt == 2) {
+            float eta;
+            if (front) {
+              eta = cur_ior / ior;
+              cur_ior = ior;
+            } else {
+              eta = cur_ior / 1.0f;
+              cur_ior = 1.0f;
+            }
+            float c = fminf(-dot(d, nn), 1.0f);
+            float s = sqrtf(1.0f - c * c);
+            bool refl = eta * s > 1.0f;
+            if (!refl) refl = schlick(c, eta) > rng.get(SLOT_LOBE);
+            nd = refl ? reflect(d, nn) : refract(d, nn, eta);
+          }
+          thr_nee = thr;
+          thr = thr * albedo;
+          alb = albedo;
+          nrm = nn;
+          alive = true;
+          if (b > 2) {
+            float rr = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+            if (rng.get(SLOT_RR) > rr) alive = false;
+            else thr = thr / rr;
+          }
+          if (last_bounce) alive = false;
+          if (alive) {
+            float3 no = hit_p + nn * 1e-4f;
+            ray_o[p] = make_float4(no.x, no.y, no.z, cur_ior);
+            ray_d[p] = make_float4(nd.x, nd.y, nd.z, nee_here ? 1.0f : 0.0f);
+            thr_b[p] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+          }
+        }
+      }
+      if (has_add) {
+        float4 r = rad_b[p];
+        rad_b[p] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, 0.0f);
+      }
+    }
+    // next-event estimation: shadow records for connect
+    if (K.mode == 0) {
+      bool emit = false;
+      float3 dir = f3(0, 0, 0), val = f3(0, 0, 0);
+      float max_t = 0.0f;
+      if (do_nee) {
+        int li;
+        float w;
+        if (K.compat) {
+          int cnt = S.n_lights;
+          li = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)cnt), cnt - 1);
+          w = (float)cnt;
+        } else {
+          int nl = S.n_lights;
+          int col = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)nl), nl - 1);
+          li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
+          w = 1.0f / S.lights[li].pick_pdf;
+        }
+        emit = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), hit_p, nrm, alb, w, dir,
+                            max_t, val);
+      }
+      int slot = warp_append(emit, &counters[C_S + b]);
+      if (emit) {
+        if (slot < K.shadow_cap) {
+          float3 so = hit_p + nrm * 1e-4f;
+          float3 c = thr_nee * val;
+          if (nee_scale != 1.0f) c = c * nee_scale;
+          float4* sp = shadow + 3 * (size_t)slot;
+          sp[0] = make_float4(so.x, so.y, so.z, max_t);
+          sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
+          sp[2] = make_float4(c.x, c.y, c.z, 0.0f);
+        } else {
+          atomicOr(err, ERR_SHADOW_OVERFLOW);
+        }
+      }
+    } else {
+      for (int li = 0; li < S.n_lights; ++li) {
+        bool emit = false;
+        float3 dir = f3(0, 0, 0), val = f3(0, 0, 0);
+        float max_t = 0.0f;
+        if (do_nee) {
+          int s1 = SLOT_ALL_LIGHTS + 4 * li;
+          emit = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), hit_p, nrm, alb, 1.0f, dir, max_t, val);
+        }
+        int slot = warp_append(emit, &counters[C_S + b]);
+        if (emit) {
+          if (slot < K.shadow_cap) {
+            float3 so = hit_p + nrm * 1e-4f;
+            float3 c = thr_nee * val;
+            if (nee_scale != 1.0f) c = c * nee_scale;
+            float4* sp = shadow + 3 * (size_t)slot;
+            sp[0] = make_float4(so.x, so.y, so.z, max_t);
+            sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
+            sp[2] = make_float4(c.x, c.y, c.z, 0.0f);
+          } else {
+            atomicOr(err, ERR_SHADOW_OVERFLOW);
+          }
+        }
+      }
+    }
+    int q = warp_append(alive, &counters[C_Q + b + 1]);
+    if (alive) {
+      if (q < K.queue_cap) qout[q] = p;
+      else atomicOr(err, ERR_QUEUE_OVERFLOW);
+    }
+  }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(128) k_connect(DevScene S, int b, int* counters, const float4* __restrict__ shadow,
+                                                 float4* __restrict__ rad, long long cap, int* err) {
+  int n = *(volatile int*)&counters[C_S + b];
+  if (n > cap) n = (int)cap;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&counters[C_FC + b], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    int i = base + lane;
+    if (i < n) {
+      const float4* sp = shadow + 3 * (size_t)i;
+      float4 s0 = sp[0], s1 = sp[1];
+      if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
+        float4 s2 = sp[2];
+        int p = __float_as_int(s1.w);
+        float* r = reinterpret_cast<float*>(rad + p);
+        atomicAdd(r, s2.x);
+        atomicAdd(r + 1, s2.y);
+        atomicAdd(r + 2, s2.z);
+      }
+    }
+  }
+}
+
+// trace.py:262-283: clamp, running mean of radiance and first-hit guides,
+// display = sqrt(min(acc, 1)).  Frames of the wave are folded in order.
+__global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, const float4* __restrict__ rad,
+                             const float4* __restrict__ gn, const float4* __restrict__ ga,
+                             float4* __restrict__ acc_r, float4* __restrict__ acc_n, float4* __restrict__ acc_a,
+                             float4* __restrict__ pixels) {
+  int fb = *frame_base;
+  for (long long pix = blockIdx.x * (long long)blockDim.x + threadIdx.x; pix < K.P;
+       pix += (long long)gridDim.x * blockDim.x) {
+    float4 a = acc_r[pix], an = acc_n[pix], aa = acc_a[pix];
+    for (int f = 0; f < K.spf; ++f) {
+      long long p = (long long)f * K.P + pix;
+      float4 s = rad[p];
+      if (K.clamp > 0.0f) {
+        s.x = fminf(fmaxf(s.x, 0.0f), K.clamp);
+        s.y = fminf(fmaxf(s.y, 0.0f), K.clamp);
+        s.z = fminf(fmaxf(s.z, 0.0f), K.clamp);
+      }
+      float4 g = gn[p], al = ga[p];
+      int frame = fb + f;
+      if (frame == 0) {
+        a = make_float4(s.x, s.y, s.z, 0.0f);
+        an = g;
+        aa = make_float4(al.x, al.y, al.z, 0.0f);
+      } else {
+        float F = (float)frame, F1 = (float)(frame + 1);
+        a = make_float4((a.x * F + s.x) / F1, (a.y * F + s.y) / F1, (a.z * F + s.z) / F1, 0.0f);
+        an = make_float4((an.x * F + g.x) / F1, (an.y * F + g.y) / F1, (an.z * F + g.z) / F1,
+                         (an.w * F + g.w) / F1);
+        aa = make_float4((aa.x * F + al.x) / F1, (aa.y * F + al.y) / F1, (aa.z * F + al.z) / F1, 0.0f);
+      }
+    }
+    acc_r[pix] = a;
+    acc_n[pix] = an;
+    acc_a[pix] = aa;
+    pixels[pix] = make_float4(sqrtf(fminf(a.x, 1.0f)), sqrtf(fminf(a.y, 1.0f)), sqrtf(fminf(a.z, 1.0f)), 0.0f);
+  }
+}
+
+__global__ void k_finish(const int* __restrict__ counters, int max_depth, int* __restrict__ frame_base,
+                         unsigned long long* __restrict__ rays, int spf) {
+  unsigned long long r = 0;
+  for (int b = 0; b < max_depth; ++b) r += (unsigned long long)counters[C_Q + b] + (unsigned long long)counters[C_S + b];
+  *rays += r;
+  *frame_base += spf;
+}
+
+__global__ void k_pack(long long P, const float4* __restrict__ src, int comp, float* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P; i += (long long)gridDim.x * blockDim.x) {
+    float4 v = src[i];
+    if (comp == 1) {
+      dst[i] = v.w;
+    } else {
+      dst[3 * i] = v.x;
+      dst[3 * i + 1] = v.y;
+      dst[3 * i + 2] = v.z;
+    }
+  }
+}
+
+// -------------------------------------------------------------------- host
+enum { K_EXTEND = 0, K_SHADE = 1, K_CONNECT = 2, K_OTHER = 3, K_CLASSES = 4 };
+
+struct Accum {
+  Ctx* ctx = nullptr;
+  int W = 0, H = 0;
+  long long P = 0;
+  DevBuf<float4> acc_r, acc_n, acc_a, pixels;
+  DevBuf<int> frame_base;
+  DevBuf<unsigned long long> rays;
+  int frames = 0;
+  // wavefront state
+  long long cap = 0, shadow_cap = 0;
+  DevBuf<float4> ray_o, ray_d, thr, rad, gn, ga, hits, shadow;
+  DevBuf<int> q0, q1, counters;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  bool g_timed = false;
+  Scene* g_scene = nullptr;
+  uint64_t g_ver = 0;
+  rx_render_params g_params;
+  int g_spf = 0;
+  int g_launches = 0;
+  // timing
+  int timing = 0;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ev_class;
+  float last_ms = 0.0f;
+  float last_k[K_CLASSES] = {0, 0, 0, 0};
+  int last_launches = 0;
+  // denoise scratch
+  DevBuf<float4> dn0, dn1, dn_out;
+  int occ_ext = 0, occ_shade = 0, occ_conn = 0;
+
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+  }
+  ~Accum() {
+    drop_graph();
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+Accum* accum_new(Ctx* ctx, int w, int h) {
+  Accum* a = new Accum();
+  a->ctx = ctx;
+  a->W = w;
+  a->H = h;
+  a->P = (long long)w * h;
+  bool ok = a->acc_r.alloc(ctx, a->P) && a->acc_n.alloc(ctx, a->P) && a->acc_a.alloc(ctx, a->P) &&
+            a->pixels.alloc(ctx, a->P) && a->frame_base.alloc(ctx, 1) && a->rays.alloc(ctx, 1) &&
+            a->counters.alloc(ctx, C_N);
+  if (!ok) {
+    delete a;
+    return nullptr;
+  }
+  accum_reset(a);
+  return a;
+}
+
+void accum_delete(Accum* a) { delete a; }
+
+int accum_reset(Accum* a) {
+  Ctx* ctx = a->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaMemsetAsync(a->acc_r.p, 0, a->acc_r.bytes(), st);
+  cudaMemsetAsync(a->acc_n.p, 0, a->acc_n.bytes(), st);
+  cudaMemsetAsync(a->acc_a.p, 0, a->acc_a.bytes(), st);
+  cudaMemsetAsync(a->pixels.p, 0, a->pixels.bytes(), st);
+  cudaMemsetAsync(a->frame_base.p, 0, sizeof(int), st);
+  cudaMemsetAsync(a->rays.p, 0, sizeof(unsigned long long), st);
+  a->frames = 0;
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return RX_OK;
+}
+
+static RenderK make_k(const rx_render_params* p, const Accum* a, int spf, long long shadow_cap) {
+  RenderK K;
+  K.W = p->width;
+  K.H = p->height;
+  K.P = (long long)p->width * p->height;
+  K.spf = spf;
+  K.fov_tan = p->fov_tan;
+  K.aspect = p->aspect;
+  K.cam_pos = f3(p->cam_pos[0], p->cam_pos[1], p->cam_pos[2]);
+  K.cam_fwd = f3(p->cam_fwd[0], p->cam_fwd[1], p->cam_fwd[2]);
+  K.cam_right = f3(p->cam_right[0], p->cam_right[1], p->cam_right[2]);
+  K.cam_up = f3(p->cam_up[0], p->cam_up[1], p->cam_up[2]);
+  K.max_depth = p->max_depth;
+  K.use_sky = p->use_sky;
+  K.bg = f3(p->bg[0], p->bg[1], p->bg[2]);
+  K.mode = p->direct_light_mode;
+  K.dlmd = p->direct_light_max_depth;
+  K.clamp = p->sample_clamp;
+  K.compat = p->reference_compat;
+  K.seed = p->seed;
+  K.shadow_cap = shadow_cap;
+  K.queue_cap = a->cap;
+  return K;
+}
+
+static int blocks_for(Ctx* ctx, const void* fn, int block) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * ctx->num_sms;
+}
+
+// Records the launch sequence of one wave on the context stream.  With
+// `timed`, an event is recorded after every kernel (class in ev_class).
+static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int* n_launch) {
+  Ctx* ctx = a->ctx;
+  cudaStream_t st = ctx->stream;
+  DevScene S = sc->view();
+  int launches = 0;
+  int ev_i = 0;
+  auto mark = [&](int cls) {
+    if (timed) {
+      cudaEventRecord(a->ev[ev_i], st);
+      a->ev_class[ev_i] = cls;
+      ++ev_i;
+    }
+  };
+  mark(K_OTHER);
+  cudaMemsetAsync(a->counters.p, 0, sizeof(int) * C_N, st);
+  long long total = (long long)K.spf * K.P;
+  int gblocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
+  k_generate<<<std::max(gblocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p,
+                                                    a->gn.p, a->ga.p, a->q0.p, a->counters.p);
+  ++launches;
+  mark(K_OTHER);
+  for (int b = 0; b < K.max_depth; ++b) {
+    const int* qin = (b & 1) ? a->q1.p : a->q0.p;
+    int* qout = (b & 1) ? a->q0.p : a->q1.p;
+    if (S.exact_slab)
+      k_extend<true><<<a->occ_ext, 128, 0, st>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p,
+                                                 ctx->d_err);
+    else
+      k_extend<false><<<a->occ_ext, 128, 0, st>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p,
+                                                  ctx->d_err);
+    ++launches;
+    mark(K_EXTEND);
+    k_shade<<<a->occ_shade, 128, 0, st>>>(S, K, b, qin, qout, a->counters.p, a->frame_base.p, a->ray_o.p,
+                                           a->ray_d.p, a->thr.p, a->rad.p, a->gn.p, a->ga.p, a->hits.p,
+                                           a->shadow.p, ctx->d_err);
+    ++launches;
+    mark(K_SHADE);
+    if (b < K.dlmd && S.n_lights > 0) {
+      if (S.exact_slab)
+        k_connect<true><<<a->occ_conn, 128, 0, st>>>(S, b, a->counters.p, a->shadow.p, a->rad.p, K.shadow_cap,
+                                                     ctx->d_err);
+      else
+        k_connect<false><<<a->occ_conn, 128, 0, st>>>(S, b, a->counters.p, a->shadow.p, a->rad.p, K.shadow_cap,
+                                                      ctx->d_err);
+      ++launches;
+      mark(K_CONNECT);
+    }
+  }
+  int ablocks = (int)std::min<long long>((K.P + 255) / 256, (long long)ctx->num_sms * 16);
+  k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->rad.p, a->gn.p, a->ga.p, a->acc_r.p,
+                                                      a->acc_n.p, a->acc_a.p, a->pixels.p);
+  k_finish<<<1, 1, 0, st>>>(a->counters.p, K.max_depth, a->frame_base.p, a->rays.p, K.spf);
+  launches += 2;
+  mark(K_OTHER);
+  *n_launch = launches;
+}
+
+static int ensure_wave_buffers(Accum* a, long long cap, long long shadow_cap) {
+  Ctx* ctx = a->ctx;
+  if (cap > a->cap) {
+    a->drop_graph();
+    bool ok = a->ray_o.alloc(ctx, cap) && a->ray_d.alloc(ctx, cap) && a->thr.alloc(ctx, cap) &&
+              a->rad.alloc(ctx, cap) && a->gn.alloc(ctx, cap) && a->ga.alloc(ctx, cap) &&
+              a->hits.alloc(ctx, cap) && a->q0.alloc(ctx, cap) && a->q1.alloc(ctx, cap);
+    if (!ok) {
+      a->cap = 0;
+      set_error(ctx, "out of device memory for %lld wavefront paths", cap);
+      return RX_ERR_CAPACITY;
+    }
+    a->cap = cap;
+  }
+  if (shadow_cap > a->shadow_cap) {
+    a->drop_graph();
+    if (!a->shadow.alloc(ctx, (size_t)3 * shadow_cap)) {
+      a->shadow_cap = 0;
+      set_error(ctx, "out of device memory for %lld shadow rays", shadow_cap);
+      return RX_ERR_CAPACITY;
+    }
+    a->shadow_cap = shadow_cap;
+  }
+  if (!a->occ_ext) {
+    a->occ_ext = blocks_for(ctx, (const void*)k_extend<false>, 128);
+    a->occ_shade = blocks_for(ctx, (const void*)k_shade, 128);
+    a->occ_conn = blocks_for(ctx, (const void*)k_connect<false>, 128);
+  }
+  return RX_OK;
+}
+
+static int check_device_error(Ctx* ctx) {
+  int e = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (e) {
+    cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+    set_error(ctx, "device error flags 0x%x (stack/queue/shadow overflow)", e);
+    return RX_ERR_DEVICE;
+  }
+  return RX_OK;
+}
+
+int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
+  Ctx* ctx = a->ctx;
+  if (!p || frames < 0) return set_error(ctx, "render: bad arguments"), RX_ERR_ARG;
+  if (p->width != a->W || p->height != a->H)
+    return set_error(ctx, "render: %dx%d does not match the accumulator %dx%d", p->width, p->height, a->W, a->H),
+           RX_ERR_ARG;
+  if (p->max_depth < 0 || p->max_depth > kMaxBounce - 1)
+    return set_error(ctx, "render: max_depth must be in [0, %d]", kMaxBounce - 1), RX_ERR_ARG;
+  if (p->direct_light_mode != 0 && p->direct_light_mode != 1)
+    return set_error(ctx, "direct_light_mode must be 'one' or 'all'"), RX_ERR_ARG;
+  if (sc->n_tris > 0 && sc->n_nodes == 0) return set_error(ctx, "render: scene has triangles but no BVH"), RX_ERR_STATE;
+  if (frames == 0) return RX_OK;
+  int rc = sc->upload_palette(ctx);
+  if (rc) return rc;
+  long long target = p->wave_paths > 0 ? p->wave_paths : (1LL << 22);
+  int spf = (int)std::max<long long>(1, std::min<long long>(frames, target / std::max<long long>(a->P, 1)));
+  long long cap = (long long)spf * a->P;
+  if (cap >= (1LL << 31)) return set_error(ctx, "render: wavefront of %lld paths is too large", cap), RX_ERR_CAPACITY;
+  int nl = sc->n_lights;
+  long long shadow_cap = cap * (p->direct_light_mode == 1 ? std::max(nl, 1) : 1);
+  rc = ensure_wave_buffers(a, cap, shadow_cap);
+  if (rc) return rc;
+  if (p->max_depth == 0) {
+    // no bounce: every sample is black (the reference's loop never runs)
+  }
+  bool timed = a->timing != 0;
+  int max_events = 4 + 3 * std::max(p->max_depth, 1) + 4;
+  if (timed && (int)a->ev.size() < max_events) {
+    for (int i = (int)a->ev.size(); i < max_events; ++i) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      a->ev.push_back(e);
+    }
+    a->ev_class.resize(a->ev.size());
+    a->drop_graph();
+  }
+  cudaStream_t st = ctx->stream;
+  float k_ms[K_CLASSES] = {0, 0, 0, 0};
+  float total_ms = 0.0f;
+  int launches_total = 0;
+  int remaining = frames;
+  while (remaining > 0) {
+    int k = std::min(spf, remaining);
+    RenderK K = make_k(p, a, k, shadow_cap);
+    int nlaunch = 0;
+    if (k == spf) {
+      bool cached = a->gexec && a->g_scene == sc && a->g_ver == sc->version && a->g_spf == spf &&
+                    a->g_timed == timed && std::memcmp(&a->g_params, p, sizeof(*p)) == 0;
+      if (!cached) {
+        a->drop_graph();
+        cudaGraph_t g;
+        CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_wave(a, sc, K, timed, &nlaunch);
+        CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+        CUDA_TRY(ctx, cudaGraphInstantiate(&a->gexec, g, 0));
+        cudaGraphDestroy(g);
+        a->g_scene = sc;
+        a->g_ver = sc->version;
+        a->g_spf = spf;
+        a->g_timed = timed;
+        a->g_params = *p;
+        a->g_launches = nlaunch;
+      }
+      nlaunch = a->g_launches;
+      CUDA_TRY(ctx, cudaGraphLaunch(a->gexec, st));
+    } else {
+      enqueue_wave(a, sc, K, timed, &nlaunch);
+    }
+    launches_total += nlaunch;
+    if (timed) {
+      CUDA_TRY(ctx, cudaStreamSynchronize(st));
+      // events: start, after generate, after each bounce kernel, after accumulate
+      int ne = 2;
+      for (int b = 0; b < p->max_depth; ++b) ne += (b < p->direct_light_max_depth && nl > 0) ? 3 : 2;
+      ne += 1;
+      for (int i = 1; i < ne; ++i) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a->ev[i - 1], a->ev[i]);
+        k_ms[a->ev_class[i]] += ms;
+        total_ms += ms;
+      }
+    }
+    remaining -= k;
+  }
+  a->frames += frames;
+  a->last_launches = launches_total;
+  if (timed) {
+    a->last_ms = total_ms;
+    for (int i = 0; i < K_CLASSES; ++i) a->last_k[i] = k_ms[i];
+  }
+  return check_device_error(ctx);
+}
+
+int accum_read(Accum* a, int which, float* host_out) {
+  Ctx* ctx = a->ctx;
+  const float4* src = nullptr;
+  int comp = 3;
+  switch (which) {
+    case RX_ACC_RADIANCE: src = a->acc_r.p; break;
+    case RX_ACC_NORMAL: src = a->acc_n.p; break;
+    case RX_ACC_ALBEDO: src = a->acc_a.p; break;
+    case RX_ACC_DEPTH: src = a->acc_n.p; comp = 1; break;
+    case RX_ACC_DISPLAY: src = a->pixels.p; break;
+    default: return set_error(ctx, "accum_read: unknown buffer %d", which), RX_ERR_ARG;
+  }
+  DevBuf<float> tmp(ctx, (size_t)a->P * comp);
+  int blocks = (int)std::min<long long>((a->P + 255) / 256, (long long)ctx->num_sms * 16);
+  k_pack<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(a->P, src, comp, tmp.p);
+  CUDA_TRY(ctx, cudaMemcpyAsync(host_out, tmp.p, tmp.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RX_OK;
+}
+
+int accum_info(Accum* a, int* w, int* h, int* frames, long long* rays) {
+  Ctx* ctx = a->ctx;
+  unsigned long long r = 0;
+  int fb = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&r, a->rays.p, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(&fb, a->frame_base.p, sizeof(fb), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (w) *w = a->W;
+  if (h) *h = a->H;
+  if (frames) *frames = fb;
+  if (rays) *rays = (long long)r;
+  return RX_OK;
+}
+
+int accum_set_timing(Accum* a, int on) {
+  a->timing = on;
+  return RX_OK;
+}
+
+int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernels, int* launches) {
+  if (ms_total) *ms_total = a->last_ms;
+  for (int i = 0; i < n_kernels && i < K_CLASSES; ++i) ms_kernels[i] = a->last_k[i];
+  if (launches) *launches = a->last_launches;
+  return RX_OK;
+}
+
+int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out) {
+  Ctx* ctx = a->ctx;
+  if (!a->dn0.p) {
+    if (!a->dn0.alloc(ctx, a->P) || !a->dn1.alloc(ctx, a->P) || !a->dn_out.alloc(ctx, a->P))
+      return set_error(ctx, "out of device memory for denoise buffers"), RX_ERR_CAPACITY;
+  }
+  int rc = denoise_device(ctx, a->H, a->W, a->acc_r.p, a->acc_n.p, a->acc_a.p, dp->use_normal, dp->use_albedo,
+                          dp->use_depth, dp, a->dn_out.p, a->dn0.p, a->dn1.p, dp->to_display);
+  if (rc) return rc;
+  if (host_out) {
+    DevBuf<float> tmp(ctx, (size_t)a->P * 3);
+    int blocks = (int)std::min<long long>((a->P + 255) / 256, (long long)ctx->num_sms * 16);
+    k_pack<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(a->P, a->dn_out.p, 3, tmp.p);
+    CUDA_TRY(ctx, cudaMemcpyAsync(host_out, tmp.p, tmp.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return RX_OK;
+}
+
+}  // namespace rx

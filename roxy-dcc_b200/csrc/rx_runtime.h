@@ -1,0 +1,191 @@
+// Host-side runtime objects behind the C ABI: context (device, stream, error
+// text), stream-ordered device buffers, scene and accumulation state.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rx_internal.cuh"
+
+namespace rx {
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  std::string err;
+  std::recursive_mutex mu;
+  int* d_err = nullptr;  // device error bits
+};
+
+void set_error(Ctx* ctx, const char* fmt, ...);
+
+#define CUDA_TRY(ctx, expr)                                                          \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess) {                                                         \
+      ::rx::set_error((ctx), "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                      __FILE__, __LINE__);                                           \
+      return RX_ERR_CUDA;                                                            \
+    }                                                                                \
+  } while (0)
+
+// Device buffer allocated and freed in stream order on the context's stream,
+// so temporaries may be released right after the kernels that use them are
+// enqueued.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  Ctx* ctx = nullptr;
+  DevBuf() {}
+  DevBuf(Ctx* c, size_t count) { alloc(c, count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  bool alloc(Ctx* c, size_t count) {
+    release();
+    ctx = c;
+    n = count;
+    if (count == 0) return true;
+    if (cudaMallocAsync((void**)&p, sizeof(T) * count, c->stream) != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+      return false;
+    }
+    return true;
+  }
+  void release() {
+    if (p && ctx) cudaFreeAsync(p, ctx->stream);
+    p = nullptr;
+    n = 0;
+  }
+  void swap(DevBuf& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+    std::swap(ctx, o.ctx);
+  }
+  size_t bytes() const { return sizeof(T) * n; }
+};
+
+struct HostMat {
+  int type;
+  float albedo[3];
+  float roughness, ior, emission;
+};
+
+struct Scene {
+  Ctx* ctx = nullptr;
+  // source triangles (caller order)
+  int n_tris = 0;
+  DevBuf<float> v0b, v1b, v2b, n0b, n1b, n2b;
+  DevBuf<int> tri_matb;
+  float *d_v0 = nullptr, *d_v1 = nullptr, *d_v2 = nullptr;
+  float *d_n0 = nullptr, *d_n1 = nullptr, *d_n2 = nullptr;
+  int* d_tri_mat = nullptr;
+  // palette: caller materials followed by one entry per object slot
+  std::vector<HostMat> user_mats;
+  std::vector<HostMat> obj_mats;
+  DevBuf<float4> mat_a, mat_b;
+  int n_mats = 0;
+  // object slots (reference _obj_* layout)
+  std::vector<ObjSlot> objs;
+  DevBuf<ObjSlot> d_objs;
+  int n_lin = 0;
+  std::vector<int> lin_slot;         // linear index -> object slot
+  std::vector<int> bvh_sphere_slots;
+  // lights
+  DevBuf<Light> d_lights;
+  DevBuf<float> d_alias_prob;
+  DevBuf<int> d_alias_idx;
+  int n_lights = 0;
+  // traversal structure
+  DevBuf<float4> d_nodes, d_prims, d_shade;
+  int n_nodes = 0, n_prims = 0, n_bvh_spheres = 0;
+  float3 root_min = {0, 0, 0}, root_max = {0, 0, 0};
+  int method = -1, exact_slab = 0, leaf_size = 0, depth = 0;
+  // reference-format copy (reference builder / uploaded trees)
+  DevBuf<int> ref_left, ref_right, ref_start, ref_count, order;
+  DevBuf<float3> ref_min, ref_max;
+  DevBuf<uint32_t> tmp_codes;
+  uint64_t version = 0;  // bumped on every change; invalidates cached graphs
+
+  void clear_bvh() {
+    d_nodes.release();
+    d_prims.release();
+    d_shade.release();
+    ref_left.release();
+    ref_right.release();
+    ref_start.release();
+    ref_count.release();
+    order.release();
+    ref_min.release();
+    ref_max.release();
+    n_nodes = n_prims = n_bvh_spheres = 0;
+    depth = 0;
+    method = -1;
+    ++version;
+  }
+  int upload_palette(Ctx* c);
+  int upload_linear_objects(Ctx* c, bool exclude_spheres);
+  DevScene view() const {
+    DevScene s;
+    s.nodes = d_nodes.p;
+    s.n_nodes = n_nodes;
+    s.root_min = root_min;
+    s.root_max = root_max;
+    s.prims = d_prims.p;
+    s.shade = d_shade.p;
+    s.n_prims = n_prims;
+    s.mat_a = mat_a.p;
+    s.mat_b = mat_b.p;
+    s.n_mats = n_mats;
+    s.objs = d_objs.p;
+    s.n_objs = n_lin;
+    s.lights = d_lights.p;
+    s.alias_prob = d_alias_prob.p;
+    s.alias_idx = d_alias_idx.p;
+    s.n_lights = n_lights;
+    s.exact_slab = exact_slab;
+    return s;
+  }
+};
+
+// BVH builders (rx_bvh.cu)
+int build_reference(Ctx* ctx, Scene* sc, int leaf);
+int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t, float c_i);
+int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min, const float* node_max,
+                        const int* left, const int* right, const int* start, const int* count, const int* order);
+
+// traversal entry points (rx_trace.cu)
+int trace_closest(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_rd, float* d_t, int* d_id,
+                  float* d_u, float* d_v);
+int trace_any(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_rd, const float* d_tmax, int* d_occ);
+int scene_query(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_rd, float* d_t, int* d_kind,
+                int* d_id, float* d_u, float* d_v, float* d_n);
+
+// Per-image accumulation and wavefront state (rx_render.cu)
+struct Accum;
+Accum* accum_new(Ctx* ctx, int w, int h);
+void accum_delete(Accum* a);
+int accum_reset(Accum* a);
+int render(Scene* sc, Accum* a, const rx_render_params* p, int frames);
+int accum_read(Accum* a, int which, float* host_out);
+int accum_info(Accum* a, int* w, int* h, int* frames, long long* rays);
+int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out);
+int accum_set_timing(Accum* a, int on);
+int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
+
+// Denoise on caller buffers (rx_denoise.cu)
+int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal, const float* albedo,
+                 const float* depth, const rx_denoise_params* dp, float* out);
+int denoise_device(Ctx* ctx, int h, int w, const float4* d_color, const float4* d_guide_n, const float4* d_guide_a,
+                   int has_normal, int has_albedo, int has_depth, const rx_denoise_params* dp, float4* d_out,
+                   float4* d_scratch0, float4* d_scratch1, int to_display);
+
+}  // namespace rx

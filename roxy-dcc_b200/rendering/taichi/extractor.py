@@ -1,0 +1,215 @@
+"""extract_scene: scene graph -> device scene (rendering/taichi/extractor.py).
+
+Flattens World objects the way the reference does — Mesh triangles and
+IndexedMesh arrays in world space into one triangle set with a material
+palette, analytic primitives into object slots — but in vectorised numpy
+and one upload per array instead of per-element field stores.  The BVH is
+built on the GPU.
+"""
+import numpy as np
+
+import roxy_native as nat
+from rendering.taichi.bvh_builder import GPUBVHBuilder, TriangleBatch
+from rendering.taichi.lights import build_lights
+
+_DEFAULT_ALBEDO = (0.8, 0.8, 0.8)
+
+
+def _mat_record(mat):
+    from scene.scene_object import SceneObject
+    if mat is None:
+        return {"mat_type": 0, "albedo": list(_DEFAULT_ALBEDO), "roughness": 0.0, "ior": 1.0, "emission": 0.0,
+                "texture_idx": -1}
+    r = SceneObject.material_record(mat)
+    r["texture_idx"] = -1
+    return r
+
+
+def _xform_points(M, pts):
+    """Row-by-row `M.transform_point` with the same double-precision order."""
+    r = M.rows
+    x, y, z = pts[:, 0], pts[:, 1], pts[:, 2]
+    X = x * r[0][0] + y * r[0][1] + z * r[0][2] + r[0][3]
+    Y = x * r[1][0] + y * r[1][1] + z * r[1][2] + r[1][3]
+    Z = x * r[2][0] + y * r[2][1] + z * r[2][2] + r[2][3]
+    W = x * r[3][0] + y * r[3][1] + z * r[3][2] + r[3][3]
+    out = np.stack([X, Y, Z], axis=1)
+    nz = W != 0
+    out[nz] = out[nz] / W[nz, None]
+    return out
+
+
+def _xform_normals(M, nrm):
+    """`inv_T.transform_vector(n).normalize()` per row (v * (1 / |v|))."""
+    r = M.rows
+    x, y, z = nrm[:, 0], nrm[:, 1], nrm[:, 2]
+    X = x * r[0][0] + y * r[0][1] + z * r[0][2]
+    Y = x * r[1][0] + y * r[1][1] + z * r[1][2]
+    Z = x * r[2][0] + y * r[2][1] + z * r[2][2]
+    length = np.sqrt(X * X + Y * Y + Z * Z)
+    inv = np.where(length > 0, 1.0 / np.where(length > 0, length, 1.0), 0.0)
+    return np.stack([X * inv, Y * inv, Z * inv], axis=1)
+
+
+def _mesh_batch(obj, shape, mesh):
+    tris = mesh._triangles
+    if not tris:
+        return None
+    M = obj.world_matrix
+    inv_T = obj.world_inverse_transpose_matrix
+    n = len(tris)
+    V = np.empty((n, 3, 3), np.float64)
+    N = np.empty((n, 3, 3), np.float64)
+    UV = np.zeros((n, 3, 2), np.float64)
+    has_uv = np.zeros(n, np.int32)
+    groups = {}
+    mat_idx = np.empty(n, np.int32)
+    recs = []
+    for i, t in enumerate(tris):
+        V[i, 0], V[i, 1], V[i, 2] = tuple(t._v0), tuple(t._v1), tuple(t._v2)
+        f = t._normal
+        N[i, 0] = tuple(t._n0 if t._n0 is not None else f)
+        N[i, 1] = tuple(t._n1 if t._n1 is not None else f)
+        N[i, 2] = tuple(t._n2 if t._n2 is not None else f)
+        if t._uv0 is not None and t._uv1 is not None and t._uv2 is not None:
+            UV[i, 0], UV[i, 1], UV[i, 2] = tuple(t._uv0), tuple(t._uv1), tuple(t._uv2)
+            has_uv[i] = 1
+        g = t._group
+        if g not in groups:
+            groups[g] = len(recs)
+            recs.append(_mat_record(shape.material_for_group(g)))
+        mat_idx[i] = groups[g]
+    Vw = _xform_points(M, V.reshape((-1, 3))).reshape((n, 3, 3)).astype(np.float32)
+    Nw = _xform_normals(inv_T, N.reshape((-1, 3))).reshape((n, 3, 3)).astype(np.float32)
+    k = len(recs)
+    return TriangleBatch(Vw[:, 0], Vw[:, 1], Vw[:, 2], Nw[:, 0], Nw[:, 1], Nw[:, 2],
+                         np.array([r["mat_type"] for r in recs], np.int32).reshape(k),
+                         np.array([r["albedo"] for r in recs], np.float32).reshape((k, 3)),
+                         np.array([r["roughness"] for r in recs], np.float32).reshape(k),
+                         np.array([r["ior"] for r in recs], np.float32).reshape(k),
+                         np.array([r["emission"] for r in recs], np.float32).reshape(k),
+                         uv0=UV[:, 0], uv1=UV[:, 1], uv2=UV[:, 2], has_uv=has_uv,
+                         texture_idx=np.full(k, -1, np.int32), mat_idx=mat_idx)
+
+
+def collect(world):
+    """(triangle batches, object slots) of every renderable object.  IndexedMesh
+    batches come first in visit order and Mesh triangles after them, the
+    order extract_scene gives the reference's builder."""
+    from scene.mesh import IndexedMesh, Mesh
+    slots, batches, mesh_batches = [], [], []
+
+    def visit(obj):
+        if not obj.renderable:
+            return
+        for shape in obj.shapes:
+            geo = shape.geometry
+            if isinstance(geo, Mesh):
+                b = _mesh_batch(obj, shape, geo)
+                if b is not None:
+                    mesh_batches.append(b)
+            elif isinstance(geo, IndexedMesh):
+                arrays = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+                mats = {gi: _mat_record(shape.material_for_group(g)) for gi, g in enumerate(arrays["groups"])}
+                batches.append(TriangleBatch.from_indexed_arrays(arrays, mats))
+            else:
+                exported = obj.taichi_export()
+                if isinstance(exported, list):
+                    slots.extend(exported)
+                elif exported:
+                    slots.append(exported)
+                break
+        for child in obj.children:
+            visit(child)
+
+    for o in world.objects:
+        visit(o)
+    return batches + mesh_batches, slots
+
+
+def slot_arrays(slots):
+    n = len(slots)
+    z3 = [0.0, 0.0, 0.0]
+    g = lambda k, d: [s.get(k, d) for s in slots]  # noqa: E731
+    return {"type": np.array(g("type", 0), np.int32).reshape(n),
+            "center": np.array(g("center", z3), np.float32).reshape((n, 3)),
+            "radius": np.array(g("radius", 0.0), np.float32).reshape(n),
+            "normal": np.array(g("normal", z3), np.float32).reshape((n, 3)),
+            "offset": np.array(g("offset", 0.0), np.float32).reshape(n),
+            "extra": np.array(g("extra", z3), np.float32).reshape((n, 3)),
+            "v0": np.array(g("v0", z3), np.float32).reshape((n, 3)),
+            "v1": np.array(g("v1", z3), np.float32).reshape((n, 3)),
+            "v2": np.array(g("v2", z3), np.float32).reshape((n, 3)),
+            "mat_type": np.array(g("mat_type", 0), np.int32).reshape(n),
+            "albedo": np.array(g("albedo", z3), np.float32).reshape((n, 3)),
+            "roughness": np.array(g("roughness", 0.0), np.float32).reshape(n),
+            "ior": np.array(g("ior", 1.0), np.float32).reshape(n),
+            "emission": np.array(g("emission", 0.0), np.float32).reshape(n)}
+
+
+class DeviceScene:
+    """Everything the renderer needs for one world: the native scene (with its
+    BVH), object slots and both light lists."""
+
+    def __init__(self, builder, slots, stats):
+        self.builder = builder
+        self.native = builder.native
+        self.slots = slots
+        self.stats = stats
+        self._lights_mode = None
+        b = builder._batch
+        pal = builder.palette_arrays()
+        self._light_args = (b.v0, b.v1, b.v2, builder._source_mat_idx, pal[0], pal[1], pal[4])
+
+    def use_lights(self, compat):
+        compat = bool(compat)
+        if self._lights_mode is compat:
+            return
+        lights = build_lights(self.slots, *self._light_args, compat=compat)
+        self.native.set_lights(lights)
+        self._lights_mode = compat
+
+
+class HostScene:
+    """Host-side flattening of a world: concatenated triangles, palette,
+    per-triangle palette index and object slots (no device work)."""
+
+    def __init__(self, world):
+        batches, slots = collect(world)
+        self.batches = batches
+        self.slots = slots
+        self.batch = TriangleBatch.concat(batches)
+        self.builder = GPUBVHBuilder()
+        self.mat_idx = (self.builder._material_indices(self.batch) if self.batch.triangle_count
+                        else np.zeros(0, np.int32))
+        self.palette = self.builder.palette_arrays()
+
+    def lights(self, compat):
+        b = self.batch
+        return build_lights(self.slots, b.v0, b.v1, b.v2, self.mat_idx, self.palette[0], self.palette[1],
+                            self.palette[4], compat=compat)
+
+
+def build_device_scene(world, method="lbvh", leaf_size=None):
+    batches, slots = collect(world)
+    builder = GPUBVHBuilder()
+    if leaf_size is not None:
+        builder.MAX_LEAF_SIZE = leaf_size
+    elif method == "lbvh":
+        builder.MAX_LEAF_SIZE = 4
+    native = nat.NativeScene()
+    native.set_objects(slot_arrays(slots) if slots else None)
+    builder.build(batches, method=method, native=native)
+    stats = {"primitive_count": len(slots), "bvh_nodes": len(builder.nodes),
+             "bvh_triangles": builder.triangle_count, "bvh_materials": len(builder.mat_palette) if batches else 0,
+             "bvh_leaf_size": builder.MAX_LEAF_SIZE if builder.triangle_count else 0}
+    return DeviceScene(builder, slots, stats)
+
+
+def extract_scene(world, method="lbvh"):
+    """Extract `world` to the device and make it the scene `render_kernel`
+    traces.  Returns the reference's stats dict."""
+    from rendering.taichi import fields
+    ds = build_device_scene(world, method=method)
+    fields.bind_scene(ds)
+    return dict(ds.stats)

@@ -1,0 +1,412 @@
+"""ctypes binding of libroxy_cuda.so (the C ABI in include/roxy.h).
+
+Every renderer, BVH and denoise entry point of this package goes through
+here.  There is no CPU fallback: if the library or a CUDA device is missing,
+`lib()` raises `NativeUnavailable` and the caller's operation fails.
+"""
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libroxy_cuda.so")
+REPO = os.path.dirname(HERE)
+SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu"]
+HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
+
+RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE = range(6)
+RX_BVH_REFERENCE, RX_BVH_LBVH_SAH = 0, 1
+RX_ACC_RADIANCE, RX_ACC_NORMAL, RX_ACC_ALBEDO, RX_ACC_DEPTH, RX_ACC_DISPLAY = range(5)
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i32p = ctypes.POINTER(ctypes.c_int)
+
+
+class NativeUnavailable(RuntimeError):
+    """The CUDA library or a CUDA device is not available."""
+
+
+class RxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class RenderParams(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("fov_tan", ctypes.c_float), ("aspect", ctypes.c_float),
+        ("cam_pos", ctypes.c_float * 3), ("cam_fwd", ctypes.c_float * 3), ("cam_right", ctypes.c_float * 3),
+        ("cam_up", ctypes.c_float * 3), ("max_depth", ctypes.c_int), ("use_sky", ctypes.c_int),
+        ("bg", ctypes.c_float * 3), ("direct_light_mode", ctypes.c_int), ("direct_light_max_depth", ctypes.c_int),
+        ("sample_clamp", ctypes.c_float), ("reference_compat", ctypes.c_int), ("seed", ctypes.c_uint32),
+        ("wave_paths", ctypes.c_int),
+    ]
+
+
+class DenoiseParams(ctypes.Structure):
+    _fields_ = [
+        ("radius", ctypes.c_int), ("passes", ctypes.c_int), ("sigma_color", ctypes.c_float),
+        ("sigma_normal", ctypes.c_float), ("sigma_albedo", ctypes.c_float), ("sigma_depth", ctypes.c_float),
+        ("amount", ctypes.c_float), ("use_normal", ctypes.c_int), ("use_albedo", ctypes.c_int),
+        ("use_depth", ctypes.c_int), ("to_display", ctypes.c_int),
+    ]
+
+
+def nvcc_command(out=LIB_PATH):
+    csrc = os.path.join(HERE, "csrc")
+    return ["nvcc", "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+            "-fmad=false", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static", "-o", out] + \
+        [os.path.join(csrc, s) for s in SOURCES]
+
+
+def build(force=False):
+    """Compile libroxy_cuda.so in-tree for sm_100a."""
+    csrc = os.path.join(HERE, "csrc")
+    deps = [os.path.join(csrc, s) for s in SOURCES + HEADERS] + [os.path.join(REPO, "include", "roxy.h")]
+    if not force and os.path.exists(LIB_PATH):
+        t = os.path.getmtime(LIB_PATH)
+        if all(os.path.getmtime(d) <= t for d in deps):
+            return LIB_PATH
+    subprocess.run(nvcc_command(), check=True)
+    return LIB_PATH
+
+
+_LIB = None
+_LOCK = threading.Lock()
+
+_SIGS = {
+    "rx_version": ([], ctypes.c_int),
+    "rx_device_count": ([_i32p], ctypes.c_int),
+    "rx_ctx_create": ([ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rx_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "rx_ctx_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_ctx_stream": ([ctypes.c_void_p], ctypes.c_void_p),
+    "rx_scene_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rx_scene_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_scene_set_triangles": ([ctypes.c_void_p, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
+    "rx_scene_set_materials": ([ctypes.c_void_p, ctypes.c_int, _i32p, _f32p, _f32p, _f32p, _f32p], ctypes.c_int),
+    "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 9 + [_i32p] + [_f32p] * 4,
+                             ctypes.c_int),
+    "rx_scene_set_lights": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p], ctypes.c_int),
+    "rx_bvh_build": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "rx_bvh_set_reference": ([ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, _i32p],
+                             ctypes.c_int),
+    "rx_bvh_info": ([ctypes.c_void_p] + [_i32p] * 5, ctypes.c_int),
+    "rx_bvh_export_reference": ([ctypes.c_void_p, _f32p, _f32p] + [_i32p] * 5, ctypes.c_int),
+    "rx_bvh_export_layout": ([ctypes.c_void_p, _f32p, _i32p], ctypes.c_int),
+    "rx_trace_closest": ([ctypes.c_void_p, ctypes.c_long, _f32p, _f32p, _f32p, _i32p, _f32p, _f32p], ctypes.c_int),
+    "rx_trace_closest_device": ([ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 6, ctypes.c_int),
+    "rx_trace_any": ([ctypes.c_void_p, ctypes.c_long, _f32p, _f32p, _f32p, _i32p], ctypes.c_int),
+    "rx_scene_intersect": ([ctypes.c_void_p, ctypes.c_long, _f32p, _f32p, _f32p, _i32p, _i32p, _f32p, _f32p, _f32p],
+                           ctypes.c_int),
+    "rx_accum_create": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+                        ctypes.c_int),
+    "rx_accum_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_accum_reset": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_render": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(RenderParams), ctypes.c_int], ctypes.c_int),
+    "rx_accum_read": ([ctypes.c_void_p, ctypes.c_int, _f32p], ctypes.c_int),
+    "rx_accum_info": ([ctypes.c_void_p, _i32p, _i32p, _i32p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "rx_accum_denoise": ([ctypes.c_void_p, ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
+    "rx_accum_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_accum_last_timing": ([ctypes.c_void_p, _f32p, _f32p, ctypes.c_int, _i32p], ctypes.c_int),
+    "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
+                    ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
+}
+
+
+def load_library(path=LIB_PATH):
+    """dlopen the library and declare every exported signature (no GPU needed)."""
+    if not os.path.exists(path):
+        raise NativeUnavailable(f"{path} is missing; build it with __graft_entry__.build()")
+    L = ctypes.CDLL(path)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+def lib():
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            _LIB = load_library()
+        return _LIB
+
+
+def fptr(a):
+    return None if a is None else a.ctypes.data_as(_f32p)
+
+
+def iptr(a):
+    return None if a is None else a.ctypes.data_as(_i32p)
+
+
+def f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """One device + stream.  Shared process-wide per device (see context())."""
+
+    def __init__(self, device=0):
+        L = lib()
+        n = ctypes.c_int(0)
+        L.rx_device_count(ctypes.byref(n))
+        if n.value <= 0:
+            raise NativeUnavailable("no CUDA device is visible to libroxy_cuda.so")
+        h = ctypes.c_void_p()
+        self._check(L.rx_ctx_create(int(device), ctypes.byref(h)), None)
+        self.h = h
+        self.device = device
+
+    def _check(self, rc, handle=None):
+        if rc != RX_OK:
+            msg = lib().rx_last_error(handle if handle is not None else getattr(self, "h", None))
+            msg = msg.decode() if msg else f"error {rc}"
+            if rc == RX_ERR_ARG:
+                raise ValueError(msg)
+            if rc == RX_ERR_CAPACITY:
+                raise AssertionError(msg)
+            raise RxError(rc, msg)
+
+    def check(self, rc):
+        self._check(rc, self.h)
+
+    @property
+    def stream(self):
+        return lib().rx_ctx_stream(self.h)
+
+    def sync(self):
+        self.check(lib().rx_ctx_sync(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rx_ctx_destroy(self.h)
+            self.h = None
+
+
+_CTX = {}
+
+
+def context(device=0):
+    if device not in _CTX:
+        _CTX[device] = Context(device)
+    return _CTX[device]
+
+
+class NativeScene:
+    """Owns an rx_scene: triangles, palette, object slots, lights and a BVH."""
+
+    def __init__(self, ctx=None):
+        self.ctx = ctx or context()
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().rx_scene_create(self.ctx.h, ctypes.byref(h)))
+        self.h = h
+        self.n_tris = 0
+        self.n_objects = 0
+        self.n_lights = 0
+
+    def set_triangles(self, v0, v1, v2, n0=None, n1=None, n2=None, mat_idx=None):
+        v0, v1, v2 = f32(v0, (-1, 3)), f32(v1, (-1, 3)), f32(v2, (-1, 3))
+        n = len(v0)
+        n0 = f32(n0, (-1, 3)) if n0 is not None else np.tile(np.float32([0, 0, 1]), (n, 1))
+        n1 = f32(n1, (-1, 3)) if n1 is not None else n0
+        n2 = f32(n2, (-1, 3)) if n2 is not None else n0
+        mat = i32(mat_idx) if mat_idx is not None else np.zeros(n, np.int32)
+        if not (len(v1) == len(v2) == len(n0) == len(n1) == len(n2) == len(mat) == n):
+            raise ValueError("triangle arrays must all have the same length")
+        self.ctx.check(lib().rx_scene_set_triangles(self.h, n, fptr(v0), fptr(v1), fptr(v2), fptr(n0), fptr(n1),
+                                                    fptr(n2), iptr(mat)))
+        self.n_tris = n
+
+    def set_materials(self, mat_type, albedo, roughness, ior, emission):
+        t = i32(mat_type)
+        n = len(t)
+        self.ctx.check(lib().rx_scene_set_materials(self.h, n, iptr(t), fptr(f32(albedo, (-1, 3))),
+                                                    fptr(f32(roughness)), fptr(f32(ior)), fptr(f32(emission))))
+
+    def set_objects(self, slots):
+        """slots: dict of arrays in the reference's _obj_* layout (len n)."""
+        n = 0 if not slots else len(slots["type"])
+        if n == 0:
+            self.ctx.check(lib().rx_scene_set_objects(self.h, 0, *([None] * 15)))
+            self.n_objects = 0
+            return
+        g = {k: f32(slots[k], (-1, 3)) for k in ("center", "normal", "extra", "v0", "v1", "v2", "albedo")}
+        s = {k: f32(slots[k]) for k in ("radius", "offset", "roughness", "ior", "emission")}
+        self.ctx.check(lib().rx_scene_set_objects(
+            self.h, n, iptr(i32(slots["type"])), fptr(g["center"]), fptr(s["radius"]), fptr(g["normal"]),
+            fptr(s["offset"]), fptr(g["extra"]), fptr(g["v0"]), fptr(g["v1"]), fptr(g["v2"]),
+            iptr(i32(slots["mat_type"])), fptr(g["albedo"]), fptr(s["roughness"]), fptr(s["ior"]),
+            fptr(s["emission"])))
+        self.n_objects = n
+
+    def set_lights(self, lights):
+        n = 0 if not lights else len(lights["kind"])
+        if n == 0:
+            self.ctx.check(lib().rx_scene_set_lights(self.h, 0, *([None] * 11)))
+            self.n_lights = 0
+            return
+        self.ctx.check(lib().rx_scene_set_lights(
+            self.h, n, iptr(i32(lights["kind"])), fptr(f32(lights["p0"], (-1, 3))), fptr(f32(lights["p1"], (-1, 3))),
+            fptr(f32(lights["p2"], (-1, 3))), fptr(f32(lights["albedo"], (-1, 3))), fptr(f32(lights["emission"])),
+            fptr(f32(lights["area"])), fptr(f32(lights["pick_pdf"])), fptr(f32(lights["alias_prob"])),
+            iptr(i32(lights["alias_idx"]))))
+        self.n_lights = n
+
+    def build_bvh(self, method=RX_BVH_LBVH_SAH, max_leaf=4, spheres_in_bvh=True):
+        self.ctx.check(lib().rx_bvh_build(self.h, int(method), int(max_leaf), int(bool(spheres_in_bvh))))
+
+    def set_reference_bvh(self, node_min, node_max, left, right, start, count, order):
+        n = len(left)
+        self.ctx.check(lib().rx_bvh_set_reference(self.h, n, fptr(f32(node_min, (-1, 3))),
+                                                  fptr(f32(node_max, (-1, 3))), iptr(i32(left)), iptr(i32(right)),
+                                                  iptr(i32(start)), iptr(i32(count)), iptr(i32(order))))
+
+    def bvh_info(self):
+        v = [ctypes.c_int() for _ in range(5)]
+        self.ctx.check(lib().rx_bvh_info(self.h, *[ctypes.byref(x) for x in v]))
+        return dict(n_nodes=v[0].value, n_prims=v[1].value, method=v[2].value, leaf_size=v[3].value,
+                    depth=v[4].value)
+
+    def export_reference(self):
+        info = self.bvh_info()
+        nn = info["n_nodes"]
+        out = dict(node_min=np.zeros((nn, 3), np.float32), node_max=np.zeros((nn, 3), np.float32),
+                   left=np.zeros(nn, np.int32), right=np.zeros(nn, np.int32), start=np.zeros(nn, np.int32),
+                   count=np.zeros(nn, np.int32), order=np.zeros(max(self.n_tris, 1), np.int32))
+        self.ctx.check(lib().rx_bvh_export_reference(self.h, fptr(out["node_min"]), fptr(out["node_max"]),
+                                                     iptr(out["left"]), iptr(out["right"]), iptr(out["start"]),
+                                                     iptr(out["count"]), iptr(out["order"])))
+        out["order"] = out["order"][: self.n_tris]
+        return out
+
+    def export_layout(self):
+        info = self.bvh_info()
+        nodes = np.zeros((info["n_nodes"], 16), np.float32)
+        order = np.zeros(max(info["n_prims"], 1), np.int32)
+        self.ctx.check(lib().rx_bvh_export_layout(self.h, fptr(nodes), iptr(order)))
+        return nodes, order[: info["n_prims"]]
+
+    def trace_closest(self, ro, rd):
+        ro, rd = f32(ro, (-1, 3)), f32(rd, (-1, 3))
+        n = len(ro)
+        t = np.zeros(n, np.float32)
+        idx = np.zeros(n, np.int32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        self.ctx.check(lib().rx_trace_closest(self.h, n, fptr(ro), fptr(rd), fptr(t), iptr(idx), fptr(u), fptr(v)))
+        return t, idx, u, v
+
+    def trace_any(self, ro, rd, tmax):
+        ro, rd, tmax = f32(ro, (-1, 3)), f32(rd, (-1, 3)), f32(tmax)
+        n = len(ro)
+        out = np.zeros(n, np.int32)
+        self.ctx.check(lib().rx_trace_any(self.h, n, fptr(ro), fptr(rd), fptr(tmax), iptr(out)))
+        return out
+
+    def intersect(self, ro, rd):
+        ro, rd = f32(ro, (-1, 3)), f32(rd, (-1, 3))
+        n = len(ro)
+        out = dict(t=np.zeros(n, np.float32), kind=np.zeros(n, np.int32), id=np.zeros(n, np.int32),
+                   u=np.zeros(n, np.float32), v=np.zeros(n, np.float32), normal=np.zeros((n, 3), np.float32))
+        self.ctx.check(lib().rx_scene_intersect(self.h, n, fptr(ro), fptr(rd), fptr(out["t"]), iptr(out["kind"]),
+                                                iptr(out["id"]), fptr(out["u"]), fptr(out["v"]),
+                                                fptr(out["normal"])))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _LIB is not None:
+            _LIB.rx_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Accumulator:
+    """rx_accum: progressive running means and wavefront buffers for W x H."""
+
+    def __init__(self, width, height, ctx=None):
+        self.ctx = ctx or context()
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().rx_accum_create(self.ctx.h, int(width), int(height), ctypes.byref(h)))
+        self.h = h
+        self.width, self.height = int(width), int(height)
+
+    def reset(self):
+        self.ctx.check(lib().rx_accum_reset(self.h))
+
+    def render(self, scene, params, frames):
+        self.ctx.check(lib().rx_render(scene.h, self.h, ctypes.byref(params), int(frames)))
+
+    def read(self, which):
+        shape = (self.height, self.width) if which == RX_ACC_DEPTH else (self.height, self.width, 3)
+        out = np.zeros(shape, np.float32)
+        self.ctx.check(lib().rx_accum_read(self.h, int(which), fptr(out)))
+        return out
+
+    def info(self):
+        w, h, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        r = ctypes.c_longlong()
+        self.ctx.check(lib().rx_accum_info(self.h, ctypes.byref(w), ctypes.byref(h), ctypes.byref(f),
+                                           ctypes.byref(r)))
+        return dict(width=w.value, height=h.value, frames=f.value, rays=r.value)
+
+    def denoise(self, params, out=True):
+        res = np.zeros((self.height, self.width, 3), np.float32) if out else None
+        self.ctx.check(lib().rx_accum_denoise(self.h, ctypes.byref(params), fptr(res)))
+        return res
+
+    def set_timing(self, on):
+        self.ctx.check(lib().rx_accum_set_timing(self.h, int(bool(on))))
+
+    def last_timing(self):
+        tot = ctypes.c_float()
+        ks = (ctypes.c_float * 4)()
+        nl = ctypes.c_int()
+        self.ctx.check(lib().rx_accum_last_timing(self.h, ctypes.byref(tot), ks, 4, ctypes.byref(nl)))
+        return dict(total_ms=tot.value, extend_ms=ks[0], shade_ms=ks[1], connect_ms=ks[2], other_ms=ks[3],
+                    launches=nl.value)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _LIB is not None:
+            _LIB.rx_accum_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def denoise(color, normal=None, albedo=None, depth=None, radius=1, sigma_color=0.08, amount=1.0,
+            sigma_normal=0.35, sigma_albedo=0.20, sigma_depth=1.0, passes=1, to_display=False, ctx=None):
+    """edge_aware_denoise / a-trous on host arrays through rx_denoise."""
+    ctx = ctx or context()
+    c = f32(color)
+    H, W = c.shape[:2]
+    p = DenoiseParams(int(radius), int(passes), float(sigma_color), float(sigma_normal), float(sigma_albedo),
+                      float(sigma_depth), float(amount), 0, 0, 0, int(bool(to_display)))
+    out = np.zeros((H, W, 3), np.float32)
+    nn = f32(normal) if normal is not None else None
+    aa = f32(albedo) if albedo is not None else None
+    dd = f32(depth).reshape(H, W) if depth is not None else None
+    ctx.check(lib().rx_denoise(ctx.h, H, W, fptr(c), fptr(nn), fptr(aa), fptr(dd), ctypes.byref(p), fptr(out)))
+    return out

@@ -1,0 +1,199 @@
+"""Wavefront renderer parity.
+
+1. Same random numbers: the CUDA wavefront and the oracle's per-path loop
+   draw identical Philox numbers, so per-pixel radiance agrees closely
+   (differences come only from sin/cos/acos last bits that can send a
+   grazing path elsewhere).
+2. Statistical: the default estimator (NEE to emissive triangles and
+   spheres) converges to the reference estimator (reference_compat, sphere
+   lights only, as trace.py): per-pixel means agree within 3 sigma.
+3. Ray-count and guide contracts of the reference renderers.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import golden_scenes as gs
+import helpers
+import roxy_native as nat
+import workloads
+from oracle import oracle
+from rendering.image import Image
+from rendering.ray_tracer import RayTracer
+from rendering.taichi.extractor import HostScene, build_device_scene
+from rendering.taichi.trace import make_params
+from rendering.taichi_renderer import TaichiRenderer
+from test_host_logic import _ns
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_render(world, W, H, spp, max_depth, compat=False, mode=0, dlmd=1, clamp=10.0, seed=0, wave_paths=0,
+                method="lbvh"):
+    ds = build_device_scene(world, method=method)
+    ds.use_lights(compat)
+    cam = world.active_camera
+    p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, max_depth, world._use_sky, mode,
+                    dlmd, clamp, list(world._background_color), list(cam.position), list(cam.forward),
+                    list(cam.right), list(cam.up), reference_compat=compat, seed=seed, wave_paths=wave_paths)
+    acc = nat.Accumulator(W, H)
+    acc.render(ds.native, p, spp)
+    out = {k: acc.read(w) for k, w in (("radiance", nat.RX_ACC_RADIANCE), ("normal", nat.RX_ACC_NORMAL),
+                                       ("albedo", nat.RX_ACC_ALBEDO), ("depth", nat.RX_ACC_DEPTH),
+                                       ("pixels", nat.RX_ACC_DISPLAY))}
+    out["rays"] = acc.info()["rays"]
+    return out
+
+
+def _oracle_render(world, W, H, spp, max_depth, compat=False, mode=0, dlmd=1, clamp=10.0, seed=0):
+    h = HostScene(world)
+    sc = helpers.oracle_scene(h, compat)
+    p = helpers.oracle_params(world, W, H, max_depth, compat=compat, mode=mode, dlmd=dlmd, clamp=clamp, seed=seed)
+    return oracle.render(sc, p, spp)
+
+
+def _agree(a, b, tol=1e-4):
+    d = np.abs(a - b) / (np.abs(b) + 1e-2)
+    return float(np.mean(np.all(d < tol, axis=-1) if d.ndim == 3 else d < tol))
+
+
+@pytest.mark.parametrize("compat,mode,dlmd", [(False, 0, 8), (True, 0, 8), (False, 1, 2), (True, 1, 1)])
+def test_trace_scene_same_randoms_as_oracle(compat, mode, dlmd):
+    world = gs.build_trace_scene(_ns())
+    W = H = 48
+    g = _gpu_render(world, W, H, 6, 8, compat, mode, dlmd, seed=3)
+    o = _oracle_render(world, W, H, 6, 8, compat, mode, dlmd, seed=3)
+    assert _agree(g["radiance"], o["radiance"]) > 0.97
+    assert abs(g["radiance"].mean() - o["radiance"].mean()) < 0.01 * o["radiance"].mean() + 1e-4
+    assert abs(g["rays"] - o["rays"]) <= 0.01 * o["rays"]
+    # first-hit guides and display buffer
+    assert _agree(g["normal"], o["normal"], 1e-3) > 0.97
+    assert _agree(g["albedo"], o["albedo"], 1e-4) > 0.97
+    assert _agree(g["depth"], o["depth"], 1e-4) > 0.97
+    assert _agree(g["pixels"], o["pixels"], 1e-3) > 0.97
+
+
+def test_cornell_same_randoms_and_wavefront_sizes():
+    world = workloads.cornell_box(64, 64)
+    o = _oracle_render(world, 64, 64, 8, 8, dlmd=8, seed=1)
+    for wp in (0, 4096, 64 * 64 * 3):
+        g = _gpu_render(world, 64, 64, 8, 8, dlmd=8, seed=1, wave_paths=wp)
+        assert _agree(g["radiance"], o["radiance"]) > 0.98, wp
+        assert abs(g["rays"] - o["rays"]) <= 0.005 * o["rays"]
+
+
+def _batch_means(world, W, H, batches, per, compat, seed0, **kw):
+    ds = build_device_scene(world, method="lbvh")
+    ds.use_lights(compat)
+    cam = world.active_camera
+    acc = nat.Accumulator(W, H)
+    means = []
+    for b in range(batches):
+        acc.reset()
+        p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, kw.get("max_depth", 8),
+                        world._use_sky, 0, kw.get("dlmd", 8), 0.0, list(world._background_color),
+                        list(cam.position), list(cam.forward), list(cam.right), list(cam.up),
+                        reference_compat=compat, seed=seed0 + b)
+        acc.render(ds.native, p, per)
+        means.append(acc.read(nat.RX_ACC_RADIANCE))
+    return np.array(means)
+
+
+@pytest.mark.parametrize("scene_name", ["cornell", "trace"])
+def test_converges_to_reference_estimator_3sigma(scene_name):
+    world = workloads.cornell_box(24, 24) if scene_name == "cornell" else gs.build_trace_scene(_ns())
+    W = H = 24
+    new = _batch_means(world, W, H, 16, 32, False, 100)
+    ref = _batch_means(world, W, H, 16, 32, True, 500)
+    m_new, m_ref = new.mean(0), ref.mean(0)
+    se = np.sqrt(new.var(0, ddof=1) / len(new) + ref.var(0, ddof=1) / len(ref)) + 1e-6
+    z = np.abs(m_new - m_ref) / se
+    # with ~1700 independent channel tests, |z| > 3 occurs ~0.3 % of the time
+    assert np.mean(z > 3) < 0.02, np.mean(z > 3)
+    assert abs(m_new.mean() - m_ref.mean()) < 0.02 * m_ref.mean()
+
+
+def _tiny_world(use_sky):
+    from core import Color, Vec3
+    from scene import Camera, World
+    w = World(use_sky=use_sky)
+    w.add_camera(Camera(width=4, height=4))
+    return w, Vec3, Color
+
+
+def test_ray_count_contracts():
+    w, Vec3, Color = _tiny_world(True)
+    rt = RayTracer(w, Image(4, 4), None, samples=3, max_depth=4, threaded=False)
+    rt.render()
+    assert rt.last_ray_count == 4 * 4 * 3 and rt.last_stats.rays_per_pixel == 3
+    assert rt.last_stats.samples_rendered == 3
+    assert (Image(4, 4).pixels == 0).all()
+    rt = RayTracer(w, Image(4, 4), None, samples=2, max_depth=0, threaded=False)
+    rt.render()
+    assert rt.last_ray_count == 0 and rt.last_stats.max_depth == 0
+    w2, _, _ = _tiny_world(False)
+    img = Image(4, 4)
+    rt = RayTracer(w2, img, None, samples=1, max_depth=4, threaded=False)
+    rt.render()
+    assert np.allclose(img.pixels, 0)
+    img = Image(4, 4)
+    rt = RayTracer(w, img, None, samples=1, max_depth=4, threaded=False)
+    rt.render()
+    assert img.pixels.max() > 0
+    assert "Render report" in rt.last_stats.format_report()
+
+
+def test_direct_light_depth_zero_skips_shadow_rays():
+    from core import Color, Vec3
+    from scene import Camera, Diffuse, Emissive, SceneObject, Sphere, World
+    w = World(use_sky=False)
+    w.add_camera(Camera(width=4, height=4))
+    w.add_object(SceneObject(shape=Sphere(), material=Diffuse(Color(0.8, 0.8, 0.8)), translation=Vec3(0, 0, -3)))
+    w.add_object(SceneObject(shape=Sphere(), material=Emissive(Color(1, 1, 1), intensity=40.0),
+                             translation=Vec3(0, 2, -1), scale=Vec3(0.5, 0.5, 0.5)))
+    img = Image(4, 4)
+    rt = RayTracer(w, img, None, samples=1, max_depth=1, threaded=False, direct_light_max_depth=0)
+    rt.render()
+    assert np.allclose(img.pixels, 0) and rt.last_ray_count == 16
+    img = Image(4, 4)
+    rt = RayTracer(w, img, None, samples=1, max_depth=1, threaded=False)
+    rt.render()
+    assert img.pixels.sum() > 0 and rt.last_ray_count > 16
+
+
+def test_taichi_renderer_end_to_end_with_denoise():
+    world = workloads.cornell_box(64, 64)
+    img = Image(64, 64)
+    r = TaichiRenderer(world, img, None, samples=8, max_depth=8, denoise=True, denoise_passes=5,
+                       direct_light_max_depth=8)
+    r.render()
+    s = r.last_stats
+    assert s.samples_rendered == 8 and s.rays_cast == r.last_ray_count > 64 * 64 * 8
+    assert s.bvh_triangles == 36 and s.bvh_nodes > 0
+    assert np.isfinite(img.pixels).all() and 0.05 < img.pixels.mean() < 1.0
+    assert img.pixels.max() <= 1.0 and img.pixels.min() >= 0.0
+    # the renderer's denoise equals the standalone filter on the same buffers
+    acc = r.accumulator
+    lin = acc.read(nat.RX_ACC_RADIANCE)
+    from rendering.denoise import edge_aware_denoise, linear_to_display
+    ref = linear_to_display(edge_aware_denoise(lin, 1, 0.08, 0.8, normal=acc.read(nat.RX_ACC_NORMAL),
+                                               albedo=acc.read(nat.RX_ACC_ALBEDO), depth=acc.read(nat.RX_ACC_DEPTH),
+                                               passes=5))
+    np.testing.assert_allclose(img.pixels, ref, atol=1e-6)
+
+
+def test_progressive_accumulation_equals_one_shot():
+    world = workloads.cornell_box(32, 32)
+    ds = build_device_scene(world)
+    ds.use_lights(False)
+    cam = world.active_camera
+    p = make_params(32, 32, math.tan(math.radians(cam.fov) / 2), 1.0, 8, 0, 0, 8, 10.0, [0, 0, 0],
+                    list(cam.position), list(cam.forward), list(cam.right), list(cam.up), seed=5)
+    a = nat.Accumulator(32, 32)
+    a.render(ds.native, p, 12)
+    b = nat.Accumulator(32, 32)
+    for k in (1, 4, 3, 4):
+        b.render(ds.native, p, k)
+    np.testing.assert_array_equal(a.read(nat.RX_ACC_RADIANCE), b.read(nat.RX_ACC_RADIANCE))
+    assert a.info()["rays"] == b.info()["rays"] and b.info()["frames"] == 12

@@ -1,0 +1,170 @@
+"""Host-side logic of the drop-in API, checked on the CPU: batches, palette
+dedupe, scene flattening, light lists, sampling helpers."""
+import os
+
+import numpy as np
+import pytest
+
+import golden_scenes as gs
+from oracle import oracle
+from rendering.sampling import (clamp_color_sample, gpu_pixel_sample_offset, mis_power_weight, philox4x32,
+                                pixel_sample_offset)
+from rendering.taichi.bvh_builder import GPUBVHBuilder, TriangleBatch
+from rendering.taichi.extractor import HostScene, slot_arrays
+from rendering.taichi.lights import alias_table
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+class NS:
+    pass
+
+
+def _ns():
+    import core
+    import scene
+    ns = NS()
+    ns.Vec3, ns.Color = core.Vec3, core.Color
+    for n in ("World", "Camera", "SceneObject", "Sphere", "Plane", "Cube", "Mesh", "Triangle", "IndexedMesh",
+              "Diffuse", "Metal", "Dielectric", "Shape", "Emissive", "Glossy"):
+        setattr(ns, n, getattr(scene, n))
+    return ns
+
+
+def _tri(x, **kw):
+    d = {'v0': [x, 0, 0], 'v1': [x + 1, 0, 0], 'v2': [x, 1, 0], 'n0': [0, 0, 1], 'n1': [0, 0, 1], 'n2': [0, 0, 1],
+         'mat_type': 0, 'albedo': [1, 1, 1], 'roughness': 0.0, 'ior': 1.0, 'emission': 0.0}
+    d.update(kw)
+    return d
+
+
+def test_triangle_batch_validation():
+    with pytest.raises(ValueError, match="same length"):
+        TriangleBatch(np.zeros((2, 3)), np.zeros((1, 3)), np.zeros((2, 3)), np.zeros((2, 3)), np.zeros((2, 3)),
+                      np.zeros((2, 3)), [0, 0], np.zeros((2, 3)), [0, 0], [1, 1], [0, 0])
+    with pytest.raises(ValueError, match="material arrays must match"):
+        TriangleBatch(np.zeros((2, 3)), np.zeros((2, 3)), np.zeros((2, 3)), np.zeros((2, 3)), np.zeros((2, 3)),
+                      np.zeros((2, 3)), [0], np.zeros((1, 3)), [0], [1], [0])
+
+
+def test_indexed_batch_keeps_compact_palette():
+    arrays = {'v0': [[0, 0, 0], [2, 0, 0], [4, 0, 0]], 'v1': [[1, 0, 0], [3, 0, 0], [5, 0, 0]],
+              'v2': [[0, 1, 0], [2, 1, 0], [4, 1, 0]], 'n0': [[0, 0, 1]] * 3, 'n1': [[0, 0, 1]] * 3,
+              'n2': [[0, 0, 1]] * 3, 'uv0': [[0, 0]] * 3, 'uv1': [[1, 0]] * 3, 'uv2': [[0, 1]] * 3,
+              'has_uv': [1, 1, 1], 'group_idx': [0, 1, 0]}
+    mats = {0: {'mat_type': 0, 'albedo': [1, 0, 0], 'roughness': 0, 'ior': 1, 'emission': 0, 'texture_idx': 3},
+            1: {'mat_type': 1, 'albedo': [0, 1, 0], 'roughness': 0.25, 'ior': 1, 'emission': 0, 'texture_idx': -1},
+            2: {'mat_type': 0, 'albedo': [0, 0, 1], 'roughness': 0, 'ior': 1, 'emission': 0, 'texture_idx': -1}}
+    b = TriangleBatch.from_indexed_arrays(arrays, mats)
+    assert b.triangle_count == 3 and len(b.mat_palette) == 2 and list(b.mat_idx) == [0, 1, 0]
+    assert b.mat_palette[0]['texture_idx'] == 3
+
+
+def test_palette_dedupe_matches_reference_builder():
+    g = np.load(os.path.join(GOLD, "bvh_palette.npz"))
+    batch = TriangleBatch.from_dicts([_tri(0), _tri(2, albedo=[0.5, 0.5, 0.5]), _tri(4, mat_type=1, roughness=0.25),
+                                      _tri(6)])
+    b = GPUBVHBuilder()
+    src = b._material_indices(batch)
+    assert [m['type'] for m in b.mat_palette] == list(g["palette_type"])
+    np.testing.assert_array_equal(np.array([m['albedo'] for m in b.mat_palette], np.float32), g["palette_albedo"])
+    # the golden is in BVH order; the dedupe assigns the same ids per triangle
+    assert sorted(src.tolist()) == sorted(g["ordered_mat_idx"].tolist())
+
+
+def test_concat_mixes_palette_and_per_triangle_batches():
+    per_tri = TriangleBatch.from_dicts([_tri(0), _tri(2, albedo=[0.5, 0.5, 0.5])])
+    arrays = {'v0': [[0, 0, 0]], 'v1': [[1, 0, 0]], 'v2': [[0, 1, 0]], 'n0': [[0, 0, 1]], 'n1': [[0, 0, 1]],
+              'n2': [[0, 0, 1]], 'group_idx': [0]}
+    pal = TriangleBatch.from_indexed_arrays(arrays, {0: {'mat_type': 1, 'albedo': [0, 1, 0], 'roughness': 0.3,
+                                                         'ior': 1, 'emission': 0}})
+    cat = TriangleBatch.concat([per_tri, pal])
+    assert cat.triangle_count == 3 and cat.mat_idx is not None
+    b = GPUBVHBuilder()
+    idx = b._material_indices(cat)
+    assert [b.mat_palette[i]['type'] for i in idx] == [0, 0, 1]
+
+
+def test_indexed_mesh_flattening_matches_reference():
+    g = np.load(os.path.join(GOLD, "indexed_arrays.npz"))
+    obj = gs.build_indexed_object(_ns())
+    geo = obj.shapes[0].geometry
+    np.testing.assert_allclose(np.array(obj.world_matrix.rows), g["world_matrix"], rtol=0, atol=1e-15)
+    arrs = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+    for k in ("v0", "v1", "v2", "n0", "n1", "n2", "uv0", "uv1", "uv2", "has_uv", "group_idx"):
+        np.testing.assert_array_equal(arrs[k], g[k], err_msg=k)
+
+
+def test_trace_scene_flattening_matches_reference_extract():
+    """Object slots, palette and BVH-ordered triangles equal extract_scene's."""
+    g = np.load(os.path.join(GOLD, "trace_scene.npz"))
+    h = HostScene(gs.build_trace_scene(_ns()))
+    sa = slot_arrays(h.slots)
+    for k in ("type", "mat_type"):
+        np.testing.assert_array_equal(sa[k], g[f"obj_{k}"], err_msg=k)
+    for k in ("center", "radius", "normal", "offset", "extra", "v0", "v1", "v2", "albedo", "roughness", "ior",
+              "emission"):
+        np.testing.assert_allclose(sa[k], g[f"obj_{k}"], rtol=1e-6, atol=1e-7, err_msg=k)
+    bvh = oracle.bvh_build_morton(h.batch.v0, h.batch.v1, h.batch.v2, 8)
+    np.testing.assert_array_equal(bvh["left"], g["left"])
+    o = bvh["order"]
+    for k in ("v0", "v1", "v2", "n0", "n1", "n2"):
+        np.testing.assert_array_equal(getattr(h.batch, k)[o], g[k], err_msg=k)
+    np.testing.assert_array_equal(h.mat_idx[o], g["tri_mat"])
+    np.testing.assert_array_equal(h.palette[0], g["mat_type"])
+    np.testing.assert_array_equal(h.palette[1], g["mat_albedo"])
+    lights = h.lights(compat=True)
+    np.testing.assert_allclose(lights["p0"], g["light_center"], rtol=1e-6)
+    np.testing.assert_allclose(lights["p1"][:, 0], g["light_radius"], rtol=1e-6)
+
+
+def test_alias_table_reproduces_distribution():
+    w = np.array([1.0, 3.0, 0.5, 5.5, 0.0])
+    prob, alias, pdf = alias_table(w)
+    n = len(w)
+    got = np.zeros(n)
+    for c in range(n):
+        got[c] += prob[c] / n
+        got[alias[c]] += (1 - prob[c]) / n
+    np.testing.assert_allclose(got, w / w.sum(), atol=1e-6)
+    np.testing.assert_allclose(pdf, w / w.sum(), atol=1e-7)
+
+
+def test_philox_python_matches_oracle():
+    for ctr, key in (([0, 0, 0, 0], (0, 0)), ([1, 2, 3, 4], (5, 6)), ([0xFFFFFFFF] * 4, (7, 0x5EEDC0DE))):
+        assert list(philox4x32(ctr, key)) == list(oracle.philox(ctr, *key))
+
+
+def test_sampling_helpers_match_reference_contracts():
+    g = np.load(os.path.join(GOLD, "sampling.npz"))["offsets"]
+    for y in range(16):
+        for x in range(16):
+            for f in range(8):
+                assert pixel_sample_offset(x, y, f) == tuple(g[y, x, f])
+    for f in range(8):
+        jx, jy = gpu_pixel_sample_offset(12, 34, f, 64)
+        assert 0.0 <= jx < 1.0 and 0.0 <= jy < 1.0
+    assert gpu_pixel_sample_offset(4, 5, 0, 64) != gpu_pixel_sample_offset(4, 5, 1, 64)
+    assert gpu_pixel_sample_offset(4, 5, 0, 64) != gpu_pixel_sample_offset(5, 5, 0, 64)
+    from core import Color
+    c = Color(20, -1, 2)
+    assert clamp_color_sample(c, None) is c and clamp_color_sample(c, 0) is c
+    cc = clamp_color_sample(c, 10.0)
+    assert (cc.r, cc.g, cc.b) == (10.0, 0.0, 2.0)
+    assert abs(mis_power_weight(2.0, 2.0) - 0.5) < 1e-12
+    assert mis_power_weight(0.0, 4.0) == 0.0 and mis_power_weight(4.0, 0.0) == 1.0 and mis_power_weight(0, 0) == 0
+
+
+def test_renderer_rejects_bad_light_mode():
+    from rendering.image import Image
+    from rendering.ray_tracer import RayTracer
+    from rendering.taichi_renderer import TaichiRenderer
+    import workloads
+    w = workloads.cornell_box(8, 8)
+    with pytest.raises(ValueError):
+        TaichiRenderer(w, Image(8, 8), None, direct_light_mode="bogus")
+    with pytest.raises(ValueError):
+        RayTracer(w, Image(8, 8), None, direct_light_mode="bogus")
+    with pytest.raises(ValueError):
+        RayTracer(w, Image(8, 8), None, adaptive_min_samples=0)
+    assert "3" in repr(TaichiRenderer(w, Image(8, 8), None, samples=3))

@@ -586,6 +586,10 @@ inline V3 direct_light_full(const orc_scene& s, const orc_params& p, Rng& rng, u
   V3 direct = mk(0.0f, 0.0f, 0.0f);
   int nl = s.n_lights;
   if (nl <= 0) return direct;
+  // light samples are taken from the normal-offset point the shadow ray and
+  // the continuation ray start from, so a grazing shadow ray cannot clip the
+  // sampled emitter's own plane before max_t
+  const V3 sp = hit_p + n * 1e-4f;
   int first = 0, last = nl;
   if (p.direct_light_mode == 0) {
     float r0 = rng.get(bounce, SLOT_LIGHT_PICK);
@@ -604,12 +608,12 @@ inline V3 direct_light_full(const orc_scene& s, const orc_params& p, Rng& rng, u
     if (s.light_kind[i] == 0) {
       V3 ldir;
       float tl, sop;
-      sphere_light_sample(hit_p, ld3(s.light_p0, i), s.light_p1[3 * i], ru1, ru2, ldir, tl, sop);
+      sphere_light_sample(sp, ld3(s.light_p0, i), s.light_p1[3 * i], ru1, ru2, ldir, tl, sop);
       float ndotl = dot(n, ldir);
       if (ndotl > 0.0f) {
         float max_t = tl * 0.999f;
         if (max_t > 0.001f) {
-          V3 so = hit_p + n * 1e-4f;
+          V3 so = sp;
           cnt.rays++;
           if (!scene_occluded(s, so, ldir, max_t))
             direct = direct + ((base * ndotl) * sop) * inv_pick;
@@ -622,7 +626,7 @@ inline V3 direct_light_full(const orc_scene& s, const orc_params& p, Rng& rng, u
       float b2 = su * ru2;
       V3 e1 = b - a, e2 = c - a;
       V3 y = (a + e1 * b1) + e2 * b2;
-      V3 to = y - hit_p;
+      V3 to = y - sp;
       float d2 = dot(to, to);
       float d = std::sqrt(d2);
       V3 wi = to * (1.0f / d);
@@ -632,7 +636,7 @@ inline V3 direct_light_full(const orc_scene& s, const orc_params& p, Rng& rng, u
         float cos_l = std::fabs(dot(ln, wi));
         float max_t = d * 0.999f;
         if (max_t > 0.001f) {
-          V3 so = hit_p + n * 1e-4f;
+          V3 so = sp;
           cnt.rays++;
           if (!scene_occluded(s, so, wi, max_t)) {
             float g = (((ndotl * cos_l) * s.light_area[i]) / (kPi * d2)) * inv_pick;

@@ -412,7 +412,12 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
         rad_b[p] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, 0.0f);
       }
     }
-    // next-event estimation: shadow records for connect
+    // next-event estimation: shadow records for connect.  The default
+    // estimator samples lights from the normal-offset point the shadow ray
+    // starts at (a grazing shadow ray then cannot clip the sampled emitter's
+    // own plane); reference_compat samples from the hit point as trace.py
+    // does.
+    const float3 nee_p = K.compat ? hit_p : hit_p + nrm * 1e-4f;
     if (K.mode == 0) {
       bool emit = false;
       float3 dir = f3(0, 0, 0), val = f3(0, 0, 0);
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
           li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
           w = 1.0f / S.lights[li].pick_pdf;
         }
-        emit = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), hit_p, nrm, alb, w, dir,
+        emit = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
                             max_t, val);
       }
       int slot = warp_append(emit, &counters[C_S + b]);
@@ -454,7 +459,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
         float max_t = 0.0f;
         if (do_nee) {
           int s1 = SLOT_ALL_LIGHTS + 4 * li;
-          emit = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), hit_p, nrm, alb, 1.0f, dir, max_t, val);
+          emit = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val);
         }
         int slot = warp_append(emit, &counters[C_S + b]);
         if (emit) {

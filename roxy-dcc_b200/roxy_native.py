@@ -89,7 +89,7 @@ _SIGS = {
     "rx_scene_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "rx_scene_set_triangles": ([ctypes.c_void_p, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
     "rx_scene_set_materials": ([ctypes.c_void_p, ctypes.c_int, _i32p, _f32p, _f32p, _f32p, _f32p], ctypes.c_int),
-    "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 9 + [_i32p] + [_f32p] * 4,
+    "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p] + [_f32p] * 4,
                              ctypes.c_int),
     "rx_scene_set_lights": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p], ctypes.c_int),
     "rx_bvh_build": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -241,7 +241,7 @@ class NativeScene:
         """slots: dict of arrays in the reference's _obj_* layout (len n)."""
         n = 0 if not slots else len(slots["type"])
         if n == 0:
-            self.ctx.check(lib().rx_scene_set_objects(self.h, 0, *([None] * 15)))
+            self.ctx.check(lib().rx_scene_set_objects(self.h, 0, *([None] * 14)))
             self.n_objects = 0
             return
         g = {k: f32(slots[k], (-1, 3)) for k in ("center", "normal", "extra", "v0", "v1", "v2", "albedo")}
@@ -256,7 +256,7 @@ class NativeScene:
     def set_lights(self, lights):
         n = 0 if not lights else len(lights["kind"])
         if n == 0:
-            self.ctx.check(lib().rx_scene_set_lights(self.h, 0, *([None] * 11)))
+            self.ctx.check(lib().rx_scene_set_lights(self.h, 0, *([None] * 10)))
             self.n_lights = 0
             return
         self.ctx.check(lib().rx_scene_set_lights(

@@ -95,9 +95,8 @@ def _box_mesh(sx, sy, sz):
 
 CORNELL = dict(width=256, height=256, samples=16, max_depth=8, fov=40.0)
 
-
-def cornell_box(width=256, height=256):
-    """Config-1 Cornell box (36 triangles)."""
+def cornell_box(width=256, height=256, light_gap=1e-3, light_size=0.25):
+    """Config-1 Cornell box (36 triangles); the light hangs `light_gap` below the ceiling."""
     world = World(use_sky=False, background_color=Color(0, 0, 0))
     world.add_camera(Camera(position=Vec3(0.5, 0.5, 2.4), forward=Vec3(0, 0, -1), up=Vec3(0, 1, 0), fov=40,
                             width=width, height=height))
@@ -105,10 +104,11 @@ def cornell_box(width=256, height=256):
     red = Diffuse(Color(0.65, 0.05, 0.05))
     green = Diffuse(Color(0.12, 0.45, 0.15))
     light = Emissive(Color(17, 12, 4), intensity=1)
-    ly = 1.0 - 1e-3
+    ly = 1.0 - light_gap
+    lo, hi = 0.5 - light_size / 2, 0.5 + light_size / 2
     pos = np.array([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1],          # floor
                     [0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1],          # ceiling
-                    [0.375, ly, 0.375], [0.625, ly, 0.375], [0.625, ly, 0.625], [0.375, ly, 0.625]],
+                    [lo, ly, lo], [hi, ly, lo], [hi, ly, hi], [lo, ly, hi]],
                    dtype=np.float64)
     faces = np.array([[0, 2, 1], [0, 3, 2],        # floor
                       [4, 5, 6], [4, 6, 7],        # ceiling

@@ -83,7 +83,7 @@ def test_cornell_same_randoms_and_wavefront_sizes():
         assert abs(g["rays"] - o["rays"]) <= 0.005 * o["rays"]
 
 
-def _batch_means(world, W, H, batches, per, compat, seed0, **kw):
+def _batch_means(world, W, H, batches, per, compat, seed0, dlmd=8, max_depth=8):
     ds = build_device_scene(world, method="lbvh")
     ds.use_lights(compat)
     cam = world.active_camera
@@ -91,10 +91,9 @@ def _batch_means(world, W, H, batches, per, compat, seed0, **kw):
     means = []
     for b in range(batches):
         acc.reset()
-        p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, kw.get("max_depth", 8),
-                        world._use_sky, 0, kw.get("dlmd", 8), 0.0, list(world._background_color),
-                        list(cam.position), list(cam.forward), list(cam.right), list(cam.up),
-                        reference_compat=compat, seed=seed0 + b)
+        p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, max_depth, world._use_sky, 0,
+                        dlmd, 0.0, list(world._background_color), list(cam.position), list(cam.forward),
+                        list(cam.right), list(cam.up), reference_compat=compat, seed=seed0 + b)
         acc.render(ds.native, p, per)
         means.append(acc.read(nat.RX_ACC_RADIANCE))
     return np.array(means)
@@ -102,16 +101,33 @@ def _batch_means(world, W, H, batches, per, compat, seed0, **kw):
 
 @pytest.mark.parametrize("scene_name", ["cornell", "trace"])
 def test_converges_to_reference_estimator_3sigma(scene_name):
-    world = workloads.cornell_box(24, 24) if scene_name == "cornell" else gs.build_trace_scene(_ns())
+    """Default estimator vs the reference's estimator, unclamped.
+
+    Cornell (light 2 cm under the ceiling): NEE to the emissive quad vs the
+    reference's BSDF-only transport (its NEE sees no triangle lights).  Mixed
+    scene (sphere light, glass, metal, glossy, plane, cube): NEE vs the
+    reference estimator without its sphere-light NEE, whose double count
+    makes it converge to a different image by construction.
+    Per 2x2 pixel block the means must agree within 3 sigma except for a few
+    blocks, and the image means within 4 sigma."""
     W = H = 24
-    new = _batch_means(world, W, H, 16, 32, False, 100)
-    ref = _batch_means(world, W, H, 16, 32, True, 500)
-    m_new, m_ref = new.mean(0), ref.mean(0)
-    se = np.sqrt(new.var(0, ddof=1) / len(new) + ref.var(0, ddof=1) / len(ref)) + 1e-6
-    z = np.abs(m_new - m_ref) / se
-    # with ~1700 independent channel tests, |z| > 3 occurs ~0.3 % of the time
-    assert np.mean(z > 3) < 0.02, np.mean(z > 3)
-    assert abs(m_new.mean() - m_ref.mean()) < 0.02 * m_ref.mean()
+    if scene_name == "cornell":
+        world = workloads.cornell_box(W, H, light_gap=0.02)
+        new = _batch_means(world, W, H, 32, 32, False, 100)
+        ref = _batch_means(world, W, H, 32, 32, True, 50000)
+    else:
+        world = gs.build_trace_scene(_ns())
+        new = _batch_means(world, W, H, 32, 32, False, 100)
+        ref = _batch_means(world, W, H, 32, 32, True, 50000, dlmd=0)
+    n = len(new)
+    A = new.reshape(n, H // 2, 2, W // 2, 2, 3).mean((2, 4))
+    R = ref.reshape(n, H // 2, 2, W // 2, 2, 3).mean((2, 4))
+    se = np.sqrt(A.var(0, ddof=1) / n + R.var(0, ddof=1) / n) + 1e-6
+    z = np.abs(A.mean(0) - R.mean(0)) / se
+    assert np.mean(z > 3) < 0.05, np.mean(z > 3)
+    ma, mr = new.mean((1, 2, 3)), ref.mean((1, 2, 3))
+    zm = abs(ma.mean() - mr.mean()) / np.sqrt(ma.var(ddof=1) / n + mr.var(ddof=1) / n)
+    assert zm < 4, (zm, ma.mean(), mr.mean())
 
 
 def _tiny_world(use_sky):

@@ -38,6 +38,16 @@ def test_binding_declares_every_symbol():
     assert set(_declared()) == set(nat._SIGS)
 
 
+def test_binding_argument_counts_match_header():
+    src = open(os.path.join(ROOT, "include", "roxy.h")).read()
+    decls = re.findall(r"^\s*(?:int|void\*|const char\*)\s+(rx_\w+)\s*\(([^;]*?)\)\s*;", src, re.M | re.S)
+    assert decls
+    for name, params in decls:
+        params = params.strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        assert len(nat._SIGS[name][0]) == n, f"{name}: header {n} args, binding {len(nat._SIGS[name][0])}"
+
+
 def test_errors_without_device_are_reported_not_raised(L):
     import ctypes
     n = ctypes.c_int(-1)

@@ -691,7 +691,8 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   int ev_i = 0;
   auto mark = [&](int cls) {
     if (timed) {
-      cudaEventRecord(a->ev[ev_i], st);
+      // External: inside stream capture this becomes an event-record node
+      cudaEventRecordWithFlags(a->ev[ev_i], st, cudaEventRecordExternal);
       a->ev_class[ev_i] = cls;
       ++ev_i;
     }
@@ -860,7 +861,7 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
       ne += 1;
       for (int i = 1; i < ne; ++i) {
         float ms = 0.0f;
-        cudaEventElapsedTime(&ms, a->ev[i - 1], a->ev[i]);
+        CUDA_TRY(ctx, cudaEventElapsedTime(&ms, a->ev[i - 1], a->ev[i]));
         k_ms[a->ev_class[i]] += ms;
         total_ms += ms;
       }

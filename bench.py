@@ -41,6 +41,10 @@ WORKLOADS = {
                       desc="displaced icosphere 327,680 tris + 64 spheres, 1920x1080, 64 spp, depth 12"),
     "cornell": dict(width=256, height=256, spp=16, max_depth=8, dlmd=8,
                     desc="Cornell box 36 tris, 256x256, 16 spp, depth 8, NEE every bounce"),
+    # same scene at 640x360 / 16 spp: the kernel-profiling case (same kernels,
+    # one wave of 3.7M paths, < 1 GB on the device)
+    "icosphere-small": dict(width=640, height=360, spp=16, max_depth=12, dlmd=1,
+                            desc="displaced icosphere 327,680 tris + 64 spheres, 640x360, 16 spp, depth 12"),
 }
 
 
@@ -48,6 +52,8 @@ def _world(name):
     import workloads
     if name == "icosphere":
         return workloads.displaced_icosphere_scene()
+    if name == "icosphere-small":
+        return workloads.displaced_icosphere_scene(640, 360)
     return workloads.cornell_box()
 
 
@@ -272,13 +278,18 @@ def run_ours(args):
     ext_rays = stats["extend_rays"]
     ext_gbs = 40.0 * ext_rays / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     shade_gbs = 272.0 * ext_rays / (shade_ms / 1e3) / 1e9 if shade_ms > 0 else 0.0
+    # DRAM bytes per k_extend launch: ncu's bytes per ray (committed summary,
+    # measured on the profiling case of this scene) times the average rays
+    # per launch here (max_depth launches per wave)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_extend.json")
+    spf = max(1, min(w["spp"], (1 << 22) // (W * H)))
+    ext_launches = w["max_depth"] * -(-w["spp"] // spf)
     if os.path.exists(tfile):
         try:
             with open(tfile) as f:
-                traffic = json.load(f).get("bytes_per_launch")
-        except (OSError, ValueError):
+                traffic = json.load(f)["bytes_per_ray"] * ext_rays / ext_launches
+        except (OSError, ValueError, KeyError):
             traffic = None
 
     # -- end to end through TaichiRenderer ------------------------------------

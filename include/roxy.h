@@ -171,6 +171,23 @@ int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int 
 int rx_denoise(rx_ctx* ctx, int height, int width, const float* color, const float* normal, const float* albedo,
                const float* depth, const rx_denoise_params* params, float* out);
 
+/* Allocation-free a-trous denoise on caller device buffers.  No counterpart in
+ * the reference: it exists for callers that cannot allocate device memory at
+ * call time (a host that owns the whole device budget through its own
+ * allocator, or a frame loop that must not pay the synchronisation an
+ * allocation can imply).  It makes no cudaMalloc/cudaFree call: the two
+ * intermediate pass buffers live in a fixed 32 MiB device array inside the
+ * library, which limits height * width to 1,048,576 pixels (larger sizes
+ * return RX_ERR_CAPACITY).  Buffers are float4 per pixel: colour (rgb, -),
+ * normal guide (xyz, depth), albedo guide (rgb, -), output (rgb, 0); guides
+ * are used as params->use_normal / use_albedo / use_depth say.  Runs on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) of the current
+ * device; the first call on a device looks the array up and should come
+ * before any stream capture.  Calls that can overlap on the GPU share the
+ * array and race; the caller orders them.  Errors: rx_last_error(NULL). */
+int rx_denoise_noalloc(int height, int width, const float* d_color, const float* d_guide_normal,
+                       const float* d_guide_albedo, const rx_denoise_params* params, float* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

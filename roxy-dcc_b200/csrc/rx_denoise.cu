@@ -15,6 +15,7 @@
 // filters its resident buffers without a copy.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "rx_internal.cuh"
 #include "rx_runtime.h"
@@ -208,4 +209,114 @@ int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal
   return RX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant (rx_denoise_noalloc).
+//
+// Some callers cannot allocate device memory when they denoise: a host
+// application that owns the whole device-memory budget through its own
+// allocator (a compositor or plugin host, a serving process with a fixed
+// HBM budget), or a frame loop that must not pay the device-wide
+// synchronisation a cudaMalloc / cudaFree can imply.  For them the two
+// intermediate a-trous buffers live in this file-scope device array instead
+// of per-call allocations.  It is sized for kNoAllocMaxPixels pixels
+// (2 x 16 B x 2^20 = 32 MiB) and every GPU that loads the library keeps it
+// until the process exits.
+//
+// The host never dereferences `g_noalloc_scratch`: in host code the name is
+// only a stand-in, so its device address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) the first time the entry
+// point runs there.  Make that first call on a device before any stream
+// capture.  Every pass writes every pixel of its output before the next pass
+// reads it, so nothing in the array has to start at zero; it keeps the last
+// call's contents.  All calls share the one array: calls whose kernels can
+// overlap on the GPU (different streams, or host threads on one device
+// without ordering) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+constexpr long long kNoAllocMaxPixels = 1LL << 20;
+static __device__ __align__(256) float4 g_noalloc_scratch[2 * kNoAllocMaxPixels];
+
+static std::mutex g_noalloc_mu;
+static float4* g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array on the current device.
+static int noalloc_scratch(float4** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(nullptr, "rx_denoise_noalloc: cudaGetDevice: %s", cudaGetErrorString(e)),
+                               RX_ERR_CUDA;
+  if (dev < 0 || dev >= 64) return set_error(nullptr, "rx_denoise_noalloc: device %d out of range", dev), RX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(nullptr, "rx_denoise_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
+    g_noalloc_ptr[dev] = static_cast<float4*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return RX_OK;
+}
+
 }  // namespace rx
+
+extern "C" int rx_denoise_noalloc(int height, int width, const float* d_color, const float* d_guide_normal,
+                                  const float* d_guide_albedo, const rx_denoise_params* params, float* d_out,
+                                  void* stream) {
+  using namespace rx;
+  if (!params || height < 0 || width < 0) return set_error(nullptr, "rx_denoise_noalloc: bad arguments"), RX_ERR_ARG;
+  long long P = (long long)height * width;
+  if (P > kNoAllocMaxPixels)
+    return set_error(nullptr, "rx_denoise_noalloc: %d x %d = %lld pixels exceeds the %lld-pixel scratch limit",
+                     height, width, P, kNoAllocMaxPixels),
+           RX_ERR_CAPACITY;
+  if (P == 0) return RX_OK;
+  if (!d_color || !d_out) return set_error(nullptr, "rx_denoise_noalloc: NULL colour or output"), RX_ERR_ARG;
+  if ((params->use_normal || params->use_depth) && !d_guide_normal)
+    return set_error(nullptr, "rx_denoise_noalloc: normal/depth guide requested but NULL"), RX_ERR_ARG;
+  if (params->use_albedo && !d_guide_albedo)
+    return set_error(nullptr, "rx_denoise_noalloc: albedo guide requested but NULL"), RX_ERR_ARG;
+  if (params->radius < 0 || params->passes < 1 || params->passes > 12)
+    return set_error(nullptr, "rx_denoise_noalloc: radius must be >= 0 and passes in [1, 12]"), RX_ERR_ARG;
+  float4* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float4* color = reinterpret_cast<const float4*>(d_color);
+  const float4* gn = reinterpret_cast<const float4*>(d_guide_normal);
+  const float4* ga = reinterpret_cast<const float4*>(d_guide_albedo);
+  float4* out = reinterpret_cast<float4*>(d_out);
+  if (params->radius <= 0 || params->amount <= 0.0f) {
+    int blocks = (int)std::min<long long>((P + 255) / 256, 4096);
+    k_copy_display<<<blocks, 256, 0, st>>>(P, color, out, params->to_display);
+  } else {
+    double amount = std::min(std::max((double)params->amount, 0.0), 1.0);
+    AtrousArgs A;
+    A.H = height;
+    A.W = width;
+    A.r = params->radius;
+    A.use_n = params->use_normal;
+    A.use_a = params->use_albedo;
+    A.use_d = params->use_depth;
+    A.s2c = two_sigma2(params->sigma_color);
+    A.s2n = two_sigma2(params->sigma_normal);
+    A.s2a = two_sigma2(params->sigma_albedo);
+    A.s2d = two_sigma2(params->sigma_depth);
+    A.keep = (float)(1.0 - amount);
+    A.amount = (float)amount;
+    A.to_display = params->to_display;
+    dim3 blk(32, 8);
+    dim3 grd((width + 31) / 32, (height + 7) / 8);
+    const float4* in = color;
+    for (int i = 0; i < params->passes; ++i) {
+      A.step = 1 << i;
+      A.last = i == params->passes - 1;
+      float4* o = A.last ? out : scratch + (size_t)(i & 1) * kNoAllocMaxPixels;
+      k_atrous<<<grd, blk, 0, st>>>(A, in, color, gn, ga, o);
+      in = o;
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_error(nullptr, "rx_denoise_noalloc: launch failed: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
+  return RX_OK;
+}

@@ -115,6 +115,8 @@ _SIGS = {
     "rx_accum_last_timing": ([ctypes.c_void_p, _f32p, _f32p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
+    "rx_denoise_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.POINTER(DenoiseParams), ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 

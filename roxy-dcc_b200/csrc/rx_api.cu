@@ -80,6 +80,15 @@ using namespace rx;
 
 #define LOCK(ctxp) std::lock_guard<std::recursive_mutex> _lk((ctxp)->mu)
 
+// SAH costs of one node traversal step and one primitive test, used to decide
+// which LBVH subtrees collapse into leaves.
+#ifndef RX_SAH_CT
+#define RX_SAH_CT 1.2f
+#endif
+#ifndef RX_SAH_CI
+#define RX_SAH_CI 1.0f
+#endif
+
 extern "C" {
 
 int rx_version(void) { return 1; }
@@ -310,12 +319,17 @@ int rx_bvh_build(rx_scene* scene, int method, int max_leaf, int spheres_in_bvh) 
   cudaSetDevice(c->device);
   if (max_leaf < 1 || max_leaf > (1 << 20)) return set_error(c, "max_leaf must be >= 1"), RX_ERR_ARG;
   int rc;
+  if ((long long)s.n_tris + (long long)s.objs.size() >= kMaxPrims)
+    return set_error(c, "bvh_build: %d primitives exceed the %d-primitive limit", s.n_tris, kMaxPrims),
+           RX_ERR_CAPACITY;
   if (method == RX_BVH_REFERENCE) {
+    if (max_leaf > kMaxLeafPrims)
+      return set_error(c, "bvh_build: leaves hold at most %d primitives", kMaxLeafPrims), RX_ERR_ARG;
     if ((rc = s.upload_linear_objects(c, false))) return rc;
     rc = build_reference(c, &s, max_leaf);
   } else if (method == RX_BVH_LBVH_SAH) {
     if (max_leaf > 15) return set_error(c, "LBVH leaves hold at most 15 primitives"), RX_ERR_ARG;
-    rc = build_lbvh(c, &s, max_leaf, spheres_in_bvh, 1.2f, 1.0f);
+    rc = build_lbvh(c, &s, max_leaf, spheres_in_bvh, RX_SAH_CT, RX_SAH_CI);
   } else {
     return set_error(c, "Unknown BVH build method: %d", method), RX_ERR_ARG;
   }
@@ -338,6 +352,9 @@ int rx_bvh_set_reference(rx_scene* scene, int n_nodes, const float* node_min, co
   // validate the tree before it reaches a kernel
   for (int i = 0; i < n_nodes; ++i) {
     if (left[i] == -1) {
+      if (tri_count[i] > kMaxLeafPrims)
+        return set_error(c, "bvh_set_reference: leaf %d holds %d > %d triangles", i, tri_count[i], kMaxLeafPrims),
+               RX_ERR_ARG;
       if (tri_start[i] < 0 || tri_count[i] < 0 || (long long)tri_start[i] + tri_count[i] > s.n_tris)
         return set_error(c, "bvh_set_reference: leaf %d range out of bounds", i), RX_ERR_ARG;
     } else if (left[i] <= 0 || left[i] >= n_nodes || right[i] <= 0 || right[i] >= n_nodes) {

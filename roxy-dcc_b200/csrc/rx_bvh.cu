@@ -365,17 +365,17 @@ __global__ void k_ref_to_layout(int n_nodes, const int* __restrict__ left, const
     if (left[i] == -1) {
       if (i != 0) continue;  // leaves live inside their parent's record
       l0 = nmin[0]; l1 = nmax[0];
-      lw = ~tstart[0]; lc = tcount[0];
+      lw = pack_leaf(tstart[0], tcount[0]); lc = tcount[0];
       r0 = f3(1e30f, 1e30f, 1e30f); r1 = r0;
-      rw = ~0; rc = 0;
+      rw = pack_leaf(0, 0); rc = 0;
     } else {
       l = left[i];
       r = right[i];
       l0 = nmin[l]; l1 = nmax[l];
       r0 = nmin[r]; r1 = nmax[r];
-      lw = left[l] == -1 ? ~tstart[l] : l;
+      lw = left[l] == -1 ? pack_leaf(tstart[l], tcount[l]) : l;
       lc = left[l] == -1 ? tcount[l] : 0;
-      rw = left[r] == -1 ? ~tstart[r] : r;
+      rw = left[r] == -1 ? pack_leaf(tstart[r], tcount[r]) : r;
       rc = left[r] == -1 ? tcount[r] : 0;
     }
     float4* o = out + 4 * (size_t)i;
@@ -542,11 +542,11 @@ __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int ncur, int o
       if (c < 0) {
         int p = order[~c];
         b0[s] = pmin[p]; b1[s] = pmax[p];
-        words[s] = c;  // ~sorted position: leaf of one primitive
+        words[s] = pack_leaf(~c, 1);  // one primitive at sorted position ~c
         counts[s] = 1;
       } else if (collapse[c]) {
         b0[s] = imin[c]; b1[s] = imax[c];
-        words[s] = ~first[c];
+        words[s] = pack_leaf(first[c], last[c] - first[c] + 1);
         counts[s] = last[c] - first[c] + 1;
       } else {
         b0[s] = imin[c]; b1[s] = imax[c];
@@ -573,16 +573,16 @@ __global__ void k_single_leaf_root(const float3* __restrict__ bmin, const float3
   out[0] = make_float4(l0.x, l1.x, l0.y, l1.y);
   out[1] = make_float4(l0.z, l1.z, r0.x, r0.x);
   out[2] = make_float4(r0.y, r0.y, r0.z, r0.z);
-  out[3] = make_float4(__int_as_float(~0), __int_as_float(~0), __int_as_float(cnt), __int_as_float(0));
+  out[3] = make_float4(__int_as_float(pack_leaf(0, cnt)), __int_as_float(pack_leaf(0, 0)), __int_as_float(cnt), __int_as_float(0));
 }
 
-__global__ void k_union_bounds(int n, const int* __restrict__ order, const float3* __restrict__ pmin,
-                               const float3* __restrict__ pmax, float3* __restrict__ out) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// Folds the per-block partial minima / maxima into out[0] (min), out[1] (max).
+__global__ void k_box_finish(int parts, const float3* __restrict__ part_min, const float3* __restrict__ part_max,
+                             float3* __restrict__ out) {
   float3 lo = f3(INFINITY, INFINITY, INFINITY), hi = f3(-INFINITY, -INFINITY, -INFINITY);
-  for (int k = 0; k < n; ++k) {
-    lo = vmin(lo, pmin[order[k]]);
-    hi = vmax(hi, pmax[order[k]]);
+  for (int k = 0; k < parts; ++k) {
+    lo = vmin(lo, part_min[k]);
+    hi = vmax(hi, part_max[k]);
   }
   out[0] = lo;
   out[1] = hi;
@@ -761,7 +761,14 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
                                                     sc->d_n1, sc->d_n2, sc->d_tri_mat, d_sph.p, d_sph_mat.p,
                                                     d_sph_slot.p, sc->d_prims.p, sc->d_shade.p);
   DevBuf<float3> rb(ctx, 2);
-  k_union_bounds<<<1, 32, 0, st>>>(n, order.p, pmin.p, pmax.p, rb.p);
+  {
+    // root box = union of all primitive boxes (two-stage parallel reduction)
+    int parts = std::min(grid_for(ctx, n), 1024);
+    DevBuf<float3> lo_min(ctx, parts), lo_max(ctx, parts), hi_min(ctx, parts), hi_max(ctx, parts);
+    k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmin.p, lo_min.p, lo_max.p);
+    k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmax.p, hi_min.p, hi_max.p);
+    k_box_finish<<<1, 1, 0, st>>>(parts, lo_min.p, hi_max.p, rb.p);
+  }
   float3 hb[2];
   cudaMemcpyAsync(hb, rb.p, sizeof(hb), cudaMemcpyDeviceToHost, st);
   int n_int = n - 1;

@@ -315,16 +315,131 @@ __device__ __forceinline__ bool slab1(float3 bmin, float3 bmax, float3 o, float3
   return tx >= te && tx >= 0.001f && te <= tmax;
 }
 
-// Closest hit over the BVH with an explicit stack of (child word, count,
-// entry distance).  Visits nodes in the reference's order: nearer child
-// first, ties to the right child (intersect.py:128-150).  tmax in: current
-// best distance (from the linear scan), out: closest hit.  Returns the
-// leaf-order primitive index or -1.
+// Packed child word: >= 0 internal node index; < 0 leaf with
+// ~word = (first primitive << kLeafBits) | primitive count.
+constexpr int kLeafBits = 5;
+constexpr int kMaxLeafPrims = (1 << kLeafBits) - 1;
+constexpr int kMaxPrims = 1 << (31 - kLeafBits);
+constexpr int kSentinel = 0x7fffffff;
+
+__host__ __device__ __forceinline__ int pack_leaf(int first, int count) { return ~((first << kLeafBits) | count); }
+__device__ __forceinline__ int leaf_first(int w) { return (~w) >> kLeafBits; }
+__device__ __forceinline__ int leaf_count(int w) { return (~w) & kMaxLeafPrims; }
+
+// Closest hit over the BVH (intersect.py:81-152 semantics): nearer child
+// first, ties to the right child, leaves tested in depth-first order, a hit
+// replaces the current one only when strictly closer.  The loop is the
+// while-while form with postponed leaves (Aila & Laine, "Understanding the
+// efficiency of ray traversal on GPUs", HPG 2009): a lane that reaches a leaf
+// parks it and keeps descending until every lane of the warp holds a leaf,
+// so leaf tests run together.  Leaves still execute in DFS order, so the
+// first hit found among equally distant ones is the reference's.
+// tmax in: current best distance (the linear scan's), out: closest hit.
+// Returns the leaf-order primitive index or -1.
 template <bool EXACT>
-__device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d, float& tmax, float& hu, float& hv,
-                                           int* err) {
+__device__ __forceinline__ int bvh_closest_ww(const DevScene& S, float3 o, float3 d, float& tmax, float& hu,
+                                              float& hv, int* err) {
+  int stack[kStack];
+  int sp = 0;
+  stack[0] = kSentinel;
+  float3 inv = make_inv_dir(d);
+  float3 oinv = o * inv;
+  int hit = -1;
+  float te;
+  if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
+  int node = 0, leaf = 0;  // leaf >= 0: no leaf parked
+  // each record is visited at most once per ray; the guard turns a
+  // malformed tree into an error flag instead of an endless loop
+  int guard = 4 * S.n_nodes + 64;
+  while (node != kSentinel) {
+    while ((unsigned)node < (unsigned)kSentinel) {
+      if (--guard < 0 || node >= S.n_nodes) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return hit;
+      }
+      const float4* np = S.nodes + 4 * (size_t)node;
+      float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+      bool hl, hr;
+      float tl, tr;
+      slab2<EXACT>(n0, n1, n2, o, inv, oinv, tmax, hl, hr, tl, tr);
+      int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
+      if (!hl && !hr) {
+        node = stack[sp--];
+      } else {
+        bool left_first = hl && (!hr || tl < tr);
+        node = left_first ? lw : rw;
+        if (hl && hr) {
+          if (sp + 1 < kStack) {
+            stack[++sp] = left_first ? rw : lw;
+          } else if (err) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+          }
+        }
+      }
+      if (node < 0 && leaf >= 0) {
+        leaf = node;
+        node = stack[sp--];
+      }
+      if (!__any_sync(__activemask(), leaf >= 0)) break;
+    }
+    while (leaf < 0) {
+      int first = leaf_first(leaf), cnt = leaf_count(leaf);
+      if (first + cnt > S.n_prims) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return hit;
+      }
+      for (int k = first; k < first + cnt; ++k) {
+        const float4* pp = S.prims + 3 * (size_t)k;
+        float4 a = __ldg(pp);
+        float t, u, v;
+        if (__float_as_int(a.w) == PRIM_TRI) {
+          float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
+          if (tri_hit(o, d, a, b, c, tmax, t, u, v)) {
+            tmax = t; hu = u; hv = v; hit = k;
+          }
+        } else {
+          float4 b = __ldg(pp + 1);
+          t = sphere_t(o, d, xyz(a), b.x);
+          if (t > 0.001f && t < tmax) {
+            tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
+          }
+        }
+      }
+      leaf = node;
+      if (node < 0) node = stack[sp--];
+    }
+  }
+  return hit;
+}
+
+// Leaf test shared by the closest-hit loops.
+__device__ __forceinline__ void leaf_closest(const DevScene& S, float3 o, float3 d, int first, int cnt, float& tmax,
+                                             float& hu, float& hv, int& hit) {
+  for (int k = first; k < first + cnt; ++k) {
+    const float4* pp = S.prims + 3 * (size_t)k;
+    float4 a = __ldg(pp);
+    float t, u, v;
+    if (__float_as_int(a.w) == PRIM_TRI) {
+      float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
+      if (tri_hit(o, d, a, b, c, tmax, t, u, v)) {
+        tmax = t; hu = u; hv = v; hit = k;
+      }
+    } else {
+      float4 b = __ldg(pp + 1);
+      t = sphere_t(o, d, xyz(a), b.x);
+      if (t > 0.001f && t < tmax) {
+        tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
+      }
+    }
+  }
+}
+
+// Closest hit, depth-first with (child word, entry distance) on the stack:
+// a popped entry farther than the current hit is skipped without a fetch.
+template <bool EXACT>
+__device__ __forceinline__ int bvh_closest_ii(const DevScene& S, float3 o, float3 d, float& tmax, float& hu,
+                                              float& hv, int* err) {
   int stk_w[kStack];
-  int stk_c[kStack];
   float stk_t[kStack];
   int sp = 0;
   float3 inv = make_inv_dir(d);
@@ -332,20 +447,14 @@ __device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d
   int hit = -1;
   float te;
   if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
-  int word = 0, cnt = 0;
+  int word = 0;
   float wt = te;
-  // a tree visits each record at most once per ray; the guard turns a
-  // malformed tree into an error flag instead of an endless loop
   int guard = 4 * S.n_nodes + 64;
   for (;;) {
-    if (--guard < 0) {
-      if (err) atomicOr(err, ERR_BAD_NODE);
-      break;
-    }
     if (wt <= tmax) {
-      if (word >= S.n_nodes || (word < 0 && (~word + cnt > S.n_prims || cnt < 0))) {
+      if (--guard < 0 || word >= S.n_nodes) {
         if (err) atomicOr(err, ERR_BAD_NODE);
-        break;
+        return hit;
       }
       if (word >= 0) {
         const float4* np = S.nodes + 4 * (size_t)word;
@@ -354,103 +463,169 @@ __device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d
         float tl, tr;
         slab2<EXACT>(n0, n1, n2, o, inv, oinv, tmax, hl, hr, tl, tr);
         int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
-        int lc = __float_as_int(n3.z), rc = __float_as_int(n3.w);
-        if (hl && hr) {
-          bool left_first = tl < tr;
-          int fw = left_first ? rw : lw, fc = left_first ? rc : lc;
-          float ft = left_first ? tr : tl;
-          if (sp < kStack) {
-            stk_w[sp] = fw; stk_c[sp] = fc; stk_t[sp] = ft; ++sp;
-          } else if (err) {
-            atomicOr(err, ERR_STACK_OVERFLOW);
+        if (hl || hr) {
+          bool left_first = hl && (!hr || tl < tr);
+          if (hl && hr) {
+            if (sp < kStack) {
+              stk_w[sp] = left_first ? rw : lw;
+              stk_t[sp] = left_first ? tr : tl;
+              ++sp;
+            } else if (err) {
+              atomicOr(err, ERR_STACK_OVERFLOW);
+            }
           }
           word = left_first ? lw : rw;
-          cnt = left_first ? lc : rc;
           wt = left_first ? tl : tr;
-          continue;
-        } else if (hl) {
-          word = lw; cnt = lc; wt = tl;
-          continue;
-        } else if (hr) {
-          word = rw; cnt = rc; wt = tr;
           continue;
         }
       } else {
-        int first = ~word;
-        for (int k = first; k < first + cnt; ++k) {
-          const float4* pp = S.prims + 3 * (size_t)k;
-          float4 a = __ldg(pp);
-          float t, u, v;
-          if (__float_as_int(a.w) == PRIM_TRI) {
-            float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
-            if (tri_hit(o, d, a, b, c, tmax, t, u, v)) {
-              tmax = t; hu = u; hv = v; hit = k;
-            }
-          } else {
-            float4 b = __ldg(pp + 1);
-            t = sphere_t(o, d, xyz(a), b.x);
-            if (t > 0.001f && t < tmax) {
-              tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
-            }
-          }
+        int first = leaf_first(word), cnt = leaf_count(word);
+        if (first + cnt > S.n_prims) {
+          if (err) atomicOr(err, ERR_BAD_NODE);
+          return hit;
         }
+        leaf_closest(S, o, d, first, cnt, tmax, hu, hv, hit);
       }
     }
     if (sp == 0) break;
     --sp;
-    word = stk_w[sp]; cnt = stk_c[sp]; wt = stk_t[sp];
+    word = stk_w[sp];
+    wt = stk_t[sp];
   }
   return hit;
 }
 
-// Any hit before max_t (intersect.py:155-219).
+// While-while form with postponed leaves and pop culling.
+template <bool EXACT>
+__device__ __forceinline__ int bvh_closest_wwt(const DevScene& S, float3 o, float3 d, float& tmax, float& hu,
+                                               float& hv, int* err) {
+  int stk_w[kStack];
+  float stk_t[kStack];
+  int sp = 0;
+  stk_w[0] = kSentinel;
+  stk_t[0] = -INFINITY;
+  float3 inv = make_inv_dir(d);
+  float3 oinv = o * inv;
+  int hit = -1;
+  float te;
+  if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
+  int node = 0, leaf = 0;
+  int guard = 4 * S.n_nodes + 64;
+  auto pop = [&]() {
+    int w;
+    float t;
+    do {
+      w = stk_w[sp];
+      t = stk_t[sp];
+      --sp;
+    } while (t > tmax);
+    return w;
+  };
+  while (node != kSentinel) {
+    while ((unsigned)node < (unsigned)kSentinel) {
+      if (--guard < 0 || node >= S.n_nodes) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return hit;
+      }
+      const float4* np = S.nodes + 4 * (size_t)node;
+      float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+      bool hl, hr;
+      float tl, tr;
+      slab2<EXACT>(n0, n1, n2, o, inv, oinv, tmax, hl, hr, tl, tr);
+      int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
+      if (!hl && !hr) {
+        node = pop();
+      } else {
+        bool left_first = hl && (!hr || tl < tr);
+        node = left_first ? lw : rw;
+        if (hl && hr) {
+          if (sp + 1 < kStack) {
+            ++sp;
+            stk_w[sp] = left_first ? rw : lw;
+            stk_t[sp] = left_first ? tr : tl;
+          } else if (err) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+          }
+        }
+      }
+      if (node < 0 && leaf >= 0) {
+        leaf = node;
+        node = pop();
+      }
+      if (!__any_sync(__activemask(), leaf >= 0)) break;
+    }
+    while (leaf < 0) {
+      int first = leaf_first(leaf), cnt = leaf_count(leaf);
+      if (first + cnt > S.n_prims) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return hit;
+      }
+      leaf_closest(S, o, d, first, cnt, tmax, hu, hv, hit);
+      leaf = node;
+      if (node < 0) node = pop();
+    }
+  }
+  return hit;
+}
+
+#ifndef RX_TRAV
+#define RX_TRAV 0
+#endif
+
+template <bool EXACT>
+__device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d, float& tmax, float& hu, float& hv,
+                                           int* err) {
+#if RX_TRAV == 1
+  return bvh_closest_ww<EXACT>(S, o, d, tmax, hu, hv, err);
+#elif RX_TRAV == 2
+  return bvh_closest_wwt<EXACT>(S, o, d, tmax, hu, hv, err);
+#else
+  return bvh_closest_ii<EXACT>(S, o, d, tmax, hu, hv, err);
+#endif
+}
+
+// Any hit before max_t (intersect.py:155-219): stops at the first hit.
 template <bool EXACT>
 __device__ __forceinline__ bool bvh_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
-  int stk_w[kStack];
-  int stk_c[kStack];
+  int stack[kStack];
   int sp = 0;
+  stack[0] = kSentinel;
   float3 inv = make_inv_dir(d);
   float3 oinv = o * inv;
   float te;
   if (S.n_nodes <= 0 || !slab1(S.root_min, S.root_max, o, inv, max_t, te)) return false;
-  int word = 0, cnt = 0;
+  int node = 0;
   int guard = 4 * S.n_nodes + 64;
-  for (;;) {
-    if (--guard < 0) {
+  while (node != kSentinel) {
+    if (--guard < 0 || node >= S.n_nodes) {
       if (err) atomicOr(err, ERR_BAD_NODE);
       return false;
     }
-    if (word >= S.n_nodes || (word < 0 && (~word + cnt > S.n_prims || cnt < 0))) {
-      if (err) atomicOr(err, ERR_BAD_NODE);
-      return false;
-    }
-    if (word >= 0) {
-      const float4* np = S.nodes + 4 * (size_t)word;
+    if (node >= 0) {
+      const float4* np = S.nodes + 4 * (size_t)node;
       float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
       bool hl, hr;
       float tl, tr;
       slab2<EXACT>(n0, n1, n2, o, inv, oinv, max_t, hl, hr, tl, tr);
       int lw = __float_as_int(n3.x), rw = __float_as_int(n3.y);
-      int lc = __float_as_int(n3.z), rc = __float_as_int(n3.w);
-      if (hl && hr) {
-        bool left_first = tl < tr;
-        if (sp < kStack) {
-          stk_w[sp] = left_first ? rw : lw; stk_c[sp] = left_first ? rc : lc; ++sp;
-        } else if (err) {
-          atomicOr(err, ERR_STACK_OVERFLOW);
+      if (hl || hr) {
+        bool left_first = hl && (!hr || tl < tr);
+        node = left_first ? lw : rw;
+        if (hl && hr) {
+          if (sp + 1 < kStack) {
+            stack[++sp] = left_first ? rw : lw;
+          } else if (err) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+          }
         }
-        word = left_first ? lw : rw;
-        cnt = left_first ? lc : rc;
-        continue;
-      } else if (hl) {
-        word = lw; cnt = lc;
-        continue;
-      } else if (hr) {
-        word = rw; cnt = rc;
         continue;
       }
     } else {
-      int first = ~word;
+      int first = leaf_first(node), cnt = leaf_count(node);
+      if (first + cnt > S.n_prims) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return false;
+      }
       for (int k = first; k < first + cnt; ++k) {
         const float4* pp = S.prims + 3 * (size_t)k;
         float4 a = __ldg(pp);
@@ -465,12 +640,11 @@ __device__ __forceinline__ bool bvh_any(const DevScene& S, float3 o, float3 d, f
         }
       }
     }
-    if (sp == 0) break;
-    --sp;
-    word = stk_w[sp]; cnt = stk_c[sp];
+    node = stack[sp--];
   }
   return false;
 }
+
 
 // Hit record from the full scene query (intersect.py:249-309): the linear
 // object slots first, then the BVH, which wins only when strictly closer.

@@ -5,10 +5,11 @@
 // material branches.  Here one wavefront holds `spf` frames x W x H paths
 // whose state lives in structure-of-arrays buffers in HBM; each bounce is
 //
-//   extend  (closest hit for the active queue)        rx_internal.cuh traversal
+//   extend  (closest hit for the active queue, plus any-hit for the shadow
+//            rays the previous bounce emitted, adding unoccluded
+//            contributions)                            rx_internal.cuh traversal
 //   shade   (materials, emission, NEE sample, scatter, Russian roulette;
 //            warp-aggregated pushes into the next queue and the shadow queue)
-//   connect (any-hit for the shadow queue, adds unoccluded contributions)
 //
 // followed by one accumulate pass that applies the sample clamp and folds
 // the frames into the running means exactly as the reference does.  The
@@ -223,16 +224,27 @@ __global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4
 }
 
 template <bool EXACT>
-__global__ void __launch_bounds__(128) k_extend(DevScene S, int b, const int* __restrict__ qin, int* counters,
-                                                const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
-                                                float4* __restrict__ hits, int* err) {
-  const int n = *(volatile int*)&counters[C_Q + b];
+#ifndef RX_EXT_MINB
+#define RX_EXT_MINB 1
+#endif
+__global__ void __launch_bounds__(128, RX_EXT_MINB)
+    k_extend(DevScene S, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
+             const float4* __restrict__ ray_d, float4* __restrict__ hits, int sb, const float4* __restrict__ shadow,
+             float4* __restrict__ rad, long long shadow_cap, int* err) {
+  // Items [0, n): closest hit of bounce b's queue.  Items [n, n + ns): the
+  // shadow rays bounce sb (the previous one) emitted, traced any-hit here so
+  // they share this launch instead of paying for a small one of their own.
+  const int n = b >= 0 ? *(volatile int*)&counters[C_Q + b] : 0;
+  long long ns = sb >= 0 ? *(volatile int*)&counters[C_S + sb] : 0;
+  if (ns > shadow_cap) ns = shadow_cap;
+  const int total = n + (int)ns;
+  int* fetch = &counters[C_FE + (b >= 0 ? b : kMaxBounce - 1)];
   const int lane = threadIdx.x & 31;
   for (;;) {
     int base = 0;
-    if (lane == 0) base = atomicAdd(&counters[C_FE + b], 32);
+    if (lane == 0) base = atomicAdd(fetch, 32);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
+    if (base >= total) break;
     int i = base + lane;
     if (i < n) {
       int p = qin[i];
@@ -240,6 +252,16 @@ __global__ void __launch_bounds__(128) k_extend(DevScene S, int b, const int* __
       SceneHit h = scene_closest<EXACT>(S, xyz(o), xyz(d), err);
       int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
       hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
+    } else if (i < total) {
+      const float4* sp = shadow + 3 * (size_t)(i - n);
+      float4 s0 = sp[0], s1 = sp[1];
+      if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
+        float4 s2 = sp[2];
+        float* r = reinterpret_cast<float*>(rad + __float_as_int(s1.w));
+        atomicAdd(r, s2.x);
+        atomicAdd(r + 1, s2.y);
+        atomicAdd(r + 2, s2.z);
+      }
     }
   }
 }
@@ -485,33 +507,6 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
   }
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(128) k_connect(DevScene S, int b, int* counters, const float4* __restrict__ shadow,
-                                                 float4* __restrict__ rad, long long cap, int* err) {
-  int n = *(volatile int*)&counters[C_S + b];
-  if (n > cap) n = (int)cap;
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&counters[C_FC + b], 32);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    int i = base + lane;
-    if (i < n) {
-      const float4* sp = shadow + 3 * (size_t)i;
-      float4 s0 = sp[0], s1 = sp[1];
-      if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
-        float4 s2 = sp[2];
-        int p = __float_as_int(s1.w);
-        float* r = reinterpret_cast<float*>(rad + p);
-        atomicAdd(r, s2.x);
-        atomicAdd(r + 1, s2.y);
-        atomicAdd(r + 2, s2.z);
-      }
-    }
-  }
-}
-
 // trace.py:262-283: clamp, running mean of radiance and first-hit guides,
 // display = sqrt(min(acc, 1)).  Frames of the wave are folded in order.
 __global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, const float4* __restrict__ rad,
@@ -604,7 +599,7 @@ struct Accum {
   int last_launches = 0;
   // denoise scratch
   DevBuf<float4> dn0, dn1, dn_out;
-  int occ_ext = 0, occ_shade = 0, occ_conn = 0;
+  int occ_ext = 0, occ_shade = 0;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -681,6 +676,18 @@ static int blocks_for(Ctx* ctx, const void* fn, int block) {
   return per_sm * ctx->num_sms;
 }
 
+static void launch_extend(Accum* a, const DevScene& S, const RenderK& K, int b, const int* qin, int sb) {
+  Ctx* ctx = a->ctx;
+  if (S.exact_slab)
+    k_extend<true><<<a->occ_ext, 128, 0, ctx->stream>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p,
+                                                         a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
+                                                         ctx->d_err);
+  else
+    k_extend<false><<<a->occ_ext, 128, 0, ctx->stream>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p,
+                                                          a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
+                                                          ctx->d_err);
+}
+
 // Records the launch sequence of one wave on the context stream.  With
 // `timed`, an event is recorded after every kernel (class in ev_class).
 static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int* n_launch) {
@@ -708,12 +715,9 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   for (int b = 0; b < K.max_depth; ++b) {
     const int* qin = (b & 1) ? a->q1.p : a->q0.p;
     int* qout = (b & 1) ? a->q0.p : a->q1.p;
-    if (S.exact_slab)
-      k_extend<true><<<a->occ_ext, 128, 0, st>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p,
-                                                 ctx->d_err);
-    else
-      k_extend<false><<<a->occ_ext, 128, 0, st>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p,
-                                                  ctx->d_err);
+    // the previous bounce's shadow rays ride along in this extend launch
+    int sb = (b >= 1 && b - 1 < K.dlmd && S.n_lights > 0) ? b - 1 : -1;
+    launch_extend(a, S, K, b, qin, sb);
     ++launches;
     mark(K_EXTEND);
     k_shade<<<a->occ_shade, 128, 0, st>>>(S, K, b, qin, qout, a->counters.p, a->frame_base.p, a->ray_o.p,
@@ -721,16 +725,12 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
                                            a->shadow.p, ctx->d_err);
     ++launches;
     mark(K_SHADE);
-    if (b < K.dlmd && S.n_lights > 0) {
-      if (S.exact_slab)
-        k_connect<true><<<a->occ_conn, 128, 0, st>>>(S, b, a->counters.p, a->shadow.p, a->rad.p, K.shadow_cap,
-                                                     ctx->d_err);
-      else
-        k_connect<false><<<a->occ_conn, 128, 0, st>>>(S, b, a->counters.p, a->shadow.p, a->rad.p, K.shadow_cap,
-                                                      ctx->d_err);
-      ++launches;
-      mark(K_CONNECT);
-    }
+  }
+  if (K.max_depth > 0 && K.max_depth - 1 < K.dlmd && S.n_lights > 0) {
+    // shadow rays of the last bounce: an extend launch with no bounce rays
+    launch_extend(a, S, K, -1, nullptr, K.max_depth - 1);
+    ++launches;
+    mark(K_CONNECT);
   }
   int ablocks = (int)std::min<long long>((K.P + 255) / 256, (long long)ctx->num_sms * 16);
   k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->rad.p, a->gn.p, a->ga.p, a->acc_r.p,
@@ -767,7 +767,6 @@ static int ensure_wave_buffers(Accum* a, long long cap, long long shadow_cap) {
   if (!a->occ_ext) {
     a->occ_ext = blocks_for(ctx, (const void*)k_extend<false>, 128);
     a->occ_shade = blocks_for(ctx, (const void*)k_shade, 128);
-    a->occ_conn = blocks_for(ctx, (const void*)k_connect<false>, 128);
   }
   return RX_OK;
 }
@@ -798,7 +797,7 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
   if (frames == 0) return RX_OK;
   int rc = sc->upload_palette(ctx);
   if (rc) return rc;
-  long long target = p->wave_paths > 0 ? p->wave_paths : (1LL << 22);
+  long long target = p->wave_paths > 0 ? p->wave_paths : (1LL << 23);
   int spf = (int)std::max<long long>(1, std::min<long long>(frames, target / std::max<long long>(a->P, 1)));
   long long cap = (long long)spf * a->P;
   if (cap >= (1LL << 31)) return set_error(ctx, "render: wavefront of %lld paths is too large", cap), RX_ERR_CAPACITY;
@@ -857,7 +856,8 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
       CUDA_TRY(ctx, cudaStreamSynchronize(st));
       // events: start, after generate, after each bounce kernel, after accumulate
       int ne = 2;
-      for (int b = 0; b < p->max_depth; ++b) ne += (b < p->direct_light_max_depth && nl > 0) ? 3 : 2;
+      ne += 2 * p->max_depth;
+      if (p->max_depth > 0 && p->max_depth - 1 < p->direct_light_max_depth && nl > 0) ne += 1;
       ne += 1;
       for (int i = 1; i < ne; ++i) {
         float ms = 0.0f;

@@ -12,7 +12,8 @@ import threading
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libroxy_cuda.so")
+# ROXY_CUDA_LIB selects another build of the library (e.g. an installed copy)
+LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
 SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]

@@ -120,7 +120,8 @@ def _check_layout(nodes, order, n_prims, pmin, pmax):
             if w >= 0:
                 stack.append(w)
                 continue
-            first = ~w
+            first, packed_count = (~w) >> 5, (~w) & 31
+            assert packed_count == c
             for k in range(first, first + c):
                 p = order[k]
                 seen[p] += 1

@@ -32,6 +32,8 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# paths per wavefront when rx_render_params.wave_paths is 0 (rx_render.cu)
+WAVE_PATHS = 1 << 25
 sys.path[:0] = [os.path.join(ROOT, "roxy-dcc_b200"), ROOT]
 
 import numpy as np  # noqa: E402
@@ -283,7 +285,7 @@ def run_ours(args):
     # per launch here (max_depth launches per wave)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_extend.json")
-    spf = max(1, min(w["spp"], (1 << 22) // (W * H)))
+    spf = max(1, min(w["spp"], WAVE_PATHS // (W * H)))
     ext_launches = w["max_depth"] * -(-w["spp"] // spf)
     if os.path.exists(tfile):
         try:

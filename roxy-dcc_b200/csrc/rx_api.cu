@@ -83,7 +83,7 @@ using namespace rx;
 // SAH costs of one node traversal step and one primitive test, used to decide
 // which LBVH subtrees collapse into leaves.
 #ifndef RX_SAH_CT
-#define RX_SAH_CT 1.2f
+#define RX_SAH_CT 0.6f
 #endif
 #ifndef RX_SAH_CI
 #define RX_SAH_CI 1.0f

@@ -307,9 +307,7 @@ def run_ours(args):
         ctx.sync()
         e2e_times.append(time.perf_counter() - t0)
         e2e_rays.append(r.last_ray_count)
-    b = r._scene.builder._batch
-    h2d = int(sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + b.triangle_count * 4 +
-              len(r._scene.slots) * 96)
+    h2d = int(r._scene.h2d_bytes + len(r._scene.slots) * 96)
     d2h = W * H * 3 * 4
     e2e_val = sum(e2e_rays) / sum(e2e_times) / 1e6
     if dist:

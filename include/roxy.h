@@ -91,6 +91,33 @@ int rx_scene_destroy(rx_scene* scene);
  * (TriangleBatch, bvh_builder.py:8-272). */
 int rx_scene_set_triangles(rx_scene* scene, int n, const float* v0, const float* v1, const float* v2,
                            const float* n0, const float* n1, const float* n2, const int* mat_idx);
+/* Scene extraction on the device: the triangle arrays are sized once, then
+ * filled piecewise.  Replaces the host flattening of
+ * rendering/taichi/extractor.py:60-96 (Mesh triangles and
+ * IndexedMesh.indexed_triangle_arrays, scene/mesh.py:397-430) followed by the
+ * field upload of bvh_builder.py:560-655.
+ *   rx_scene_alloc_triangles  n rows, zero-filled; drops any BVH.
+ *   rx_scene_put_triangles    rows [offset, offset+n) from host float32 rows
+ *                             (n0..n2 NULL -> copies of v0; mat_idx NULL -> 0).
+ *   rx_scene_put_indexed      rows [offset, offset+n_tris) from an indexed mesh:
+ *                             positions (n_pos,3) float64, tri_pos_idx (n_tris,3),
+ *                             normals (n_nrm,3) float64 + tri_nrm_idx (n_tris,3)
+ *                             or NULL (a row with an index < 0 takes the face
+ *                             normal), matrix: 16 float64 row-major world matrix
+ *                             or NULL, normal_matrix: 16 float64 row-major
+ *                             inverse transpose or NULL, tri_group_idx (n_tris,)
+ *                             or NULL, group_mat (n_groups,) palette index of each
+ *                             group.  Out-of-range indices -> RX_ERR_ARG.
+ *   rx_scene_get_triangles    copies rows back (any output may be NULL). */
+int rx_scene_alloc_triangles(rx_scene* scene, int n);
+int rx_scene_put_triangles(rx_scene* scene, int offset, int n, const float* v0, const float* v1, const float* v2,
+                           const float* n0, const float* n1, const float* n2, const int* mat_idx);
+int rx_scene_put_indexed(rx_scene* scene, int offset, int n_tris, int n_pos, const double* positions,
+                         const int* tri_pos_idx, int n_nrm, const double* normals, const int* tri_nrm_idx,
+                         const double* matrix, const double* normal_matrix, const int* tri_group_idx,
+                         int n_groups, const int* group_mat);
+int rx_scene_get_triangles(rx_scene* scene, int offset, int n, float* v0, float* v1, float* v2, float* n0,
+                           float* n1, float* n2, int* mat_idx);
 /* Material palette (fields.py:73-78). */
 int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float* albedo,
                            const float* roughness, const float* ior, const float* emission);

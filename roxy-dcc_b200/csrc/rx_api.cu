@@ -208,6 +208,53 @@ int rx_scene_set_triangles(rx_scene* scene, int n, const float* v0, const float*
   return RX_OK;
 }
 
+int rx_scene_alloc_triangles(rx_scene* scene, int n) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  if (n < 0) return set_error(c, "alloc_triangles: negative count"), RX_ERR_ARG;
+  if (n >= (1 << 30)) return set_error(c, "alloc_triangles: %d triangles exceed the limit", n), RX_ERR_CAPACITY;
+  return scene_alloc_triangles(c, &s, n);
+}
+
+int rx_scene_put_triangles(rx_scene* scene, int offset, int n, const float* v0, const float* v1, const float* v2,
+                           const float* n0, const float* n1, const float* n2, const int* mat_idx) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  if (n > 0 && (!v0 || !v1 || !v2)) return set_error(c, "put_triangles: bad arguments"), RX_ERR_ARG;
+  const float* rows[6] = {v0, v1, v2, n0, n1, n2};
+  return scene_put_triangles(c, &s, offset, n, rows, mat_idx);
+}
+
+int rx_scene_put_indexed(rx_scene* scene, int offset, int n_tris, int n_pos, const double* positions,
+                         const int* tri_pos_idx, int n_nrm, const double* normals, const int* tri_nrm_idx,
+                         const double* matrix, const double* normal_matrix, const int* tri_group_idx, int n_groups,
+                         const int* group_mat) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  return scene_put_indexed(c, &s, offset, n_tris, n_pos, positions, tri_pos_idx, n_nrm, normals, tri_nrm_idx, matrix,
+                           normal_matrix, tri_group_idx, n_groups, group_mat);
+}
+
+int rx_scene_get_triangles(rx_scene* scene, int offset, int n, float* v0, float* v1, float* v2, float* n0, float* n1,
+                           float* n2, int* mat_idx) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  float* rows[6] = {v0, v1, v2, n0, n1, n2};
+  return scene_get_triangles(c, &s, offset, n, rows, mat_idx);
+}
+
 int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float* albedo, const float* roughness,
                            const float* ior, const float* emission) {
   if (!scene) return RX_ERR_ARG;

@@ -1,0 +1,262 @@
+// Scene extraction on the device.
+//
+// The reference flattens an IndexedMesh on the host before every render
+// (scene/mesh.py:397-430 indexed_triangle_arrays, called from
+// rendering/taichi/extractor.py:60-96): gather the three positions of each
+// triangle, transform them by the object's world matrix in float64, take the
+// vertex normals (or the normalised face normal of the untransformed
+// triangle), transform them by the inverse-transpose matrix, normalise, and
+// round everything to float32.  Here the caller uploads the mesh's own arrays
+// (positions, index tables, per-group palette index) and one thread per
+// triangle writes the float32 rows straight into the scene's triangle arrays.
+//
+// Arithmetic follows numpy's element-wise float64 order: a point row is
+// ((x*m0 + y*m1) + z*m2) + m3, the length of a row is sqrt((x*x + y*y) + z*z)
+// (np.linalg.norm along axis 1 sums left to right), numpy's cross product
+// takes a1*b2 - a2*b1 etc., and the library is compiled without FMA
+// contraction.  The reference multiplies by the matrix through BLAS, whose
+// float64 results may differ from this order in the last bit; after the
+// rounding to float32 the rows agree except when a float64 value lies within
+// one float64 ulp of a float32 rounding boundary.
+#include <vector>
+
+#include "rx_internal.cuh"
+#include "rx_runtime.h"
+
+namespace rx {
+
+struct IndexedArgs {
+  int n_tris, n_pos, n_nrm, n_groups;
+  const double* pos;      // (n_pos, 3)
+  const int* tri_pos;     // (n_tris, 3)
+  const double* nrm;      // (n_nrm, 3) or null
+  const int* tri_nrm;     // (n_tris, 3) or null; a row with any index < 0 uses the face normal
+  const int* tri_group;   // (n_tris,) or null (group 0)
+  const int* group_mat;   // (n_groups,) palette index of each group
+  double m[12];           // rows 0..2 of the world matrix
+  double mw[4];           // row 3 (projective divide when |w| > 1e-12)
+  double nm[9];           // rows 0..2, columns 0..2 of the normal matrix
+  int has_m, has_nm;
+  float *v0, *v1, *v2, *n0, *n1, *n2;  // destination rows, already offset
+  int* mat;
+  int* err;               // bit 1: position index, 2: normal index, 4: group index out of range
+};
+
+struct D3 {
+  double x, y, z;
+};
+
+__device__ __forceinline__ D3 ldd3(const double* p, long i) { return D3{p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+
+__device__ __forceinline__ D3 xform_point(const IndexedArgs& A, D3 p) {
+  if (!A.has_m) return p;
+  const double* m = A.m;
+  D3 r;
+  r.x = ((p.x * m[0] + p.y * m[1]) + p.z * m[2]) + m[3];
+  r.y = ((p.x * m[4] + p.y * m[5]) + p.z * m[6]) + m[7];
+  r.z = ((p.x * m[8] + p.y * m[9]) + p.z * m[10]) + m[11];
+  double w = ((p.x * A.mw[0] + p.y * A.mw[1]) + p.z * A.mw[2]) + A.mw[3];
+  if (fabs(w) > 1e-12) {
+    r.x = r.x / w;
+    r.y = r.y / w;
+    r.z = r.z / w;
+  }
+  return r;
+}
+
+__device__ __forceinline__ D3 xform_vector(const IndexedArgs& A, D3 v) {
+  if (!A.has_nm) return v;
+  const double* m = A.nm;
+  return D3{(v.x * m[0] + v.y * m[1]) + v.z * m[2], (v.x * m[3] + v.y * m[4]) + v.z * m[5],
+            (v.x * m[6] + v.y * m[7]) + v.z * m[8]};
+}
+
+__device__ __forceinline__ D3 normalize_row(D3 v) {
+  double len = sqrt((v.x * v.x + v.y * v.y) + v.z * v.z);
+  if (len > 1e-12) return D3{v.x / len, v.y / len, v.z / len};
+  return v;
+}
+
+__device__ __forceinline__ void st3(float* p, long i, D3 v) {
+  p[3 * i] = (float)v.x;
+  p[3 * i + 1] = (float)v.y;
+  p[3 * i + 2] = (float)v.z;
+}
+
+__global__ void __launch_bounds__(256) k_extract_indexed(IndexedArgs A) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < A.n_tris; t += (long)gridDim.x * blockDim.x) {
+    int i0 = __ldg(A.tri_pos + 3 * t), i1 = __ldg(A.tri_pos + 3 * t + 1), i2 = __ldg(A.tri_pos + 3 * t + 2);
+    int bad = 0;
+    if ((unsigned)i0 >= (unsigned)A.n_pos || (unsigned)i1 >= (unsigned)A.n_pos || (unsigned)i2 >= (unsigned)A.n_pos) {
+      bad |= 1;
+      i0 = i1 = i2 = 0;
+    }
+    D3 p0 = ldd3(A.pos, i0), p1 = ldd3(A.pos, i1), p2 = ldd3(A.pos, i2);
+    st3(A.v0, t, xform_point(A, p0));
+    st3(A.v1, t, xform_point(A, p1));
+    st3(A.v2, t, xform_point(A, p2));
+
+    D3 q0, q1, q2;
+    int j0 = -1, j1 = -1, j2 = -1;
+    if (A.nrm && A.tri_nrm) {
+      j0 = __ldg(A.tri_nrm + 3 * t);
+      j1 = __ldg(A.tri_nrm + 3 * t + 1);
+      j2 = __ldg(A.tri_nrm + 3 * t + 2);
+    }
+    if (j0 >= 0 && j1 >= 0 && j2 >= 0) {
+      if (j0 >= A.n_nrm || j1 >= A.n_nrm || j2 >= A.n_nrm) {
+        bad |= 2;
+        j0 = j1 = j2 = 0;
+      }
+      q0 = ldd3(A.nrm, j0);
+      q1 = ldd3(A.nrm, j1);
+      q2 = ldd3(A.nrm, j2);
+    } else {
+      D3 a{p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
+      D3 b{p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
+      D3 c{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+      q0 = q1 = q2 = normalize_row(c);
+    }
+    st3(A.n0, t, normalize_row(xform_vector(A, q0)));
+    st3(A.n1, t, normalize_row(xform_vector(A, q1)));
+    st3(A.n2, t, normalize_row(xform_vector(A, q2)));
+
+    int g = A.tri_group ? __ldg(A.tri_group + t) : 0;
+    if ((unsigned)g >= (unsigned)A.n_groups) {
+      bad |= 4;
+      g = 0;
+    }
+    A.mat[t] = __ldg(A.group_mat + g);
+    if (bad) atomicOr(A.err, bad);
+  }
+}
+
+template <class T>
+static int upload_tmp(Ctx* c, DevBuf<T>& b, const T* host, size_t n) {
+  if (!b.alloc(c, n ? n : 1)) return set_error(c, "out of device memory (%zu elements)", n), RX_ERR_CAPACITY;
+  if (n && host) CUDA_TRY(c, cudaMemcpyAsync(b.p, host, sizeof(T) * n, cudaMemcpyHostToDevice, c->stream));
+  return RX_OK;
+}
+
+int scene_alloc_triangles(Ctx* c, Scene* s, int n) {
+  size_t k = (size_t)3 * std::max(n, 1);
+  if (!s->v0b.alloc(c, k) || !s->v1b.alloc(c, k) || !s->v2b.alloc(c, k) || !s->n0b.alloc(c, k) ||
+      !s->n1b.alloc(c, k) || !s->n2b.alloc(c, k) || !s->tri_matb.alloc(c, std::max(n, 1)))
+    return set_error(c, "alloc_triangles: out of device memory for %d triangles", n), RX_ERR_CAPACITY;
+  // rows not written by a put call stay zero (degenerate, never hit)
+  for (DevBuf<float>* b : {&s->v0b, &s->v1b, &s->v2b, &s->n0b, &s->n1b, &s->n2b})
+    CUDA_TRY(c, cudaMemsetAsync(b->p, 0, b->bytes(), c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(s->tri_matb.p, 0, s->tri_matb.bytes(), c->stream));
+  s->d_v0 = s->v0b.p; s->d_v1 = s->v1b.p; s->d_v2 = s->v2b.p;
+  s->d_n0 = s->n0b.p; s->d_n1 = s->n1b.p; s->d_n2 = s->n2b.p;
+  s->d_tri_mat = s->tri_matb.p;
+  s->n_tris = n;
+  s->clear_bvh();
+  return RX_OK;
+}
+
+int scene_put_triangles(Ctx* c, Scene* s, int offset, int n, const float* const* rows, const int* mat_idx) {
+  if (offset < 0 || n < 0 || (long long)offset + n > s->n_tris)
+    return set_error(c, "put_triangles: rows [%d, %d) outside the %d allocated", offset, offset + n, s->n_tris),
+           RX_ERR_ARG;
+  if (n == 0) return RX_OK;
+  float* dst[6] = {s->d_v0, s->d_v1, s->d_v2, s->d_n0, s->d_n1, s->d_n2};
+  for (int k = 0; k < 6; ++k) {
+    const float* src = rows[k] ? rows[k] : rows[0];
+    CUDA_TRY(c, cudaMemcpyAsync(dst[k] + (size_t)3 * offset, src, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
+                                c->stream));
+  }
+  if (mat_idx)
+    CUDA_TRY(c, cudaMemcpyAsync(s->d_tri_mat + offset, mat_idx, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+  else
+    CUDA_TRY(c, cudaMemsetAsync(s->d_tri_mat + offset, 0, sizeof(int) * n, c->stream));
+  ++s->version;
+  return RX_OK;
+}
+
+int scene_put_indexed(Ctx* c, Scene* s, int offset, int n_tris, int n_pos, const double* positions,
+                      const int* tri_pos_idx, int n_nrm, const double* normals, const int* tri_nrm_idx,
+                      const double* matrix, const double* normal_matrix, const int* tri_group_idx, int n_groups,
+                      const int* group_mat) {
+  if (offset < 0 || n_tris < 0 || (long long)offset + n_tris > s->n_tris)
+    return set_error(c, "put_indexed: rows [%d, %d) outside the %d allocated", offset, offset + n_tris, s->n_tris),
+           RX_ERR_ARG;
+  if (n_pos < 0 || n_nrm < 0 || n_groups < 1 || !group_mat || (n_tris > 0 && (!positions || !tri_pos_idx)))
+    return set_error(c, "put_indexed: bad arguments"), RX_ERR_ARG;
+  if (n_tris == 0) return RX_OK;
+  IndexedArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.n_tris = n_tris;
+  A.n_pos = n_pos;
+  A.n_nrm = (normals && tri_nrm_idx) ? n_nrm : 0;
+  A.n_groups = n_groups;
+  if (matrix) {
+    for (int i = 0; i < 12; ++i) A.m[i] = matrix[i];
+    for (int i = 0; i < 4; ++i) A.mw[i] = matrix[12 + i];
+    A.has_m = 1;
+  }
+  if (normal_matrix) {
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < 3; ++k) A.nm[3 * r + k] = normal_matrix[4 * r + k];
+    A.has_nm = 1;
+  }
+  DevBuf<double> d_pos, d_nrm;
+  DevBuf<int> d_tri_pos, d_tri_nrm, d_group, d_group_mat, d_err;
+  int rc;
+  if ((rc = upload_tmp(c, d_pos, positions, (size_t)3 * n_pos)) ||
+      (rc = upload_tmp(c, d_tri_pos, tri_pos_idx, (size_t)3 * n_tris)) ||
+      (rc = upload_tmp(c, d_group_mat, group_mat, (size_t)n_groups)) || (rc = upload_tmp(c, d_err, (int*)nullptr, 1)))
+    return rc;
+  if (A.n_nrm > 0) {
+    if ((rc = upload_tmp(c, d_nrm, normals, (size_t)3 * n_nrm)) ||
+        (rc = upload_tmp(c, d_tri_nrm, tri_nrm_idx, (size_t)3 * n_tris)))
+      return rc;
+    A.nrm = d_nrm.p;
+    A.tri_nrm = d_tri_nrm.p;
+  }
+  if (tri_group_idx) {
+    if ((rc = upload_tmp(c, d_group, tri_group_idx, (size_t)n_tris))) return rc;
+    A.tri_group = d_group.p;
+  }
+  A.pos = d_pos.p;
+  A.tri_pos = d_tri_pos.p;
+  A.group_mat = d_group_mat.p;
+  A.v0 = s->d_v0 + (size_t)3 * offset;
+  A.v1 = s->d_v1 + (size_t)3 * offset;
+  A.v2 = s->d_v2 + (size_t)3 * offset;
+  A.n0 = s->d_n0 + (size_t)3 * offset;
+  A.n1 = s->d_n1 + (size_t)3 * offset;
+  A.n2 = s->d_n2 + (size_t)3 * offset;
+  A.mat = s->d_tri_mat + offset;
+  A.err = d_err.p;
+  CUDA_TRY(c, cudaMemsetAsync(d_err.p, 0, sizeof(int), c->stream));
+  int blocks = (int)std::min<long long>((n_tris + 255) / 256, (long long)c->num_sms * 8);
+  k_extract_indexed<<<blocks, 256, 0, c->stream>>>(A);
+  CUDA_TRY(c, cudaGetLastError());
+  int herr = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&herr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  ++s->version;
+  if (herr & 1) return set_error(c, "put_indexed: a position index is outside [0, %d)", n_pos), RX_ERR_ARG;
+  if (herr & 2) return set_error(c, "put_indexed: a normal index is outside [0, %d)", n_nrm), RX_ERR_ARG;
+  if (herr & 4) return set_error(c, "put_indexed: a group index is outside [0, %d)", n_groups), RX_ERR_ARG;
+  return RX_OK;
+}
+
+int scene_get_triangles(Ctx* c, Scene* s, int offset, int n, float* const* rows, int* mat_idx) {
+  if (offset < 0 || n < 0 || (long long)offset + n > s->n_tris)
+    return set_error(c, "get_triangles: rows [%d, %d) outside the %d present", offset, offset + n, s->n_tris),
+           RX_ERR_ARG;
+  if (n == 0) return RX_OK;
+  const float* src[6] = {s->d_v0, s->d_v1, s->d_v2, s->d_n0, s->d_n1, s->d_n2};
+  for (int k = 0; k < 6; ++k)
+    if (rows[k])
+      CUDA_TRY(c, cudaMemcpyAsync(rows[k], src[k] + (size_t)3 * offset, sizeof(float) * 3 * n,
+                                  cudaMemcpyDeviceToHost, c->stream));
+  if (mat_idx)
+    CUDA_TRY(c, cudaMemcpyAsync(mat_idx, s->d_tri_mat + offset, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return RX_OK;
+}
+
+}  // namespace rx

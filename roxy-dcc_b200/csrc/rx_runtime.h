@@ -162,6 +162,15 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
 int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min, const float* node_max,
                         const int* left, const int* right, const int* start, const int* count, const int* order);
 
+// scene extraction on the device (rx_extract.cu); rows[] = v0, v1, v2, n0, n1, n2
+int scene_alloc_triangles(Ctx* c, Scene* s, int n);
+int scene_put_triangles(Ctx* c, Scene* s, int offset, int n, const float* const* rows, const int* mat_idx);
+int scene_put_indexed(Ctx* c, Scene* s, int offset, int n_tris, int n_pos, const double* positions,
+                      const int* tri_pos_idx, int n_nrm, const double* normals, const int* tri_nrm_idx,
+                      const double* matrix, const double* normal_matrix, const int* tri_group_idx, int n_groups,
+                      const int* group_mat);
+int scene_get_triangles(Ctx* c, Scene* s, int offset, int n, float* const* rows, int* mat_idx);
+
 // traversal entry points (rx_trace.cu)
 int trace_closest(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_rd, float* d_t, int* d_id,
                   float* d_u, float* d_v);

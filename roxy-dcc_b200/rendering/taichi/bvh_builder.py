@@ -106,6 +106,14 @@ class TriangleBatch:
                    uv1=col("uv1", [0.0, 0.0]), uv2=col("uv2", [0.0, 0.0]), has_uv=col("has_uv", 0),
                    texture_idx=col("texture_idx", -1))
 
+    @staticmethod
+    def palette_record(m):
+        """Palette entry of a material record, its values rounded to float32
+        as the palette arrays store them."""
+        return {"type": int(m["mat_type"]), "albedo": np.asarray(m["albedo"], np.float32).tolist(),
+                "roughness": float(np.float32(m["roughness"])), "ior": float(np.float32(m["ior"])),
+                "emission": float(np.float32(m["emission"])), "texture_idx": int(m.get("texture_idx", -1))}
+
     @classmethod
     def from_indexed_arrays(cls, arrays, material_by_group_idx):
         gidx = np.asarray(arrays["group_idx"], dtype=np.int32)
@@ -116,11 +124,7 @@ class TriangleBatch:
             local = remap[gidx]
         else:
             local = gidx
-        recs = [material_by_group_idx[int(g)] for g in used]
-        palette = [{"type": int(m["mat_type"]), "albedo": np.asarray(m["albedo"], np.float32).tolist(),
-                    "roughness": float(np.float32(m["roughness"])), "ior": float(np.float32(m["ior"])),
-                    "emission": float(np.float32(m["emission"])), "texture_idx": int(m.get("texture_idx", -1))}
-                   for m in recs]
+        palette = [cls.palette_record(material_by_group_idx[int(g)]) for g in used]
         k = len(palette)
         return cls(arrays["v0"], arrays["v1"], arrays["v2"], arrays["n0"], arrays["n1"], arrays["n2"],
                    np.array([p["type"] for p in palette], np.int32).reshape(k),

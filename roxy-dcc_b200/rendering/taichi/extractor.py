@@ -92,12 +92,12 @@ def _mesh_batch(obj, shape, mesh):
                          texture_idx=np.full(k, -1, np.int32), mat_idx=mat_idx)
 
 
-def collect(world):
-    """(triangle batches, object slots) of every renderable object.  IndexedMesh
-    batches come first in visit order and Mesh triangles after them, the
-    order extract_scene gives the reference's builder."""
+def _walk(world):
+    """Renderable geometry in visit order: (object, shape, IndexedMesh)
+    triples, (object, shape, Mesh) triples and the object-slot dicts of
+    analytic primitives."""
     from scene.mesh import IndexedMesh, Mesh
-    slots, batches, mesh_batches = [], [], []
+    indexed, meshes, slots = [], [], []
 
     def visit(obj):
         if not obj.renderable:
@@ -105,13 +105,9 @@ def collect(world):
         for shape in obj.shapes:
             geo = shape.geometry
             if isinstance(geo, Mesh):
-                b = _mesh_batch(obj, shape, geo)
-                if b is not None:
-                    mesh_batches.append(b)
+                meshes.append((obj, shape, geo))
             elif isinstance(geo, IndexedMesh):
-                arrays = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
-                mats = {gi: _mat_record(shape.material_for_group(g)) for gi, g in enumerate(arrays["groups"])}
-                batches.append(TriangleBatch.from_indexed_arrays(arrays, mats))
+                indexed.append((obj, shape, geo))
             else:
                 exported = obj.taichi_export()
                 if isinstance(exported, list):
@@ -124,6 +120,20 @@ def collect(world):
 
     for o in world.objects:
         visit(o)
+    return indexed, meshes, slots
+
+
+def collect(world):
+    """(triangle batches, object slots) of every renderable object.  IndexedMesh
+    batches come first in visit order and Mesh triangles after them, the
+    order extract_scene gives the reference's builder."""
+    indexed, meshes, slots = _walk(world)
+    batches = []
+    for obj, shape, geo in indexed:
+        arrays = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+        mats = {gi: _mat_record(shape.material_for_group(g)) for gi, g in enumerate(arrays["groups"])}
+        batches.append(TriangleBatch.from_indexed_arrays(arrays, mats))
+    mesh_batches = [b for b in (_mesh_batch(o, s, g) for o, s, g in meshes) if b is not None]
     return batches + mesh_batches, slots
 
 
@@ -149,17 +159,29 @@ def slot_arrays(slots):
 
 class DeviceScene:
     """Everything the renderer needs for one world: the native scene (with its
-    BVH), object slots and both light lists."""
+    BVH), object slots and both light lists.
 
-    def __init__(self, builder, slots, stats):
-        self.builder = builder
-        self.native = builder.native
+    light_args: (v0, v1, v2, palette index) of at least every emissive
+    triangle, in scene order, followed by the palette's type, albedo and
+    emission arrays.  h2d_bytes: bytes copied host -> device for the
+    geometry."""
+
+    def __init__(self, native, slots, stats, light_args, builder=None, h2d_bytes=0):
+        self.native = native
         self.slots = slots
         self.stats = stats
+        self.builder = builder
+        self.h2d_bytes = int(h2d_bytes)
+        self._light_args = light_args
         self._lights_mode = None
+
+    @classmethod
+    def from_builder(cls, builder, slots, stats):
         b = builder._batch
         pal = builder.palette_arrays()
-        self._light_args = (b.v0, b.v1, b.v2, builder._source_mat_idx, pal[0], pal[1], pal[4])
+        h2d = sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + 4 * b.triangle_count
+        return cls(builder.native, slots, stats, (b.v0, b.v1, b.v2, builder._source_mat_idx, pal[0], pal[1], pal[4]),
+                   builder=builder, h2d_bytes=h2d)
 
     def use_lights(self, compat):
         compat = bool(compat)
@@ -190,20 +212,116 @@ class HostScene:
                             self.palette[4], compat=compat)
 
 
+def _indexed_world_positions(geo, matrix, sel):
+    """float32 world-space corners (len(sel), 3, 3) of triangles `sel` of an
+    IndexedMesh, in the element-wise float64 order of k_extract_indexed."""
+    p = geo._positions[geo._tri_pos_idx[sel]]
+    if matrix is None:
+        return p.astype(np.float32)
+    r = np.asarray(matrix.rows, dtype=np.float64)
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    out = np.stack([((x * r[i, 0] + y * r[i, 1]) + z * r[i, 2]) + r[i, 3] for i in range(3)], axis=-1)
+    w = ((x * r[3, 0] + y * r[3, 1]) + z * r[3, 2]) + r[3, 3]
+    div = np.abs(w) > 1e-12
+    out[div] = out[div] / w[div][:, None]
+    return out.astype(np.float32)
+
+
+def _emissive(builder, palette_idx):
+    m = builder.mat_palette[int(palette_idx)]
+    return m["type"] == 3 and m["emission"] > 0.0
+
+
+def _extract_on_device(world, native, builder):
+    """Fill `native`'s triangle arrays with the world's triangles in the order
+    and palette of collect() + GPUBVHBuilder.build, transforming IndexedMesh
+    geometry on the device (rx_scene_put_indexed).  Returns (slots, triangle
+    count, emissive triangle rows, host->device bytes)."""
+    indexed, meshes, slots = _walk(world)
+    mesh_batches = [b for b in (_mesh_batch(o, s, g) for o, s, g in meshes) if b is not None]
+    total = sum(g.triangle_count for _, _, g in indexed) + sum(b.triangle_count for b in mesh_batches)
+    native.alloc_triangles(total)
+    lv0, lv1, lv2, lmat = [], [], [], []
+    off, h2d = 0, 0
+    for obj, shape, geo in indexed:
+        n = geo.triangle_count
+        if n == 0:
+            continue
+        groups = geo.groups
+        gidx = geo._tri_group_idx
+        if gidx.min() < 0 or gidx.max() >= len(groups):
+            raise ValueError("IndexedMesh group index outside its group list")
+        used = np.nonzero(np.bincount(gidx, minlength=len(groups)))[0]
+        group_mat = np.zeros(len(groups), np.int32)
+        for g in used:
+            rec = TriangleBatch.palette_record(_mat_record(shape.material_for_group(groups[g])))
+            group_mat[g] = builder._add_material(rec)
+        has_n = geo._normals is not None
+        native.put_indexed(off, geo._positions, geo._tri_pos_idx, geo._normals if has_n else None,
+                           geo._tri_normal_idx if has_n else None, obj.world_matrix.rows,
+                           obj.world_inverse_transpose_matrix.rows, gidx, group_mat)
+        h2d += geo._positions.nbytes + geo._tri_pos_idx.nbytes + gidx.nbytes + group_mat.nbytes
+        if has_n:
+            h2d += geo._normals.nbytes + geo._tri_normal_idx.nbytes
+        em = [g for g in used if _emissive(builder, group_mat[g])]
+        if em:
+            sel = np.nonzero(np.isin(gidx, em))[0]
+            w = _indexed_world_positions(geo, obj.world_matrix, sel)
+            lv0.append(w[:, 0])
+            lv1.append(w[:, 1])
+            lv2.append(w[:, 2])
+            lmat.append(group_mat[gidx[sel]])
+        off += n
+    for b in mesh_batches:
+        remap = np.array([builder._add_material(m) for m in b.mat_palette], np.int32)
+        mat = remap[b.mat_idx]
+        native.put_triangles(off, b.v0, b.v1, b.v2, b.n0, b.n1, b.n2, mat)
+        h2d += sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + mat.nbytes
+        sel = np.nonzero([_emissive(builder, k) for k in remap])[0]
+        if len(sel):
+            rows = np.nonzero(np.isin(b.mat_idx, sel))[0]
+            lv0.append(b.v0[rows])
+            lv1.append(b.v1[rows])
+            lv2.append(b.v2[rows])
+            lmat.append(mat[rows])
+        off += b.triangle_count
+    cat3 = lambda xs: np.concatenate(xs) if xs else np.zeros((0, 3), np.float32)  # noqa: E731
+    lights = (cat3(lv0), cat3(lv1), cat3(lv2), np.concatenate(lmat) if lmat else np.zeros(0, np.int32))
+    return slots, total, lights, h2d
+
+
 def build_device_scene(world, method="lbvh", leaf_size=None):
-    batches, slots = collect(world)
-    builder = GPUBVHBuilder()
-    if leaf_size is not None:
-        builder.MAX_LEAF_SIZE = leaf_size
-    elif method == "lbvh":
-        builder.MAX_LEAF_SIZE = 4
+    """Extract `world` to a device scene with a BVH.  method "lbvh" (the
+    renderer's) transforms IndexedMesh geometry on the device; "morton" and
+    "median" go through GPUBVHBuilder's host flattening so that the
+    reference-format tree and ordered arrays stay available."""
+    if method != "lbvh":
+        batches, slots = collect(world)
+        builder = GPUBVHBuilder()
+        if leaf_size is not None:
+            builder.MAX_LEAF_SIZE = leaf_size
+        native = nat.NativeScene()
+        native.set_objects(slot_arrays(slots) if slots else None)
+        builder.build(batches, method=method, native=native)
+        stats = {"primitive_count": len(slots), "bvh_nodes": len(builder.nodes),
+                 "bvh_triangles": builder.triangle_count,
+                 "bvh_materials": len(builder.mat_palette) if batches else 0,
+                 "bvh_leaf_size": builder.MAX_LEAF_SIZE if builder.triangle_count else 0}
+        return DeviceScene.from_builder(builder, slots, stats)
+    leaf = 4 if leaf_size is None else int(leaf_size)
     native = nat.NativeScene()
+    builder = GPUBVHBuilder()  # palette bookkeeping only
+    slots, total, light_tris, h2d = _extract_on_device(world, native, builder)
     native.set_objects(slot_arrays(slots) if slots else None)
-    builder.build(batches, method=method, native=native)
-    stats = {"primitive_count": len(slots), "bvh_nodes": len(builder.nodes),
-             "bvh_triangles": builder.triangle_count, "bvh_materials": len(builder.mat_palette) if batches else 0,
-             "bvh_leaf_size": builder.MAX_LEAF_SIZE if builder.triangle_count else 0}
-    return DeviceScene(builder, slots, stats)
+    pal = builder.palette_arrays()
+    native.set_materials(*pal)
+    n_nodes = 0
+    if total:
+        native.build_bvh(nat.RX_BVH_LBVH_SAH, min(leaf, 15), True)
+        n_nodes = native.bvh_info()["n_nodes"]
+    stats = {"primitive_count": len(slots), "bvh_nodes": n_nodes, "bvh_triangles": total,
+             "bvh_materials": len(builder.mat_palette), "bvh_leaf_size": leaf if total else 0}
+    return DeviceScene(native, slots, stats, light_tris + (pal[0], pal[1], pal[4]), h2d_bytes=h2d)
 
 
 def extract_scene(world, method="lbvh"):

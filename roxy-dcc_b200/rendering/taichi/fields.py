@@ -25,7 +25,7 @@ def bind_builder(builder):
     from rendering.taichi.extractor import DeviceScene
     stats = {"primitive_count": 0, "bvh_nodes": len(builder.nodes), "bvh_triangles": builder.triangle_count,
              "bvh_materials": len(builder.mat_palette), "bvh_leaf_size": builder.MAX_LEAF_SIZE}
-    _state["scene"] = DeviceScene(builder, [], stats)
+    _state["scene"] = DeviceScene.from_builder(builder, [], stats)
 
 
 def current_scene():

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # ROXY_CUDA_LIB selects another build of the library (e.g. an installed copy)
 LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
-SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu"]
+SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
 
 RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE = range(6)
@@ -24,6 +24,7 @@ RX_ACC_RADIANCE, RX_ACC_NORMAL, RX_ACC_ALBEDO, RX_ACC_DEPTH, RX_ACC_DISPLAY = ra
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
 
 
 class NativeUnavailable(RuntimeError):
@@ -89,6 +90,11 @@ _SIGS = {
     "rx_scene_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "rx_scene_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "rx_scene_set_triangles": ([ctypes.c_void_p, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
+    "rx_scene_alloc_triangles": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_scene_put_triangles": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
+    "rx_scene_put_indexed": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p, _i32p, ctypes.c_int,
+                              _f64p, _i32p, _f64p, _f64p, _i32p, ctypes.c_int, _i32p], ctypes.c_int),
+    "rx_scene_get_triangles": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
     "rx_scene_set_materials": ([ctypes.c_void_p, ctypes.c_int, _i32p, _f32p, _f32p, _f32p, _f32p], ctypes.c_int),
     "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p] + [_f32p] * 4,
                              ctypes.c_int),
@@ -233,6 +239,55 @@ class NativeScene:
         self.ctx.check(lib().rx_scene_set_triangles(self.h, n, fptr(v0), fptr(v1), fptr(v2), fptr(n0), fptr(n1),
                                                     fptr(n2), iptr(mat)))
         self.n_tris = n
+
+    # -- piecewise extraction on the device --------------------------------------
+    def alloc_triangles(self, n):
+        self.ctx.check(lib().rx_scene_alloc_triangles(self.h, int(n)))
+        self.n_tris = int(n)
+
+    def put_triangles(self, offset, v0, v1, v2, n0=None, n1=None, n2=None, mat_idx=None):
+        v0, v1, v2 = f32(v0, (-1, 3)), f32(v1, (-1, 3)), f32(v2, (-1, 3))
+        n = len(v0)
+        rows = [f32(a, (-1, 3)) if a is not None else None for a in (n0, n1, n2)]
+        mat = i32(mat_idx) if mat_idx is not None else None
+        if any(len(a) != n for a in [v1, v2] + [r for r in rows if r is not None]) or (mat is not None and
+                                                                                        len(mat) != n):
+            raise ValueError("triangle arrays must all have the same length")
+        self.ctx.check(lib().rx_scene_put_triangles(self.h, int(offset), n, fptr(v0), fptr(v1), fptr(v2),
+                                                    *[fptr(r) for r in rows], iptr(mat)))
+
+    def put_indexed(self, offset, positions, tri_pos_idx, normals=None, tri_normal_idx=None, matrix=None,
+                    normal_matrix=None, tri_group_idx=None, group_mat=None):
+        """Rows [offset, offset + len(tri_pos_idx)) from an indexed mesh,
+        transformed on the device (rx_scene_put_indexed)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape((-1, 3))
+        tri = i32(tri_pos_idx).reshape((-1, 3))
+        n = len(tri)
+        nrm = tn = None
+        if normals is not None and tri_normal_idx is not None:
+            nrm = np.ascontiguousarray(normals, dtype=np.float64).reshape((-1, 3))
+            tn = i32(tri_normal_idx).reshape((-1, 3))
+            if len(tn) != n:
+                raise ValueError("tri_normal_idx must have one row per triangle")
+        gi = None
+        if tri_group_idx is not None:
+            gi = i32(tri_group_idx).reshape(-1)
+            if len(gi) != n:
+                raise ValueError("tri_group_idx must have one entry per triangle")
+        gm = i32(group_mat if group_mat is not None else [0]).reshape(-1)
+        m4 = lambda m: None if m is None else np.ascontiguousarray(m, dtype=np.float64).reshape(16)  # noqa: E731
+        M, NM = m4(matrix), m4(normal_matrix)
+        dp = lambda a: None if a is None else a.ctypes.data_as(_f64p)  # noqa: E731
+        self.ctx.check(lib().rx_scene_put_indexed(self.h, int(offset), n, len(pos), dp(pos), iptr(tri),
+                                                  0 if nrm is None else len(nrm), dp(nrm), iptr(tn), dp(M), dp(NM),
+                                                  iptr(gi), len(gm), iptr(gm)))
+
+    def get_triangles(self, offset=0, n=None):
+        n = self.n_tris - offset if n is None else int(n)
+        out = [np.empty((n, 3), np.float32) for _ in range(6)]
+        mat = np.empty(n, np.int32)
+        self.ctx.check(lib().rx_scene_get_triangles(self.h, int(offset), n, *[fptr(a) for a in out], iptr(mat)))
+        return dict(zip(("v0", "v1", "v2", "n0", "n1", "n2"), out), mat_idx=mat)
 
     def set_materials(self, mat_type, albedo, roughness, ior, emission):
         t = i32(mat_type)

@@ -9,7 +9,7 @@ import pytest
 import golden_scenes as gs
 import roxy_native as nat
 from rendering.denoise import edge_aware_denoise, linear_to_display
-from rendering.taichi.extractor import build_device_scene
+from rendering.taichi.extractor import HostScene, build_device_scene
 from test_host_logic import _ns
 
 pytestmark = pytest.mark.gpu
@@ -19,10 +19,11 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 @pytest.mark.parametrize("method", ["morton", "lbvh"])
 def test_scene_intersect_matches_reference(method):
     g = np.load(os.path.join(GOLD, "trace_scene.npz"))
-    ds = build_device_scene(gs.build_trace_scene(_ns()), method=method)
+    world = gs.build_trace_scene(_ns())
+    ds = build_device_scene(world, method=method)
     r = ds.native.intersect(g["si_ro"], g["si_rd"])
     # golden ids: object slot (is_bvh 0) or BVH-order triangle (is_bvh 1)
-    bv = oracle_order(ds)
+    bv = oracle_order(world)
     for i in range(len(g["si_t"])):
         ref_bvh = g["si_is_bvh"][i] == 1
         if g["si_idx"][i] < 0:
@@ -37,9 +38,9 @@ def test_scene_intersect_matches_reference(method):
     np.testing.assert_allclose(r["normal"][hit], g["si_normal"][hit], atol=2e-7)
 
 
-def oracle_order(ds):
+def oracle_order(world):
     from oracle import oracle
-    b = ds.builder._batch
+    b = HostScene(world).batch
     return oracle.bvh_build_morton(b.v0, b.v1, b.v2, 8)["order"]
 
 

@@ -95,6 +95,20 @@ def test_indexed_mesh_flattening_matches_reference():
         np.testing.assert_array_equal(arrs[k], g[k], err_msg=k)
 
 
+def test_emissive_rows_use_the_device_kernel_order():
+    """Light triangles are transformed on the host in the element-wise order
+    of k_extract_indexed; on the golden object that equals the reference's
+    BLAS transform after rounding to float32."""
+    from rendering.taichi.extractor import _indexed_world_positions
+    g = np.load(os.path.join(GOLD, "indexed_arrays.npz"))
+    obj = gs.build_indexed_object(_ns())
+    geo = obj.shapes[0].geometry
+    sel = np.arange(0, geo.triangle_count, 3)
+    w = _indexed_world_positions(geo, obj.world_matrix, sel)
+    for c, k in enumerate(("v0", "v1", "v2")):
+        assert np.array_equal(w[:, c].view(np.uint32), g[k][sel].view(np.uint32)), k
+
+
 def test_trace_scene_flattening_matches_reference_extract():
     """Object slots, palette and BVH-ordered triangles equal extract_scene's."""
     g = np.load(os.path.join(GOLD, "trace_scene.npz"))

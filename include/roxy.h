@@ -118,6 +118,23 @@ int rx_scene_put_indexed(rx_scene* scene, int offset, int n_tris, int n_pos, con
                          int n_groups, const int* group_mat);
 int rx_scene_get_triangles(rx_scene* scene, int offset, int n, float* v0, float* v1, float* v2, float* n0,
                            float* n1, float* n2, int* mat_idx);
+/* Albedo textures (rendering/taichi/extractor.py:53-81 _upload_textures,
+ * sampled as trace.py:96-136 _sample_texture / _bvh_albedo).
+ *   rx_scene_put_uvs   per source triangle uv0..uv2 (n,2) float32 and has_uv
+ *                      (n,) (NULL -> all 1) for rows [offset, offset+n); rows
+ *                      never written have no uvs.  Triangle uploads drop them.
+ *   rx_scene_set_textures  n RGB u8 images, width[i] x height[i], row-major,
+ *                      concatenated in `texels`; flip_v[i] != 0 flips v.
+ *   rx_scene_set_material_textures  texture index (-1 none) per entry of the
+ *                      palette given to rx_scene_set_materials (call it after
+ *                      that function, which resets them to -1).
+ * A BVH triangle whose material has a texture and whose row has uvs shades
+ * with albedo x bilinear texel / 255; a texture index >= n samples white. */
+int rx_scene_put_uvs(rx_scene* scene, int offset, int n, const float* uv0, const float* uv1, const float* uv2,
+                     const int* has_uv);
+int rx_scene_set_textures(rx_scene* scene, int n, const int* width, const int* height, const int* flip_v,
+                          const unsigned char* texels);
+int rx_scene_set_material_textures(rx_scene* scene, int n, const int* texture_idx);
 /* Material palette (fields.py:73-78). */
 int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float* albedo,
                            const float* roughness, const float* ior, const float* emission);

@@ -163,6 +163,15 @@ typedef struct {
   const float* alias_prob;      // alias table
   const int* alias_idx;
   const int* light_obj;         // sphere light: object slot | triangle light: -1
+  // albedo textures (fields.py:64-66,80-87): BVH-order uvs, texture index per
+  // material, RGB u8 images packed back to back
+  const float* uv0; const float* uv1; const float* uv2;  // [n_tris*2] or null
+  const int* has_uv;                                      // [n_tris] or null
+  const int* mat_texture;                                 // [n_mats] or null
+  int n_tex;
+  const int* tex_w; const int* tex_h; const int* tex_flip;
+  const long long* tex_off;
+  const unsigned char* texels;
 } orc_scene;
 
 typedef struct {
@@ -654,6 +663,44 @@ struct PathOut {
   float depth;
 };
 
+// trace.py:96-126 _sample_texture.
+inline V3 sample_texture(const orc_scene& s, int ti, float uu, float vv) {
+  V3 r = mk(1.0f, 1.0f, 1.0f);
+  if (ti < 0 || ti >= s.n_tex) return r;
+  int w = s.tex_w[ti], h = s.tex_h[ti];
+  if (w > 0 && h > 0) {
+    float u = uu - std::floor(uu);
+    float v = vv - std::floor(vv);
+    if (s.tex_flip[ti] != 0) v = 1.0f - v;
+    float x = u * (float)(w - 1);
+    float y = v * (float)(h - 1);
+    int x0 = (int)std::floor(x), y0 = (int)std::floor(y);
+    int x1 = std::min(x0 + 1, w - 1), y1 = std::min(y0 + 1, h - 1);
+    float tx = x - (float)x0, ty = y - (float)y0;
+    const unsigned char* px = s.texels + s.tex_off[ti];
+    auto texel = [&](int yy, int xx) {
+      const unsigned char* q = px + 3 * ((size_t)yy * w + xx);
+      return mk((float)q[0] / 255.0f, (float)q[1] / 255.0f, (float)q[2] / 255.0f);
+    };
+    V3 c0 = texel(y0, x0) * (1.0f - tx) + texel(y0, x1) * tx;
+    V3 c1 = texel(y1, x0) * (1.0f - tx) + texel(y1, x1) * tx;
+    r = c0 * (1.0f - ty) + c1 * ty;
+  }
+  return r;
+}
+
+// trace.py:129-136 _bvh_albedo (tri = BVH-order triangle).
+inline V3 bvh_albedo(const orc_scene& s, int tri, int mat, float bu, float bv, V3 base) {
+  int ti = s.mat_texture ? s.mat_texture[mat] : -1;
+  if (ti >= 0 && s.has_uv && s.has_uv[tri] != 0) {
+    float w = 1.0f - bu - bv;
+    float u = (s.uv0[2 * tri] * w + s.uv1[2 * tri] * bu) + s.uv2[2 * tri] * bv;
+    float v = (s.uv0[2 * tri + 1] * w + s.uv1[2 * tri + 1] * bu) + s.uv2[2 * tri + 1] * bv;
+    return base * sample_texture(s, ti, u, v);
+  }
+  return base;
+}
+
 // trace.py:139-236 — the per-path bounce loop.
 inline PathOut trace(const orc_scene& s, const orc_params& p, Rng& rng, V3 ro, V3 rd, Counters& cnt) {
   V3 color = mk(0.0f, 0.0f, 0.0f);
@@ -687,11 +734,12 @@ inline PathOut trace(const orc_scene& s, const orc_params& p, Rng& rng, V3 ro, V
     bool listed_light;
     if (h.is_bvh) {
       mt = s.mat_type[h.bvh_mat];
-      alb = ld3(s.mat_albedo, h.bvh_mat);
+      alb = bvh_albedo(s, h.idx, h.bvh_mat, h.u, h.v, ld3(s.mat_albedo, h.bvh_mat));
       rough = s.mat_roughness[h.bvh_mat];
       ior = s.mat_ior[h.bvh_mat];
       em = s.mat_emission[h.bvh_mat];
-      listed_light = true;  // every emissive BVH triangle is in the light list
+      // every emissive BVH triangle is in the light list except textured ones
+      listed_light = !(s.mat_texture && s.mat_texture[h.bvh_mat] >= 0);
     } else {
       mt = s.obj_mat_type[h.idx];
       alb = ld3(s.obj_albedo, h.idx);
@@ -865,6 +913,24 @@ void orc_tri_intersect(long n, const float* ro, const float* rd, const float* v0
 }
 
 // One path from (ro, rd) with the random numbers taken in call order from
+// _sample_texture for n uvs of texture `ti` -> out[n*3].
+void orc_sample_texture(const orc_scene* s, int ti, int n, const float* uv, float* out) {
+  for (int i = 0; i < n; ++i) {
+    V3 c = sample_texture(*s, ti, uv[2 * i], uv[2 * i + 1]);
+    out[3 * i] = c.x; out[3 * i + 1] = c.y; out[3 * i + 2] = c.z;
+  }
+}
+
+// _bvh_albedo of BVH-order triangles tri[i] with material mat[i] at
+// barycentrics (u[i], v[i]) over base albedo base[i*3] -> out[n*3].
+void orc_bvh_albedo(const orc_scene* s, int n, const int* tri, const int* mat, const float* u, const float* v,
+                    const float* base, float* out) {
+  for (int i = 0; i < n; ++i) {
+    V3 c = bvh_albedo(*s, tri[i], mat[i], u[i], v[i], mk(base[3 * i], base[3 * i + 1], base[3 * i + 2]));
+    out[3 * i] = c.x; out[3 * i + 1] = c.y; out[3 * i + 2] = c.z;
+  }
+}
+
 // `stream` — the way the reference's trace() consumes ti.random().  Used to
 // pin this restatement against the reference's own trace source.
 int orc_trace_scripted(const orc_scene* s, const orc_params* p, const float* ro, const float* rd,

@@ -46,6 +46,9 @@ class OrcScene(ctypes.Structure):
         ("n_lights", ctypes.c_int), ("light_kind", _i32p), ("light_p0", _f32p), ("light_p1", _f32p),
         ("light_p2", _f32p), ("light_albedo", _f32p), ("light_emission", _f32p), ("light_area", _f32p),
         ("light_pick_pdf", _f32p), ("alias_prob", _f32p), ("alias_idx", _i32p), ("light_obj", _i32p),
+        ("uv0", _f32p), ("uv1", _f32p), ("uv2", _f32p), ("has_uv", _i32p), ("mat_texture", _i32p),
+        ("n_tex", ctypes.c_int), ("tex_w", _i32p), ("tex_h", _i32p), ("tex_flip", _i32p),
+        ("tex_off", ctypes.POINTER(ctypes.c_longlong)), ("texels", ctypes.c_void_p),
     ]
 
 
@@ -99,7 +102,8 @@ class Scene:
     def __init__(self, *, node_min=None, node_max=None, left=None, right=None, start=None, count=None,
                  v0=None, v1=None, v2=None, n0=None, n1=None, n2=None, tri_mat=None,
                  mat_type=None, mat_albedo=None, mat_roughness=None, mat_ior=None, mat_emission=None,
-                 objects=None, lights=None):
+                 objects=None, lights=None, uv0=None, uv1=None, uv2=None, has_uv=None, mat_texture=None,
+                 textures=None, tex_flip=None):
         keep = {}
         s = OrcScene()
 
@@ -158,6 +162,22 @@ class Scene:
         s.light_area, s.light_pick_pdf = F("lar", L.get("area")), F("lpp", L.get("pick_pdf"))
         s.alias_prob, s.alias_idx = F("lap", L.get("alias_prob")), I("lai", L.get("alias_idx"))
         s.light_obj = I("lo", L.get("obj"))
+        # textures: uv rows in BVH order, texture index per material, list of
+        # (H, W, 3) uint8 images
+        s.uv0, s.uv1, s.uv2 = F("uv0", uv0), F("uv1", uv1), F("uv2", uv2)
+        s.has_uv, s.mat_texture = I("huv", has_uv), I("mtex", mat_texture)
+        imgs = [np.ascontiguousarray(im, dtype=np.uint8) for im in (textures or [])]
+        s.n_tex = len(imgs)
+        if imgs:
+            s.tex_w = I("tw", [im.shape[1] for im in imgs])
+            s.tex_h = I("th", [im.shape[0] for im in imgs])
+            s.tex_flip = I("tf", tex_flip if tex_flip is not None else [0] * len(imgs))
+            off = np.cumsum([0] + [im.size for im in imgs[:-1]]).astype(np.int64)
+            keep["toff"] = off
+            s.tex_off = off.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+            tx = np.concatenate([im.reshape(-1) for im in imgs])
+            keep["texels"] = tx
+            s.texels = tx.ctypes.data_as(ctypes.c_void_p)
         self._keep = keep
         self.s = s
 
@@ -257,6 +277,24 @@ def trace_scripted(scene, params, ro, rd, stream):
                                     len(stream), _p(color), _p(nrm), _p(alb), _p(dep),
                                     rays.ctypes.data_as(ctypes.POINTER(ctypes.c_long)))
     return dict(color=color, normal=nrm, albedo=alb, depth=float(dep[0]), consumed=used, rays=int(rays[0]))
+
+
+def sample_texture(scene, tex_idx, uv):
+    """_sample_texture (trace.py:96-126) at each uv row -> (n, 3)."""
+    uv = _f(uv).reshape((-1, 2))
+    out = np.zeros((len(uv), 3), np.float32)
+    lib().orc_sample_texture(scene.ptr(), int(tex_idx), len(uv), _p(uv), _p(out))
+    return out
+
+
+def bvh_albedo(scene, tri, mat, u, v, base):
+    """_bvh_albedo (trace.py:129-136) per (BVH-order triangle, material,
+    barycentrics, base albedo) -> (n, 3)."""
+    tri, mat = _i(tri), _i(mat)
+    u, v, base = _f(u), _f(v), _f(base).reshape((-1, 3))
+    out = np.zeros((len(tri), 3), np.float32)
+    lib().orc_bvh_albedo(scene.ptr(), len(tri), _p(tri, _i32p), _p(mat, _i32p), _p(u), _p(v), _p(base), _p(out))
+    return out
 
 
 def render(scene, params, frames, rows=None, n_threads=0):

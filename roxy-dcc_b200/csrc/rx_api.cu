@@ -38,7 +38,7 @@ int Scene::upload_palette(Ctx* c) {
   std::vector<float4> a, b;
   auto push = [&](const HostMat& m) {
     a.push_back(make_float4(m.albedo[0], m.albedo[1], m.albedo[2], int_bits_as_float(m.type)));
-    b.push_back(make_float4(m.roughness, m.ior, m.emission, int_bits_as_float(-1)));
+    b.push_back(make_float4(m.roughness, m.ior, m.emission, int_bits_as_float(m.texture)));
   };
   for (auto& m : user_mats) push(m);
   for (auto& m : obj_mats) push(m);
@@ -203,6 +203,7 @@ int rx_scene_set_triangles(rx_scene* scene, int n, const float* v0, const float*
   s.d_n0 = s.n0b.p; s.d_n1 = s.n1b.p; s.d_n2 = s.n2b.p;
   s.d_tri_mat = s.tri_matb.p;
   s.n_tris = n;
+  s.uvb.release();
   s.clear_bvh();
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return RX_OK;
@@ -255,6 +256,43 @@ int rx_scene_get_triangles(rx_scene* scene, int offset, int n, float* v0, float*
   return scene_get_triangles(c, &s, offset, n, rows, mat_idx);
 }
 
+int rx_scene_put_uvs(rx_scene* scene, int offset, int n, const float* uv0, const float* uv1, const float* uv2,
+                     const int* has_uv) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  return scene_put_uvs(c, &s, offset, n, uv0, uv1, uv2, has_uv);
+}
+
+int rx_scene_set_textures(rx_scene* scene, int n, const int* width, const int* height, const int* flip_v,
+                          const unsigned char* texels) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  return scene_set_textures(c, &s, n, width, height, flip_v, texels);
+}
+
+int rx_scene_set_material_textures(rx_scene* scene, int n, const int* texture_idx) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  if (n != (int)s.user_mats.size() || (n > 0 && !texture_idx))
+    return set_error(c, "set_material_textures: %d entries for a palette of %zu", n, s.user_mats.size()),
+           RX_ERR_ARG;
+  for (int i = 0; i < n; ++i) s.user_mats[i].texture = texture_idx[i] < 0 ? -1 : texture_idx[i];
+  int rc = s.upload_palette(c);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  ++s.version;
+  return RX_OK;
+}
+
 int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float* albedo, const float* roughness,
                            const float* ior, const float* emission) {
   if (!scene) return RX_ERR_ARG;
@@ -271,6 +309,7 @@ int rx_scene_set_materials(rx_scene* scene, int n, const int* type, const float*
     m.roughness = roughness[i];
     m.ior = ior[i];
     m.emission = emission[i];
+    m.texture = -1;
   }
   // object materials follow the caller's palette: re-index the slots
   for (int i = 0; i < (int)s.objs.size(); ++i) s.objs[i].mat = n + i;

@@ -151,6 +151,7 @@ int scene_alloc_triangles(Ctx* c, Scene* s, int n) {
   s->d_n0 = s->n0b.p; s->d_n1 = s->n1b.p; s->d_n2 = s->n2b.p;
   s->d_tri_mat = s->tri_matb.p;
   s->n_tris = n;
+  s->uvb.release();
   s->clear_bvh();
   return RX_OK;
 }
@@ -240,6 +241,70 @@ int scene_put_indexed(Ctx* c, Scene* s, int offset, int n_tris, int n_pos, const
   if (herr & 1) return set_error(c, "put_indexed: a position index is outside [0, %d)", n_pos), RX_ERR_ARG;
   if (herr & 2) return set_error(c, "put_indexed: a normal index is outside [0, %d)", n_nrm), RX_ERR_ARG;
   if (herr & 4) return set_error(c, "put_indexed: a group index is outside [0, %d)", n_groups), RX_ERR_ARG;
+  return RX_OK;
+}
+
+__global__ void k_pack_uvs(int n, const float* __restrict__ uv0, const float* __restrict__ uv1,
+                           const float* __restrict__ uv2, const int* __restrict__ has_uv, float4* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    out[2 * (size_t)i] = make_float4(uv0[2 * i], uv0[2 * i + 1], uv1[2 * i], uv1[2 * i + 1]);
+    out[2 * (size_t)i + 1] = make_float4(uv2[2 * i], uv2[2 * i + 1], __int_as_float(has_uv ? (has_uv[i] != 0) : 1),
+                                         0.0f);
+  }
+}
+
+int scene_put_uvs(Ctx* c, Scene* s, int offset, int n, const float* uv0, const float* uv1, const float* uv2,
+                  const int* has_uv) {
+  if (offset < 0 || n < 0 || (long long)offset + n > s->n_tris)
+    return set_error(c, "put_uvs: rows [%d, %d) outside the %d present", offset, offset + n, s->n_tris), RX_ERR_ARG;
+  if (n > 0 && (!uv0 || !uv1 || !uv2)) return set_error(c, "put_uvs: bad arguments"), RX_ERR_ARG;
+  if (!s->uvb.p) {
+    // rows without uvs read has_uv = 0
+    if (!s->uvb.alloc(c, 2 * (size_t)std::max(s->n_tris, 1)))
+      return set_error(c, "put_uvs: out of device memory"), RX_ERR_CAPACITY;
+    CUDA_TRY(c, cudaMemsetAsync(s->uvb.p, 0, s->uvb.bytes(), c->stream));
+  }
+  if (n == 0) return RX_OK;
+  DevBuf<float> d0, d1, d2;
+  DevBuf<int> dh;
+  int rc;
+  if ((rc = upload_tmp(c, d0, uv0, (size_t)2 * n)) || (rc = upload_tmp(c, d1, uv1, (size_t)2 * n)) ||
+      (rc = upload_tmp(c, d2, uv2, (size_t)2 * n)))
+    return rc;
+  if (has_uv && (rc = upload_tmp(c, dh, has_uv, (size_t)n))) return rc;
+  int blocks = (int)std::min<long long>((n + 255) / 256, (long long)c->num_sms * 8);
+  k_pack_uvs<<<blocks, 256, 0, c->stream>>>(n, d0.p, d1.p, d2.p, has_uv ? dh.p : nullptr, s->uvb.p + 2 * (size_t)offset);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  ++s->version;
+  return RX_OK;
+}
+
+int scene_set_textures(Ctx* c, Scene* s, int n, const int* width, const int* height, const int* flip_v,
+                       const unsigned char* texels) {
+  if (n < 0 || (n > 0 && (!width || !height))) return set_error(c, "set_textures: bad arguments"), RX_ERR_ARG;
+  std::vector<TexInfo> info(std::max(n, 1));
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    if (width[i] < 0 || height[i] < 0 || width[i] > (1 << 16) || height[i] > (1 << 16))
+      return set_error(c, "set_textures: texture %d has size %dx%d", i, width[i], height[i]), RX_ERR_ARG;
+    info[i].offset = total;
+    info[i].w = width[i];
+    info[i].h = height[i];
+    info[i].flip_v = flip_v ? (flip_v[i] != 0) : 0;
+    info[i].pad = 0;
+    total += 3LL * width[i] * height[i];
+  }
+  if (total > 0 && !texels) return set_error(c, "set_textures: texels is NULL"), RX_ERR_ARG;
+  if (!s->d_tex.alloc(c, info.size()) || !s->d_texels.alloc(c, (size_t)std::max<long long>(total, 1)))
+    return set_error(c, "set_textures: out of device memory for %lld texel bytes", total), RX_ERR_CAPACITY;
+  CUDA_TRY(c, cudaMemcpyAsync(s->d_tex.p, info.data(), sizeof(TexInfo) * info.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+  if (total > 0)
+    CUDA_TRY(c, cudaMemcpyAsync(s->d_texels.p, texels, (size_t)total, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  s->n_tex = n;
+  ++s->version;
   return RX_OK;
 }
 

@@ -88,6 +88,14 @@ struct Light {
   float3 albedo;
 };
 
+// Albedo texture: RGB u8 texels, row-major, at byte `offset` of the scene's
+// texel buffer (rendering/taichi/fields.py:82-87 keeps them in a fixed
+// 8 x 2048 x 2048 field; here they are packed back to back).
+struct TexInfo {
+  long long offset;
+  int w, h, flip_v, pad;
+};
+
 struct DevScene {
   const float4* nodes;     // n_nodes * 4
   int n_nodes;
@@ -105,7 +113,52 @@ struct DevScene {
   const int* alias_idx;
   int n_lights;
   int exact_slab;          // 1: slab test with the reference's operation order
+  const float4* uvs;       // 2 per source triangle: (uv0, uv1), (uv2, has_uv, 0), or null
+  const TexInfo* tex;
+  const unsigned char* texels;
+  int n_tex;
 };
+
+// _sample_texture (rendering/taichi/trace.py:96-126): repeat wrap, optional
+// v flip, bilinear over texels / 255, in the reference's float32 order.
+__device__ __forceinline__ float3 tex_sample(const DevScene& S, int ti, float uu, float vv) {
+  float3 r = make_float3(1.0f, 1.0f, 1.0f);
+  if (ti < 0 || ti >= S.n_tex) return r;
+  TexInfo T = S.tex[ti];
+  if (T.w > 0 && T.h > 0) {
+    float u = uu - floorf(uu), v = vv - floorf(vv);
+    if (T.flip_v != 0) v = 1.0f - v;
+    float x = u * (float)(T.w - 1), y = v * (float)(T.h - 1);
+    int x0 = (int)floorf(x), y0 = (int)floorf(y);
+    float tx = x - (float)x0, ty = y - (float)y0;
+    // finite uv keep x0, y0 inside the image; the clamp only guards memory
+    x0 = min(max(x0, 0), T.w - 1);
+    y0 = min(max(y0, 0), T.h - 1);
+    int x1 = min(x0 + 1, T.w - 1), y1 = min(y0 + 1, T.h - 1);
+    const unsigned char* px = S.texels + T.offset;
+    auto texel = [&](int yy, int xx) {
+      const unsigned char* q = px + 3 * ((size_t)yy * T.w + xx);
+      return make_float3((float)q[0] / 255.0f, (float)q[1] / 255.0f, (float)q[2] / 255.0f);
+    };
+    float3 c00 = texel(y0, x0), c10 = texel(y0, x1), c01 = texel(y1, x0), c11 = texel(y1, x1);
+    float3 c0 = c00 * (1.0f - tx) + c10 * tx;
+    float3 c1 = c01 * (1.0f - tx) + c11 * tx;
+    r = c0 * (1.0f - ty) + c1 * ty;
+  }
+  return r;
+}
+
+// _bvh_albedo (trace.py:129-136): base albedo times the texture at the
+// barycentric uv of source triangle `src`, when it has uvs.
+__device__ __forceinline__ float3 textured_albedo(const DevScene& S, int src, int ti, float bu, float bv, float3 base) {
+  if (ti < 0 || !S.uvs) return base;
+  float4 a = __ldg(S.uvs + 2 * (size_t)src), b = __ldg(S.uvs + 2 * (size_t)src + 1);
+  if (__float_as_int(b.z) == 0) return base;
+  float w = 1.0f - bu - bv;
+  float u = (a.x * w + a.z * bu) + b.x * bv;
+  float v = (a.y * w + a.w * bu) + b.y * bv;
+  return base * tex_sample(S, ti, u, v);
+}
 
 // --------------------------------------------------------------------- RNG
 // Philox4x32-10 (Salmon et al., SC'11): counter = (pixel, sample, bounce,

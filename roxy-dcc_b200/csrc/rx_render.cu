@@ -329,6 +329,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
         float t = h.x;
         float3 nn;
         int m;
+        int src_tri = -1;
         bool listed;
         if (code >= 0) {
           const float4* sp = S.shade + 3 * (size_t)code;
@@ -337,7 +338,9 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
           m = __float_as_int(s0.w);
           if (__float_as_int(pa.w) == PRIM_TRI) {
             float w = 1.0f - h.z - h.w;
-            nn = normalized((xyz(s0) * w + xyz(__ldg(sp + 1)) * h.z) + xyz(__ldg(sp + 2)) * h.w);
+            float4 s1 = __ldg(sp + 1);
+            src_tri = __float_as_int(s1.w);
+            nn = normalized((xyz(s0) * w + xyz(s1) * h.z) + xyz(__ldg(sp + 2)) * h.w);
           } else {
             nn = normalized((o + d * t) - xyz(pa));
           }
@@ -358,7 +361,11 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
         int mt = __float_as_int(ma.w);
         float3 albedo = xyz(ma);
         float rough = mb.x, ior = mb.y, em = mb.z;
-        listed = listed && mt == 3 && em > 0.0f;
+        int tex = __float_as_int(mb.w);
+        if (src_tri >= 0 && tex >= 0) albedo = textured_albedo(S, src_tri, tex, h.z, h.w, albedo);
+        // textured emitters are left out of the light list (their radiance
+        // varies over the surface), so BSDF hits always count them
+        listed = listed && mt == 3 && em > 0.0f && !(src_tri >= 0 && tex >= 0);
         if (b == 0) {
           gn[p] = make_float4(nn.x, nn.y, nn.z, t);
           ga[p] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);

@@ -77,6 +77,7 @@ struct HostMat {
   int type;
   float albedo[3];
   float roughness, ior, emission;
+  int texture = -1;
 };
 
 struct Scene {
@@ -88,6 +89,12 @@ struct Scene {
   float *d_v0 = nullptr, *d_v1 = nullptr, *d_v2 = nullptr;
   float *d_n0 = nullptr, *d_n1 = nullptr, *d_n2 = nullptr;
   int* d_tri_mat = nullptr;
+  // per source triangle uvs (2 float4), allocated by the first put_uvs
+  DevBuf<float4> uvb;
+  // albedo textures
+  DevBuf<TexInfo> d_tex;
+  DevBuf<unsigned char> d_texels;
+  int n_tex = 0;
   // palette: caller materials followed by one entry per object slot
   std::vector<HostMat> user_mats;
   std::vector<HostMat> obj_mats;
@@ -152,6 +159,10 @@ struct Scene {
     s.alias_idx = d_alias_idx.p;
     s.n_lights = n_lights;
     s.exact_slab = exact_slab;
+    s.uvs = uvb.p;
+    s.tex = d_tex.p;
+    s.texels = d_texels.p;
+    s.n_tex = n_tex;
     return s;
   }
 };
@@ -170,6 +181,10 @@ int scene_put_indexed(Ctx* c, Scene* s, int offset, int n_tris, int n_pos, const
                       const double* matrix, const double* normal_matrix, const int* tri_group_idx, int n_groups,
                       const int* group_mat);
 int scene_get_triangles(Ctx* c, Scene* s, int offset, int n, float* const* rows, int* mat_idx);
+int scene_put_uvs(Ctx* c, Scene* s, int offset, int n, const float* uv0, const float* uv1, const float* uv2,
+                  const int* has_uv);
+int scene_set_textures(Ctx* c, Scene* s, int n, const int* width, const int* height, const int* flip_v,
+                       const unsigned char* texels);
 
 // traversal entry points (rx_trace.cu)
 int trace_closest(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_rd, float* d_t, int* d_id,

@@ -284,6 +284,11 @@ class GPUBVHBuilder:
                 np.array([m["roughness"] for m in pal], np.float32), np.array([m["ior"] for m in pal], np.float32),
                 np.array([m["emission"] for m in pal], np.float32))
 
+    def palette_textures(self):
+        """Texture index of each palette entry (-1: untextured)."""
+        pal = self.mat_palette or [{}]
+        return np.array([int(m.get("texture_idx", -1)) for m in pal], np.int32)
+
     # -- build ------------------------------------------------------------------
     def build(self, tri_data, method=None, native=None):
         """Build from TriangleBatch objects or legacy triangle dicts."""

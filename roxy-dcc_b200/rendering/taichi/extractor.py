@@ -2,9 +2,10 @@
 
 Flattens World objects the way the reference does — Mesh triangles and
 IndexedMesh arrays in world space into one triangle set with a material
-palette, analytic primitives into object slots — but in vectorised numpy
-and one upload per array instead of per-element field stores.  The BVH is
-built on the GPU.
+palette, analytic primitives into object slots, albedo textures into an
+indexed table — but in vectorised numpy and one upload per array instead
+of per-element field stores.  The renderer's path ("lbvh") transforms
+IndexedMesh geometry on the device; the BVH is built on the GPU.
 """
 import numpy as np
 
@@ -13,15 +14,53 @@ from rendering.taichi.bvh_builder import GPUBVHBuilder, TriangleBatch
 from rendering.taichi.lights import build_lights
 
 _DEFAULT_ALBEDO = (0.8, 0.8, 0.8)
+MAX_TEXTURES = 8
+MAX_TEXTURE_SIZE = 2048
 
 
-def _mat_record(mat):
+class TextureTable:
+    """Albedo textures in the order extract_scene numbers them
+    (extractor.py:96-117): first use in visit order, keyed by (path, flip_v,
+    identity of an in-memory texture)."""
+
+    def __init__(self):
+        self.textures = []
+        self._index = {}
+
+    def index(self, mat):
+        tex = getattr(mat, "_albedo_texture", None)
+        if tex is None:
+            return -1
+        key = (tex.path, bool(tex.flip_v), id(tex) if tex.path is None else None)
+        if key not in self._index:
+            if len(self.textures) >= MAX_TEXTURES:
+                raise ValueError(f"Scene has more than {MAX_TEXTURES} image textures; "
+                                 "increase MAX_TEXTURES in rendering/taichi/fields.py")
+            self._index[key] = len(self.textures)
+            self.textures.append(tex)
+        return self._index[key]
+
+    def images(self):
+        """(uint8 HxWx3 images, flip_v flags) as _upload_textures stores them."""
+        imgs = []
+        for t in self.textures:
+            data = np.asarray(t.load_pixels_u8(max_size=MAX_TEXTURE_SIZE), dtype=np.uint8)
+            if data.shape[0] > MAX_TEXTURE_SIZE or data.shape[1] > MAX_TEXTURE_SIZE:
+                raise ValueError(f"texture of {data.shape[1]}x{data.shape[0]} exceeds {MAX_TEXTURE_SIZE}")
+            imgs.append(data[:, :, :3])
+        return imgs, [1 if t.flip_v else 0 for t in self.textures]
+
+    def __len__(self):
+        return len(self.textures)
+
+
+def _mat_record(mat, textures=None):
     from scene.scene_object import SceneObject
     if mat is None:
         return {"mat_type": 0, "albedo": list(_DEFAULT_ALBEDO), "roughness": 0.0, "ior": 1.0, "emission": 0.0,
                 "texture_idx": -1}
     r = SceneObject.material_record(mat)
-    r["texture_idx"] = -1
+    r["texture_idx"] = textures.index(mat) if textures is not None else -1
     return r
 
 
@@ -51,7 +90,7 @@ def _xform_normals(M, nrm):
     return np.stack([X * inv, Y * inv, Z * inv], axis=1)
 
 
-def _mesh_batch(obj, shape, mesh):
+def _mesh_batch(obj, shape, mesh, textures=None):
     tris = mesh._triangles
     if not tris:
         return None
@@ -77,7 +116,7 @@ def _mesh_batch(obj, shape, mesh):
         g = t._group
         if g not in groups:
             groups[g] = len(recs)
-            recs.append(_mat_record(shape.material_for_group(g)))
+            recs.append(_mat_record(shape.material_for_group(g), textures))
         mat_idx[i] = groups[g]
     Vw = _xform_points(M, V.reshape((-1, 3))).reshape((n, 3, 3)).astype(np.float32)
     Nw = _xform_normals(inv_T, N.reshape((-1, 3))).reshape((n, 3, 3)).astype(np.float32)
@@ -89,15 +128,15 @@ def _mesh_batch(obj, shape, mesh):
                          np.array([r["ior"] for r in recs], np.float32).reshape(k),
                          np.array([r["emission"] for r in recs], np.float32).reshape(k),
                          uv0=UV[:, 0], uv1=UV[:, 1], uv2=UV[:, 2], has_uv=has_uv,
-                         texture_idx=np.full(k, -1, np.int32), mat_idx=mat_idx)
+                         texture_idx=np.array([r["texture_idx"] for r in recs], np.int32).reshape(k),
+                         mat_idx=mat_idx)
 
 
 def _walk(world):
-    """Renderable geometry in visit order: (object, shape, IndexedMesh)
-    triples, (object, shape, Mesh) triples and the object-slot dicts of
-    analytic primitives."""
+    """Renderable geometry in visit order: ("mesh" | "indexed", object, shape,
+    geometry) items and the object-slot dicts of analytic primitives."""
     from scene.mesh import IndexedMesh, Mesh
-    indexed, meshes, slots = [], [], []
+    items, slots = [], []
 
     def visit(obj):
         if not obj.renderable:
@@ -105,9 +144,9 @@ def _walk(world):
         for shape in obj.shapes:
             geo = shape.geometry
             if isinstance(geo, Mesh):
-                meshes.append((obj, shape, geo))
+                items.append(("mesh", obj, shape, geo))
             elif isinstance(geo, IndexedMesh):
-                indexed.append((obj, shape, geo))
+                items.append(("indexed", obj, shape, geo))
             else:
                 exported = obj.taichi_export()
                 if isinstance(exported, list):
@@ -120,21 +159,30 @@ def _walk(world):
 
     for o in world.objects:
         visit(o)
-    return indexed, meshes, slots
+    return items, slots
 
 
-def collect(world):
+def _group_records(shape, geo, textures):
+    """Material record of every group of an IndexedMesh, in group order."""
+    return {gi: _mat_record(shape.material_for_group(g), textures) for gi, g in enumerate(geo.groups)}
+
+
+def collect(world, textures=None):
     """(triangle batches, object slots) of every renderable object.  IndexedMesh
     batches come first in visit order and Mesh triangles after them, the
-    order extract_scene gives the reference's builder."""
-    indexed, meshes, slots = _walk(world)
-    batches = []
-    for obj, shape, geo in indexed:
-        arrays = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
-        mats = {gi: _mat_record(shape.material_for_group(g)) for gi, g in enumerate(arrays["groups"])}
-        batches.append(TriangleBatch.from_indexed_arrays(arrays, mats))
-    mesh_batches = [b for b in (_mesh_batch(o, s, g) for o, s, g in meshes) if b is not None]
-    return batches + mesh_batches, slots
+    order extract_scene gives the reference's builder; `textures` (a
+    TextureTable) receives the albedo textures in the reference's order."""
+    items, slots = _walk(world)
+    indexed, meshes = [], []
+    for kind, obj, shape, geo in items:
+        if kind == "indexed":
+            arrays = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+            indexed.append(TriangleBatch.from_indexed_arrays(arrays, _group_records(shape, geo, textures)))
+        else:
+            b = _mesh_batch(obj, shape, geo, textures)
+            if b is not None:
+                meshes.append(b)
+    return indexed + meshes, slots
 
 
 def slot_arrays(slots):
@@ -163,41 +211,43 @@ class DeviceScene:
 
     light_args: (v0, v1, v2, palette index) of at least every emissive
     triangle, in scene order, followed by the palette's type, albedo and
-    emission arrays.  h2d_bytes: bytes copied host -> device for the
-    geometry."""
+    emission arrays; pal_texture: texture index per palette entry.
+    h2d_bytes: bytes copied host -> device for the geometry."""
 
-    def __init__(self, native, slots, stats, light_args, builder=None, h2d_bytes=0):
+    def __init__(self, native, slots, stats, light_args, builder=None, h2d_bytes=0, pal_texture=None):
         self.native = native
         self.slots = slots
         self.stats = stats
         self.builder = builder
         self.h2d_bytes = int(h2d_bytes)
         self._light_args = light_args
+        self.pal_texture = pal_texture
         self._lights_mode = None
 
     @classmethod
-    def from_builder(cls, builder, slots, stats):
+    def from_builder(cls, builder, slots, stats, h2d_extra=0):
         b = builder._batch
         pal = builder.palette_arrays()
-        h2d = sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + 4 * b.triangle_count
+        h2d = sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + 4 * b.triangle_count + h2d_extra
         return cls(builder.native, slots, stats, (b.v0, b.v1, b.v2, builder._source_mat_idx, pal[0], pal[1], pal[4]),
-                   builder=builder, h2d_bytes=h2d)
+                   builder=builder, h2d_bytes=h2d, pal_texture=builder.palette_textures())
 
     def use_lights(self, compat):
         compat = bool(compat)
         if self._lights_mode is compat:
             return
-        lights = build_lights(self.slots, *self._light_args, compat=compat)
+        lights = build_lights(self.slots, *self._light_args, compat=compat, pal_texture=self.pal_texture)
         self.native.set_lights(lights)
         self._lights_mode = compat
 
 
 class HostScene:
     """Host-side flattening of a world: concatenated triangles, palette,
-    per-triangle palette index and object slots (no device work)."""
+    per-triangle palette index, object slots and textures (no device work)."""
 
     def __init__(self, world):
-        batches, slots = collect(world)
+        self.texture_table = TextureTable()
+        batches, slots = collect(world, self.texture_table)
         self.batches = batches
         self.slots = slots
         self.batch = TriangleBatch.concat(batches)
@@ -205,11 +255,13 @@ class HostScene:
         self.mat_idx = (self.builder._material_indices(self.batch) if self.batch.triangle_count
                         else np.zeros(0, np.int32))
         self.palette = self.builder.palette_arrays()
+        self.mat_texture = self.builder.palette_textures()
+        self.textures, self.tex_flip = self.texture_table.images()
 
     def lights(self, compat):
         b = self.batch
         return build_lights(self.slots, b.v0, b.v1, b.v2, self.mat_idx, self.palette[0], self.palette[1],
-                            self.palette[4], compat=compat)
+                            self.palette[4], compat=compat, pal_texture=self.mat_texture)
 
 
 def _indexed_world_positions(geo, matrix, sel):
@@ -232,18 +284,31 @@ def _emissive(builder, palette_idx):
     return m["type"] == 3 and m["emission"] > 0.0
 
 
-def _extract_on_device(world, native, builder):
+def _textured(builder, palette_idx):
+    return builder.mat_palette[int(palette_idx)].get("texture_idx", -1) >= 0
+
+
+def _extract_on_device(world, native, builder, textures):
     """Fill `native`'s triangle arrays with the world's triangles in the order
     and palette of collect() + GPUBVHBuilder.build, transforming IndexedMesh
     geometry on the device (rx_scene_put_indexed).  Returns (slots, triangle
     count, emissive triangle rows, host->device bytes)."""
-    indexed, meshes, slots = _walk(world)
-    mesh_batches = [b for b in (_mesh_batch(o, s, g) for o, s, g in meshes) if b is not None]
-    total = sum(g.triangle_count for _, _, g in indexed) + sum(b.triangle_count for b in mesh_batches)
+    items, slots = _walk(world)
+    # material records in visit order (this numbers the textures as the
+    # reference does), then triangles: IndexedMesh first, Mesh after
+    indexed, mesh_batches = [], []
+    for kind, obj, shape, geo in items:
+        if kind == "indexed":
+            indexed.append((obj, geo, _group_records(shape, geo, textures)))
+        else:
+            b = _mesh_batch(obj, shape, geo, textures)
+            if b is not None:
+                mesh_batches.append(b)
+    total = sum(g.triangle_count for _, g, _ in indexed) + sum(b.triangle_count for b in mesh_batches)
     native.alloc_triangles(total)
     lv0, lv1, lv2, lmat = [], [], [], []
     off, h2d = 0, 0
-    for obj, shape, geo in indexed:
+    for obj, geo, recs in indexed:
         n = geo.triangle_count
         if n == 0:
             continue
@@ -254,8 +319,7 @@ def _extract_on_device(world, native, builder):
         used = np.nonzero(np.bincount(gidx, minlength=len(groups)))[0]
         group_mat = np.zeros(len(groups), np.int32)
         for g in used:
-            rec = TriangleBatch.palette_record(_mat_record(shape.material_for_group(groups[g])))
-            group_mat[g] = builder._add_material(rec)
+            group_mat[g] = builder._add_material(TriangleBatch.palette_record(recs[int(g)]))
         has_n = geo._normals is not None
         native.put_indexed(off, geo._positions, geo._tri_pos_idx, geo._normals if has_n else None,
                            geo._tri_normal_idx if has_n else None, obj.world_matrix.rows,
@@ -263,6 +327,10 @@ def _extract_on_device(world, native, builder):
         h2d += geo._positions.nbytes + geo._tri_pos_idx.nbytes + gidx.nbytes + group_mat.nbytes
         if has_n:
             h2d += geo._normals.nbytes + geo._tri_normal_idx.nbytes
+        if any(_textured(builder, group_mat[g]) for g in used):
+            uv = geo.indexed_uv_arrays()
+            native.put_uvs(off, uv["uv0"], uv["uv1"], uv["uv2"], uv["has_uv"])
+            h2d += sum(a.nbytes for a in uv.values())
         em = [g for g in used if _emissive(builder, group_mat[g])]
         if em:
             sel = np.nonzero(np.isin(gidx, em))[0]
@@ -277,6 +345,9 @@ def _extract_on_device(world, native, builder):
         mat = remap[b.mat_idx]
         native.put_triangles(off, b.v0, b.v1, b.v2, b.n0, b.n1, b.n2, mat)
         h2d += sum(a.nbytes for a in (b.v0, b.v1, b.v2, b.n0, b.n1, b.n2)) + mat.nbytes
+        if any(_textured(builder, k) for k in remap):
+            native.put_uvs(off, b.uv0, b.uv1, b.uv2, b.has_uv)
+            h2d += sum(a.nbytes for a in (b.uv0, b.uv1, b.uv2, b.has_uv))
         sel = np.nonzero([_emissive(builder, k) for k in remap])[0]
         if len(sel):
             rows = np.nonzero(np.isin(b.mat_idx, sel))[0]
@@ -290,38 +361,55 @@ def _extract_on_device(world, native, builder):
     return slots, total, lights, h2d
 
 
+def _upload_textures(native, builder, textures):
+    """Texture images and the palette's texture indices; bytes copied."""
+    if not len(textures):
+        return 0
+    imgs, flips = textures.images()
+    native.set_textures(imgs, flips)
+    native.set_material_textures(builder.palette_textures())
+    return sum(im.nbytes for im in imgs)
+
+
 def build_device_scene(world, method="lbvh", leaf_size=None):
     """Extract `world` to a device scene with a BVH.  method "lbvh" (the
     renderer's) transforms IndexedMesh geometry on the device; "morton" and
     "median" go through GPUBVHBuilder's host flattening so that the
     reference-format tree and ordered arrays stay available."""
+    textures = TextureTable()
     if method != "lbvh":
-        batches, slots = collect(world)
+        batches, slots = collect(world, textures)
         builder = GPUBVHBuilder()
         if leaf_size is not None:
             builder.MAX_LEAF_SIZE = leaf_size
         native = nat.NativeScene()
         native.set_objects(slot_arrays(slots) if slots else None)
         builder.build(batches, method=method, native=native)
+        h2d = _upload_textures(native, builder, textures)
+        b = builder._batch
+        if h2d and b.triangle_count:
+            native.put_uvs(0, b.uv0, b.uv1, b.uv2, b.has_uv)
         stats = {"primitive_count": len(slots), "bvh_nodes": len(builder.nodes),
                  "bvh_triangles": builder.triangle_count,
                  "bvh_materials": len(builder.mat_palette) if batches else 0,
                  "bvh_leaf_size": builder.MAX_LEAF_SIZE if builder.triangle_count else 0}
-        return DeviceScene.from_builder(builder, slots, stats)
+        return DeviceScene.from_builder(builder, slots, stats, h2d_extra=h2d)
     leaf = 4 if leaf_size is None else int(leaf_size)
     native = nat.NativeScene()
     builder = GPUBVHBuilder()  # palette bookkeeping only
-    slots, total, light_tris, h2d = _extract_on_device(world, native, builder)
+    slots, total, light_tris, h2d = _extract_on_device(world, native, builder, textures)
     native.set_objects(slot_arrays(slots) if slots else None)
     pal = builder.palette_arrays()
     native.set_materials(*pal)
+    h2d += _upload_textures(native, builder, textures)
     n_nodes = 0
     if total:
         native.build_bvh(nat.RX_BVH_LBVH_SAH, min(leaf, 15), True)
         n_nodes = native.bvh_info()["n_nodes"]
     stats = {"primitive_count": len(slots), "bvh_nodes": n_nodes, "bvh_triangles": total,
              "bvh_materials": len(builder.mat_palette), "bvh_leaf_size": leaf if total else 0}
-    return DeviceScene(native, slots, stats, light_tris + (pal[0], pal[1], pal[4]), h2d_bytes=h2d)
+    return DeviceScene(native, slots, stats, light_tris + (pal[0], pal[1], pal[4]), h2d_bytes=h2d,
+                       pal_texture=builder.palette_textures())
 
 
 def extract_scene(world, method="lbvh"):

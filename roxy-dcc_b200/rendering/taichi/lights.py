@@ -43,11 +43,14 @@ def _lum(rgb):
     return 0.2126 * rgb[:, 0] + 0.7152 * rgb[:, 1] + 0.0722 * rgb[:, 2]
 
 
-def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, pal_emission, compat):
+def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, pal_emission, compat,
+                 pal_texture=None):
     """Light arrays for rx_scene_set_lights.
 
     slots: reference object-slot dicts; tri_*: triangles in caller order with
-    palette index tri_mat; compat: sphere lights only, uniform pick.
+    palette index tri_mat; compat: sphere lights only, uniform pick;
+    pal_texture: texture index per palette entry — textured emitters are
+    left out (their radiance varies over the surface; BSDF rays find them).
     """
     kinds, p0, p1, p2, alb, em, area = [], [], [], [], [], [], []
     for s in slots:
@@ -70,7 +73,10 @@ def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, p
     if not compat and tri_mat is not None and len(tri_mat):
         pt = np.asarray(pal_type)[tri_mat]
         pe = np.asarray(pal_emission)[tri_mat]
-        sel = np.nonzero((pt == 3) & (pe > 0.0))[0]
+        keep = (pt == 3) & (pe > 0.0)
+        if pal_texture is not None:
+            keep &= np.asarray(pal_texture)[tri_mat] < 0
+        sel = np.nonzero(keep)[0]
         if len(sel):
             a, b, c = tri_v0[sel], tri_v1[sel], tri_v2[sel]
             cr = np.cross((b - a).astype(np.float64), (c - a).astype(np.float64))

@@ -95,6 +95,9 @@ _SIGS = {
     "rx_scene_put_indexed": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p, _i32p, ctypes.c_int,
                               _f64p, _i32p, _f64p, _f64p, _i32p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_scene_get_triangles": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [_f32p] * 6 + [_i32p], ctypes.c_int),
+    "rx_scene_put_uvs": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _i32p], ctypes.c_int),
+    "rx_scene_set_textures": ([ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p, ctypes.c_void_p], ctypes.c_int),
+    "rx_scene_set_material_textures": ([ctypes.c_void_p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_scene_set_materials": ([ctypes.c_void_p, ctypes.c_int, _i32p, _f32p, _f32p, _f32p, _f32p], ctypes.c_int),
     "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p] + [_f32p] * 4,
                              ctypes.c_int),
@@ -281,6 +284,29 @@ class NativeScene:
         self.ctx.check(lib().rx_scene_put_indexed(self.h, int(offset), n, len(pos), dp(pos), iptr(tri),
                                                   0 if nrm is None else len(nrm), dp(nrm), iptr(tn), dp(M), dp(NM),
                                                   iptr(gi), len(gm), iptr(gm)))
+
+    def put_uvs(self, offset, uv0, uv1, uv2, has_uv=None):
+        uv0, uv1, uv2 = (np.ascontiguousarray(a, dtype=np.float32).reshape((-1, 2)) for a in (uv0, uv1, uv2))
+        n = len(uv0)
+        hu = None if has_uv is None else i32(has_uv).reshape(-1)
+        if len(uv1) != n or len(uv2) != n or (hu is not None and len(hu) != n):
+            raise ValueError("uv arrays must all have the same length")
+        self.ctx.check(lib().rx_scene_put_uvs(self.h, int(offset), n, fptr(uv0), fptr(uv1), fptr(uv2), iptr(hu)))
+
+    def set_textures(self, images, flip_v=None):
+        """images: list of (H, W, 3) uint8 arrays."""
+        imgs = [np.ascontiguousarray(im, dtype=np.uint8).reshape((im.shape[0], im.shape[1], 3)) for im in images]
+        n = len(imgs)
+        w = np.array([im.shape[1] for im in imgs], np.int32)
+        h = np.array([im.shape[0] for im in imgs], np.int32)
+        fv = np.zeros(n, np.int32) if flip_v is None else i32(flip_v).reshape(n)
+        texels = np.concatenate([im.reshape(-1) for im in imgs]) if n else np.zeros(0, np.uint8)
+        self.ctx.check(lib().rx_scene_set_textures(self.h, n, iptr(w), iptr(h), iptr(fv),
+                                                   texels.ctypes.data_as(ctypes.c_void_p) if n else None))
+
+    def set_material_textures(self, texture_idx):
+        t = i32(texture_idx).reshape(-1)
+        self.ctx.check(lib().rx_scene_set_material_textures(self.h, len(t), iptr(t)))
 
     def get_triangles(self, offset=0, n=None):
         n = self.n_tris - offset if n is None else int(n)

@@ -112,19 +112,25 @@ class IndexedMesh:
         if normal_matrix is not None:
             tn = self._apply_vector(normal_matrix, tn)
         tn = self._normalize_rows(tn).reshape((n, 3, 3))
+        out = {
+            "v0": tv[:, 0].astype(dtype), "v1": tv[:, 1].astype(dtype), "v2": tv[:, 2].astype(dtype),
+            "n0": tn[:, 0].astype(dtype), "n1": tn[:, 1].astype(dtype), "n2": tn[:, 2].astype(dtype),
+        }
+        out.update(self.indexed_uv_arrays(dtype))
+        out["group_idx"] = self._tri_group_idx.astype(np.int32)
+        out["groups"] = list(self._groups)
+        return out
+
+    def indexed_uv_arrays(self, dtype=np.float32):
+        """uv0..uv2 (T,2) and has_uv (T,) of indexed_triangle_arrays."""
+        n = self.triangle_count
         tuv = np.zeros((n, 3, 2), np.float64)
         if self._uvs is not None:
             ok = np.all(self._tri_uv_idx >= 0, axis=1)
             if np.any(ok):
                 tuv[ok] = self._uvs[self._tri_uv_idx[ok]]
-        return {
-            "v0": tv[:, 0].astype(dtype), "v1": tv[:, 1].astype(dtype), "v2": tv[:, 2].astype(dtype),
-            "n0": tn[:, 0].astype(dtype), "n1": tn[:, 1].astype(dtype), "n2": tn[:, 2].astype(dtype),
-            "uv0": tuv[:, 0].astype(dtype), "uv1": tuv[:, 1].astype(dtype), "uv2": tuv[:, 2].astype(dtype),
-            "has_uv": np.all(self._tri_uv_idx >= 0, axis=1).astype(np.int32),
-            "group_idx": self._tri_group_idx.astype(np.int32),
-            "groups": list(self._groups),
-        }
+        return {"uv0": tuv[:, 0].astype(dtype), "uv1": tuv[:, 1].astype(dtype), "uv2": tuv[:, 2].astype(dtype),
+                "has_uv": np.all(self._tri_uv_idx >= 0, axis=1).astype(np.int32)}
 
     def __repr__(self):
         return f"IndexedMesh(vertices={self.vertex_count}, triangles={self.triangle_count}, groups={len(self._groups)})"

@@ -215,6 +215,10 @@ class Field:
 
     def from_numpy(self, arr):
         arr = np.asarray(arr)
+        if len(self.shape) > 1:
+            # multi-index field (texture texels): keep the dense array
+            self.data = arr.astype(np.uint8 if self.dtype == "u8" else arr.dtype, copy=True)
+            return
         n = arr.shape[0]
         d = {}
         used = n

@@ -152,3 +152,85 @@ def build_indexed_object(ns):
                          translation=ns.Vec3(0.1, -0.2, 0.3), rotation=ns.Vec3(15, -30, 45),
                          scale=ns.Vec3(1.0, 0.5, 2.0), name="indexed")
     return obj
+
+
+def _surface(ns, tris, indexed):
+    """Mesh (Triangle objects) or IndexedMesh of (corners (3,3), uvs (3,2) or
+    None, group) triangle specs."""
+    if not indexed:
+        out = []
+        for c, uv, g in tris:
+            kw = {} if uv is None else dict(uv0=tuple(uv[0]), uv1=tuple(uv[1]), uv2=tuple(uv[2]))
+            out.append(ns.Triangle(*(ns.Vec3(*map(float, p)) for p in c), group=g, **kw))
+        return ns.Mesh(out)
+    groups = []
+    for _, _, g in tris:
+        if g not in groups:
+            groups.append(g)
+    pos = np.concatenate([np.asarray(c, np.float64) for c, _, _ in tris])
+    uvs = np.concatenate([np.asarray(uv if uv is not None else np.zeros((3, 2)), np.float64) for _, uv, _ in tris])
+    faces = np.arange(3 * len(tris), dtype=np.int32).reshape(-1, 3)
+    tri_uv_idx = faces.copy()
+    for k, (_, uv, _) in enumerate(tris):
+        if uv is None:
+            tri_uv_idx[k] = -1
+    return ns.IndexedMesh(pos, faces, uvs=uvs, tri_uv_idx=tri_uv_idx, groups=groups,
+                          tri_group_idx=[groups.index(g) for _, _, g in tris], build_bvh=False)
+
+
+def build_texture_scene(ns, indexed=False):
+    """Textured surfaces (wrapping, flipped, partial and missing uvs, a
+    texture shared by two materials, a textured emitter, an untextured
+    triangle with uvs) plus a sphere light, all as Mesh triangles or all as
+    IndexedMesh (the reference cannot mix the two in one scene)."""
+    rng = np.random.default_rng(60)
+    world = ns.World(use_sky=False, background_color=ns.Color(0.05, 0.05, 0.08))
+    world.add_camera(ns.Camera(position=ns.Vec3(0.5, 0.5, 2.2), forward=ns.Vec3(0, 0, -1),
+                               up=ns.Vec3(0, 1, 0), fov=45, width=64, height=64))
+    tex_a = ns.ImageTexture.from_array(rng.random((5, 7, 3)), flip_v=True)
+    tex_b = ns.ImageTexture.from_array(rng.integers(0, 256, size=(4, 3, 3)).astype(np.float64), flip_v=False)
+
+    # back wall z = 0: 2x2 quads, uvs wrap past 1, one triangle without uvs
+    wall = []
+    groups = ["a", "a", "b", "b", "a", "c", "b", "a"]
+    k = 0
+    for j in range(2):
+        for i in range(2):
+            x0, y0 = 0.5 * i, 0.5 * j
+            quad = [[x0, y0, 0], [x0 + 0.5, y0, 0], [x0 + 0.5, y0 + 0.5, 0], [x0, y0 + 0.5, 0]]
+            for tri in ((0, 1, 2), (0, 2, 3)):
+                c = np.array([quad[t] for t in tri], np.float64)
+                uv = None if k == 5 else c[:, :2] * 2.0 - 0.25
+                wall.append((c, uv, groups[k]))
+                k += 1
+    world.add_object(ns.SceneObject(shapes=[ns.Shape(_surface(ns, wall, indexed), {
+        "a": ns.Diffuse(ns.Color(0.9, 0.8, 0.7), albedo_texture=tex_a),
+        "b": ns.Glossy(ns.Color(0.7, 0.9, 0.8), roughness=0.4, albedo_texture=tex_b),
+        "c": ns.Diffuse(ns.Color(0.6, 0.6, 0.6))})], name="wall"))
+    # floor y = 0 (metal sharing texture b, diffuse sharing texture a)
+    floor = [(np.array([[0, 0, 0], [1, 0, 0], [1, 0, 1]], np.float64), np.array([[0, 0], [3, 0], [3, 3]]), "f"),
+             (np.array([[0, 0, 0], [1, 0, 1], [0, 0, 1]], np.float64), np.array([[0, 0], [3, 3], [0, 3]]), "g")]
+    world.add_object(ns.SceneObject(shapes=[ns.Shape(_surface(ns, floor, indexed), {
+        "f": ns.Metal(ns.Color(0.8, 0.8, 0.8), roughness=0.2, albedo_texture=tex_b),
+        "g": ns.Diffuse(ns.Color(0.5, 0.7, 0.9), albedo_texture=tex_a)})], name="floor"))
+    # textured emitter and an untextured triangle that carries uvs
+    lamp = [(np.array([[0.2, 0.7, 0.3], [0.45, 0.7, 0.3], [0.2, 0.95, 0.3]]),
+             np.array([[0.1, 0.1], [0.9, 0.1], [0.1, 0.9]]), "e"),
+            (np.array([[0.6, 0.2, 0.4], [0.9, 0.2, 0.4], [0.6, 0.5, 0.4]]),
+             np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]]), "p")]
+    world.add_object(ns.SceneObject(shapes=[ns.Shape(_surface(ns, lamp, indexed), {
+        "e": ns.Emissive(ns.Color(1.0, 0.9, 0.8), intensity=4.0, albedo_texture=tex_a),
+        "p": ns.Diffuse(ns.Color(0.3, 0.8, 0.3))})], name="lamp"))
+    world.add_object(ns.SceneObject(shape=ns.Sphere(0.05), material=ns.Emissive(ns.Color(1, 1, 1), intensity=10.0),
+                                    translation=ns.Vec3(0.5, 0.85, 0.6), name="bulb"))
+    return world
+
+
+def texture_rays(n, seed):
+    """Camera-like rays from (0.5, 0.5, 2.2) towards the textured wall and floor."""
+    rng = np.random.default_rng(seed)
+    ro = np.tile(np.array([0.5, 0.5, 2.2], dtype=np.float32), (n, 1))
+    tgt = rng.uniform([0.02, -0.3, 0.0], [0.98, 0.98, 0.0], size=(n, 3))
+    d = tgt - ro.astype(np.float64)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return ro, d.astype(np.float32)

@@ -52,6 +52,7 @@ def _ns():
         setattr(ns, name, getattr(scene, name))
     ns.Emissive = Emissive
     ns.Glossy = Glossy
+    ns.ImageTexture = scene.ImageTexture
     return ns
 
 
@@ -241,6 +242,118 @@ def make_trace_scene(out_dir):
 
     world = gs.build_trace_scene(_ns())
     stats = extract_scene(world)
+    out = _dump_scene(F, stats)
+    # scene_intersect on camera-like rays
+    ro, rd = gs.trace_rays(300, seed=41)
+    si = {"t": [], "idx": [], "is_bvh": [], "u": [], "v": [], "normal": []}
+    for i in range(len(ro)):
+        t, nrm, idx, is_bvh, _mat, u, v = isect.scene_intersect(ti.Vector(ro[i]), ti.Vector(rd[i]))
+        si["t"].append(np.float32(t)); si["idx"].append(int(idx)); si["is_bvh"].append(int(is_bvh))
+        si["u"].append(np.float32(u)); si["v"].append(np.float32(v)); si["normal"].append(nrm.to_list())
+    out.update({"si_ro": ro, "si_rd": rd})
+    out.update({f"si_{k}": np.array(v, np.float32 if k in ("t", "u", "v", "normal") else np.int32)
+                for k, v in si.items()})
+    out.update(_scripted_traces(trace_mod, gs.trace_rays(96, seed=42), seed=43,
+                                configs=[(6, 0, 0, 1), (6, 0, 1, 3), (8, 1, 0, 8), (1, 0, 0, 0)]))
+    np.savez_compressed(os.path.join(out_dir, "trace_scene.npz"), **out)
+
+    # IndexedMesh flattening (scene/mesh.py:397-430 via extractor.py:174-191)
+    obj = gs.build_indexed_object(_ns())
+    geo = obj.shapes[0].geometry
+    arrs = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
+    np.savez_compressed(os.path.join(out_dir, "indexed_arrays.npz"),
+                        **{k: np.asarray(v) for k, v in arrs.items() if k != "groups"},
+                        world_matrix=np.array(obj.world_matrix.rows, np.float64),
+                        world_inverse=np.array(obj.world_inverse_matrix.rows, np.float64))
+    print(f"trace_scene.npz: stats={list(out['stats'])}")
+
+
+def _scripted_traces(trace_mod, rays, seed, configs):
+    """trace() with scripted ti.random() streams, per (max_depth, use_sky,
+    direct_light_mode, direct_light_max_depth) config and ray."""
+    import taichi as ti
+    counter = ti.CounterField()
+    trace_mod._ray_count = counter
+    tro, trd = rays
+    rng = np.random.default_rng(seed)
+    recs = {k: [] for k in ("color", "normal", "albedo", "depth", "consumed", "rays", "cfg")}
+    streams = []
+    bg = ti.Vector([0.05, 0.05, 0.08])
+    for ci, (md, sky, mode, dlmd) in enumerate(configs):
+        for i in range(len(tro)):
+            stream = rng.random(512).astype(np.float32)
+            ti.set_random_stream(stream)
+            counter.value = 0
+            color, nrm, alb, dep = trace_mod.trace(ti.Vector(tro[i]), ti.Vector(trd[i]), md, sky, bg,
+                                                   mode, dlmd, 1)
+            recs["color"].append(color.to_list()); recs["normal"].append(nrm.to_list())
+            recs["albedo"].append(alb.to_list()); recs["depth"].append(float(dep))
+            recs["consumed"].append(ti.consumed()); recs["rays"].append(counter.value)
+            recs["cfg"].append(ci)
+            streams.append(stream)
+    out = {"tr_ro": np.tile(tro, (len(configs), 1)), "tr_rd": np.tile(trd, (len(configs), 1)),
+           "tr_stream": np.array(streams, np.float32), "tr_configs": np.array(configs, np.int32),
+           "tr_bg": np.array([0.05, 0.05, 0.08], np.float32)}
+    for k, v in recs.items():
+        out[f"tr_{k}"] = np.array(v, np.float32 if k in ("color", "normal", "albedo", "depth") else np.int32)
+    return out
+
+
+def make_texture_scene(out_dir):
+    for indexed, name in ((False, "texture_scene.npz"), (True, "texture_scene_indexed.npz")):
+        _make_texture_scene(out_dir, indexed, name)
+
+
+def _make_texture_scene(out_dir, indexed, name):
+    """Textured scene: extract_scene's uv / texture fields, _sample_texture,
+    _bvh_albedo and trace() with scripted random streams."""
+    import taichi as ti
+    import rendering.taichi.fields as F
+    import rendering.taichi.trace  # noqa: F401
+    trace_mod = sys.modules["rendering.taichi.trace"]
+    from rendering.taichi.extractor import extract_scene
+    import golden_scenes as gs
+
+    world = gs.build_texture_scene(_ns(), indexed=indexed)
+    stats = extract_scene(world)
+    out = _dump_scene(F, stats)
+    n_tris = int(F._bvh_n_tris[None])
+    n_mats = int(F._mat_n_mats[None])
+    n_tex = int(F._tex_n[None])
+    out.update({"uv0": _dump_field(F._bvh_uv0, n_tris, 2), "uv1": _dump_field(F._bvh_uv1, n_tris, 2),
+                "uv2": _dump_field(F._bvh_uv2, n_tris, 2),
+                "has_uv": _dump_field(F._bvh_has_uv, n_tris, dtype=np.int32),
+                "mat_texture": _dump_field(F._mat_texture, n_mats, dtype=np.int32),
+                "tex_w": _dump_field(F._tex_width, n_tex, dtype=np.int32),
+                "tex_h": _dump_field(F._tex_height, n_tex, dtype=np.int32),
+                "tex_flip": _dump_field(F._tex_flip_v, n_tex, dtype=np.int32)})
+    for i in range(n_tex):
+        out[f"tex{i}"] = np.array(F._tex_pixels.data[i, :out["tex_h"][i], :out["tex_w"][i]], np.uint8)
+    # _sample_texture over wrapped, negative and edge uvs
+    rng = np.random.default_rng(61)
+    uv = rng.uniform(-2.5, 2.5, size=(300, 2)).astype(np.float32)
+    uv[:8] = [[0, 0], [1, 1], [0.999999, 0.5], [-1e-7, 0.25], [0.5, -0.0], [2.0, -3.0], [0.25, 0.75],
+              [-0.5, 1.5]]
+    samp = []
+    for t in range(n_tex):
+        samp.append([trace_mod._sample_texture(t, ti.Vector(list(x))).to_list() for x in uv])
+    out["st_uv"] = uv
+    out["st_out"] = np.array(samp, np.float32)
+    # _bvh_albedo on every BVH triangle at seeded barycentrics
+    bu = rng.uniform(0, 0.5, n_tris).astype(np.float32)
+    bv = rng.uniform(0, 0.5, n_tris).astype(np.float32)
+    ba = []
+    for i in range(n_tris):
+        m = int(F._bvh_mat_idx[i])
+        ba.append(trace_mod._bvh_albedo(i, m, bu[i], bv[i], F._mat_albedo[m]).to_list())
+    out.update({"ba_u": bu, "ba_v": bv, "ba_out": np.array(ba, np.float32)})
+    out.update(_scripted_traces(trace_mod, gs.texture_rays(80, seed=62), seed=63,
+                                configs=[(6, 0, 0, 1), (5, 1, 1, 3)]))
+    np.savez_compressed(os.path.join(out_dir, name), **out)
+    print(f"{name}: stats={list(out['stats'])} textures={n_tex}")
+
+
+def _dump_scene(F, stats):
     n_obj = int(F._n_objects[None])
     n_nodes = int(F._bvh_n_nodes[None])
     n_tris = int(F._bvh_n_tris[None])
@@ -284,58 +397,7 @@ def make_trace_scene(out_dir):
         "mat_ior": _dump_field(F._mat_ior, n_mats),
         "mat_emission": _dump_field(F._mat_emission, n_mats),
     }
-    # scene_intersect on camera-like rays
-    ro, rd = gs.trace_rays(300, seed=41)
-    si = {"t": [], "idx": [], "is_bvh": [], "u": [], "v": [], "normal": []}
-    for i in range(len(ro)):
-        t, nrm, idx, is_bvh, _mat, u, v = isect.scene_intersect(ti.Vector(ro[i]), ti.Vector(rd[i]))
-        si["t"].append(np.float32(t)); si["idx"].append(int(idx)); si["is_bvh"].append(int(is_bvh))
-        si["u"].append(np.float32(u)); si["v"].append(np.float32(v)); si["normal"].append(nrm.to_list())
-    out.update({"si_ro": ro, "si_rd": rd})
-    out.update({f"si_{k}": np.array(v, np.float32 if k in ("t", "u", "v", "normal") else np.int32)
-                for k, v in si.items()})
-
-    # trace() with scripted random streams
-    counter = ti.CounterField()
-    trace_mod._ray_count = counter
-    tro, trd = gs.trace_rays(96, seed=42)
-    rng = np.random.default_rng(43)
-    configs = [
-        # (max_depth, use_sky, direct_light_mode, direct_light_max_depth)
-        (6, 0, 0, 1), (6, 0, 1, 3), (8, 1, 0, 8), (1, 0, 0, 0),
-    ]
-    recs = {k: [] for k in ("color", "normal", "albedo", "depth", "consumed", "rays", "cfg")}
-    streams = []
-    bg = ti.Vector([0.05, 0.05, 0.08])
-    for ci, (md, sky, mode, dlmd) in enumerate(configs):
-        for i in range(len(tro)):
-            stream = rng.random(512).astype(np.float32)
-            ti.set_random_stream(stream)
-            counter.value = 0
-            color, nrm, alb, dep = trace_mod.trace(ti.Vector(tro[i]), ti.Vector(trd[i]), md, sky, bg,
-                                                   mode, dlmd, 1)
-            recs["color"].append(color.to_list()); recs["normal"].append(nrm.to_list())
-            recs["albedo"].append(alb.to_list()); recs["depth"].append(float(dep))
-            recs["consumed"].append(ti.consumed()); recs["rays"].append(counter.value)
-            recs["cfg"].append(ci)
-            streams.append(stream)
-    out.update({"tr_ro": np.tile(tro, (len(configs), 1)), "tr_rd": np.tile(trd, (len(configs), 1)),
-                "tr_stream": np.array(streams, np.float32),
-                "tr_configs": np.array(configs, np.int32),
-                "tr_bg": np.array([0.05, 0.05, 0.08], np.float32)})
-    for k, v in recs.items():
-        out[f"tr_{k}"] = np.array(v, np.float32 if k in ("color", "normal", "albedo", "depth") else np.int32)
-    np.savez_compressed(os.path.join(out_dir, "trace_scene.npz"), **out)
-
-    # IndexedMesh flattening (scene/mesh.py:397-430 via extractor.py:174-191)
-    obj = gs.build_indexed_object(_ns())
-    geo = obj.shapes[0].geometry
-    arrs = geo.indexed_triangle_arrays(obj.world_matrix, obj.world_inverse_transpose_matrix)
-    np.savez_compressed(os.path.join(out_dir, "indexed_arrays.npz"),
-                        **{k: np.asarray(v) for k, v in arrs.items() if k != "groups"},
-                        world_matrix=np.array(obj.world_matrix.rows, np.float64),
-                        world_inverse=np.array(obj.world_inverse_matrix.rows, np.float64))
-    print(f"trace_scene.npz: objects={n_obj} nodes={n_nodes} tris={n_tris} mats={n_mats} lights={n_lights}")
+    return out
 
 
 def make_denoise(out_dir):
@@ -401,12 +463,12 @@ def main():
         raise SystemExit("usage: make_golden.py <reference checkout>")
     _setup(ref_root)
     np.seterr(all="ignore")
-    make_bvh(HERE)
-    make_denoise(HERE)
-    make_sampling(HERE)
-    make_prims(HERE)
-    make_traversal(HERE)
-    make_trace_scene(HERE)
+    makers = [make_bvh, make_denoise, make_sampling, make_prims, make_traversal, make_trace_scene,
+              make_texture_scene]
+    only = sys.argv[2:]  # optional generator names, e.g. make_texture_scene
+    for fn in makers:
+        if not only or fn.__name__ in only:
+            fn(HERE)
 
 
 if __name__ == "__main__":

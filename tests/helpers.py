@@ -18,6 +18,9 @@ def oracle_scene(host, compat):
         kw = dict(node_min=bvh["node_min"], node_max=bvh["node_max"], left=bvh["left"], right=bvh["right"],
                   start=bvh["start"], count=bvh["count"], v0=b.v0[o], v1=b.v1[o], v2=b.v2[o], n0=b.n0[o],
                   n1=b.n1[o], n2=b.n2[o], tri_mat=host.mat_idx[o])
+        if host.textures:
+            kw.update(uv0=b.uv0[o], uv1=b.uv1[o], uv2=b.uv2[o], has_uv=b.has_uv[o], mat_texture=host.mat_texture,
+                      textures=host.textures, tex_flip=host.tex_flip)
     pt, pa, pr, pi, pe = host.palette
     objects = None
     if host.slots:

@@ -96,11 +96,13 @@ def _mixed_world():
     return world
 
 
-@pytest.mark.parametrize("name", ["trace", "mixed", "cornell", "icosphere"])
+@pytest.mark.parametrize("name", ["trace", "mixed", "cornell", "icosphere", "texture", "texture_indexed"])
 def test_device_extraction_equals_host_flattening(name):
     world = {"trace": lambda: gs.build_trace_scene(_ns()), "mixed": _mixed_world,
              "cornell": lambda: workloads.cornell_box(64, 64),
-             "icosphere": lambda: workloads.displaced_icosphere_scene(64, 36, subdiv=4)}[name]()
+             "icosphere": lambda: workloads.displaced_icosphere_scene(64, 36, subdiv=4),
+             "texture": lambda: gs.build_texture_scene(_ns()),
+             "texture_indexed": lambda: gs.build_texture_scene(_ns(), indexed=True)}[name]()
     ds = build_device_scene(world, method="lbvh")
     h = HostScene(world)
     got = ds.native.get_triangles()
@@ -111,10 +113,11 @@ def test_device_extraction_equals_host_flattening(name):
     pal = ds._light_args[4:]
     np.testing.assert_array_equal(pal[0], h.palette[0])
     assert _bits_equal(pal[1], h.palette[1]) and _bits_equal(pal[2], h.palette[4])
+    np.testing.assert_array_equal(ds.pal_texture, h.mat_texture)
     assert ds.stats["bvh_triangles"] == b.triangle_count
     assert ds.stats["bvh_materials"] == len(h.builder.mat_palette)
     for compat in (False, True):
-        a = build_lights(ds.slots, *ds._light_args, compat=compat)
+        a = build_lights(ds.slots, *ds._light_args, compat=compat, pal_texture=ds.pal_texture)
         r = h.lights(compat)
         assert (a is None) == (r is None)
         if a is not None:

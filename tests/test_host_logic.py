@@ -26,7 +26,7 @@ def _ns():
     ns = NS()
     ns.Vec3, ns.Color = core.Vec3, core.Color
     for n in ("World", "Camera", "SceneObject", "Sphere", "Plane", "Cube", "Mesh", "Triangle", "IndexedMesh",
-              "Diffuse", "Metal", "Dielectric", "Shape", "Emissive", "Glossy"):
+              "Diffuse", "Metal", "Dielectric", "Shape", "Emissive", "Glossy", "ImageTexture"):
         setattr(ns, n, getattr(scene, n))
     return ns
 
@@ -130,6 +130,44 @@ def test_trace_scene_flattening_matches_reference_extract():
     lights = h.lights(compat=True)
     np.testing.assert_allclose(lights["p0"], g["light_center"], rtol=1e-6)
     np.testing.assert_allclose(lights["p1"][:, 0], g["light_radius"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("indexed", [False, True])
+def test_texture_scene_flattening_matches_reference_extract(indexed):
+    """Texture table (order, u8 pixels, flips), palette texture indices and
+    BVH-ordered uvs equal extract_scene's fields."""
+    g = np.load(os.path.join(GOLD, "texture_scene_indexed.npz" if indexed else "texture_scene.npz"))
+    h = HostScene(gs.build_texture_scene(_ns(), indexed=indexed))
+    assert len(h.textures) == len(g["tex_w"])
+    for i, im in enumerate(h.textures):
+        np.testing.assert_array_equal(im, g[f"tex{i}"])
+    np.testing.assert_array_equal(h.tex_flip, g["tex_flip"])
+    np.testing.assert_array_equal(h.mat_texture, g["mat_texture"])
+    np.testing.assert_array_equal(h.palette[0], g["mat_type"])
+    bvh = oracle.bvh_build_morton(h.batch.v0, h.batch.v1, h.batch.v2, 8)
+    o = bvh["order"]
+    for k in ("v0", "v1", "v2", "n0", "n1", "n2", "uv0", "uv1", "uv2", "has_uv"):
+        np.testing.assert_array_equal(getattr(h.batch, k)[o], g[k], err_msg=k)
+    np.testing.assert_array_equal(h.mat_idx[o], g["tri_mat"])
+    # the textured emitter is not an explicit light
+    lights = h.lights(compat=False)
+    assert int(np.sum(lights["kind"] == 1)) == 0
+
+
+def test_texture_table_limits():
+    from rendering.taichi.extractor import MAX_TEXTURES, TextureTable
+    ns = _ns()
+    table = TextureTable()
+    mats = [ns.Diffuse(ns.Color(1, 1, 1), albedo_texture=ns.ImageTexture.from_array(np.ones((2, 2, 3))))
+            for _ in range(MAX_TEXTURES)]
+    assert [table.index(m) for m in mats] == list(range(MAX_TEXTURES))
+    assert table.index(mats[3]) == 3 and table.index(ns.Diffuse(ns.Color(1, 1, 1))) == -1
+    with pytest.raises(ValueError, match="more than 8 image textures"):
+        table.index(ns.Diffuse(ns.Color(1, 1, 1), albedo_texture=ns.ImageTexture.from_array(np.ones((2, 2, 3)))))
+    with pytest.raises(ValueError, match="needs either a path or pixel array"):
+        ns.ImageTexture()
+    with pytest.raises(RuntimeError, match="pygame"):
+        ns.ImageTexture(path="x.png").load_pixels_u8()
 
 
 def test_alias_table_reproduces_distribution():

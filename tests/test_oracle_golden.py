@@ -124,6 +124,60 @@ def test_trace_loop_matches_reference_trace_with_scripted_randoms():
     assert worst < 1e-4
 
 
+def texture_scene_oracle(g):
+    textures = [g[f"tex{i}"] for i in range(len(g["tex_w"]))]
+    return oracle.Scene(node_min=g["node_min"], node_max=g["node_max"], left=g["left"], right=g["right"],
+                        start=g["start"], count=g["count"], v0=g["v0"], v1=g["v1"], v2=g["v2"], n0=g["n0"],
+                        n1=g["n1"], n2=g["n2"], tri_mat=g["tri_mat"], mat_type=g["mat_type"],
+                        mat_albedo=g["mat_albedo"], mat_roughness=g["mat_roughness"], mat_ior=g["mat_ior"],
+                        mat_emission=g["mat_emission"],
+                        objects={k[4:]: g[k] for k in g.files if k.startswith("obj_")},
+                        lights=_golden_lights(g), uv0=g["uv0"], uv1=g["uv1"], uv2=g["uv2"], has_uv=g["has_uv"],
+                        mat_texture=g["mat_texture"], textures=textures, tex_flip=g["tex_flip"])
+
+
+def _golden_lights(g):
+    nl = len(g["light_radius"])
+    return dict(kind=np.zeros(nl, np.int32), p0=g["light_center"],
+                p1=np.stack([g["light_radius"], np.zeros(nl), np.zeros(nl)], 1),
+                p2=np.zeros((nl, 3)), albedo=g["light_albedo"], emission=g["light_emission"],
+                area=np.zeros(nl), pick_pdf=np.full(nl, 1.0 / max(nl, 1)), alias_prob=np.ones(nl),
+                alias_idx=np.arange(nl), obj=np.zeros(nl))
+
+
+@pytest.mark.parametrize("name", ["texture_scene.npz", "texture_scene_indexed.npz"])
+def test_texture_sampling_matches_reference(name):
+    """_sample_texture and _bvh_albedo of the restatement equal the
+    reference's float32 results bit for bit."""
+    g = _load(name)
+    sc = texture_scene_oracle(g)
+    for t in range(len(g["tex_w"])):
+        out = oracle.sample_texture(sc, t, g["st_uv"])
+        assert np.array_equal(out.view(np.uint32), g["st_out"][t].view(np.uint32)), t
+    n = len(g["tri_mat"])
+    out = oracle.bvh_albedo(sc, np.arange(n), g["tri_mat"], g["ba_u"], g["ba_v"], g["mat_albedo"][g["tri_mat"]])
+    assert np.array_equal(out.view(np.uint32), g["ba_out"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["texture_scene.npz", "texture_scene_indexed.npz"])
+def test_textured_trace_matches_reference_trace_with_scripted_randoms(name):
+    g = _load(name)
+    sc = texture_scene_oracle(g)
+    cfgs = g["tr_configs"]
+    for i in range(len(g["tr_cfg"])):
+        md, sky, mode, dlmd = (int(x) for x in cfgs[g["tr_cfg"][i]])
+        p = oracle.make_params(64, 64, 1.0, 1.0, [0, 0, 0], [0, 0, -1], [1, 0, 0], [0, 1, 0], md, sky,
+                               g["tr_bg"], direct_light_mode=mode, direct_light_max_depth=dlmd,
+                               reference_compat=1)
+        r = oracle.trace_scripted(sc, p, g["tr_ro"][i:i + 1], g["tr_rd"][i:i + 1], g["tr_stream"][i])
+        assert r["consumed"] == g["tr_consumed"][i], i
+        assert r["rays"] == g["tr_rays"][i], i
+        for key in ("color", "normal", "albedo"):
+            ref = g[f"tr_{key}"][i]
+            err = np.max(np.abs(r[key] - ref) / (np.abs(ref) + 1e-3))
+            assert err < 1e-4, (i, key, r[key], ref)
+
+
 def test_denoise_restatement_matches_reference():
     g = _load("denoise.npz")
     for case in g["case_names"]:

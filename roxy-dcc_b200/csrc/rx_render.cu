@@ -806,8 +806,8 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
   if (rc) return rc;
   // Paths per wavefront.  Each extend launch ends in a tail where the last,
   // longest rays run on an emptying GPU; larger waves amortise it (measured on
-  // the 1080p icosphere scene: 4 M paths -> 86 ms of extend per 64-spp frame,
-  // 32 M -> 36 ms).  32 M paths hold ~5.4 GB of path state.
+  // the 1080p 64-spp icosphere scene: 16 M paths -> 43.7 ms of extend per
+  // frame, 32 M -> 35.8 ms).  32 M paths hold ~5.4 GB of path state.
   long long target = p->wave_paths > 0 ? p->wave_paths : (1LL << 25);
   int spf = (int)std::max<long long>(1, std::min<long long>(frames, target / std::max<long long>(a->P, 1)));
   long long cap = (long long)spf * a->P;

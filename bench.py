@@ -294,6 +294,16 @@ def run_ours(args):
         except (OSError, ValueError, KeyError):
             traffic = None
 
+    # -- image error of the timed render against a float64 high-spp render ------
+    quality = None
+    if args.ref_spp > 0:
+        from rendering.quality import reference_render, rel_mse
+        t_ref = time.perf_counter()
+        ref = reference_render(ds.native, params, args.ref_spp, ctx=ctx)
+        quality = {"relmse": rel_mse(acc.read(nat.RX_ACC_RADIANCE), ref), "spp": w["spp"],
+                   "ref_spp": args.ref_spp, "ref": "float64-accumulated render, independent seed, same clamp",
+                   "ref_render_s": time.perf_counter() - t_ref}
+
     # -- end to end through TaichiRenderer ------------------------------------
     img = Image(W, H)
     r = TaichiRenderer(world, img, None, samples=w["spp"], max_depth=w["max_depth"],
@@ -336,6 +346,7 @@ def run_ours(args):
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
                                        "algorithmic_bytes_per_ray": 272, "ms_per_step": shade_ms}},
                 "clocks": clocks.summary(),
+                "quality": quality,
                 "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "path": "TaichiRenderer.render(): extract + H2D + GPU BVH build + render + D2H image"},
                 "cpu_baseline": cb and {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}}
@@ -369,6 +380,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-spp", type=int, default=4096,
+                    help="spp of the float64 reference render for relMSE (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

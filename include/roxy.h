@@ -209,6 +209,12 @@ int rx_accum_set_timing(rx_accum* acc, int on);
 /* ms of the last render, ms per kernel class (extend, shade, connect, other)
  * and the number of kernel launches it made. */
 int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
+/* Float64 sums of the clamped sample radiance next to the float32 running
+ * means, for high-spp reference renders (no reference counterpart: the
+ * reference accumulates in float32 only, trace.py:262-283).  Enable on a
+ * reset accumulator; rx_accum_read_f64 writes the float64 mean (H,W,3). */
+int rx_accum_set_f64(rx_accum* acc, int on);
+int rx_accum_read_f64(rx_accum* acc, double* host_out);
 
 /* edge_aware_denoise / a-trous on caller host buffers (denoise.py:23-104):
  * color (H,W,3); normal, albedo (H,W,3) and depth (H,W) may be NULL. */

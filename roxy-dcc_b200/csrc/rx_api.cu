@@ -677,6 +677,20 @@ int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int 
   return accum_last_timing(acc->a, ms_total, ms_kernels, n_kernels, launches);
 }
 
+int rx_accum_set_f64(rx_accum* acc, int on) {
+  if (!acc) return RX_ERR_ARG;
+  LOCK(acc->ctx);
+  cudaSetDevice(acc->ctx->device);
+  return accum_set_f64(acc->a, on);
+}
+
+int rx_accum_read_f64(rx_accum* acc, double* host_out) {
+  if (!acc || !host_out) return RX_ERR_ARG;
+  LOCK(acc->ctx);
+  cudaSetDevice(acc->ctx->device);
+  return accum_read_f64(acc->a, host_out);
+}
+
 int rx_denoise(rx_ctx* ctx, int height, int width, const float* color, const float* normal, const float* albedo,
                const float* depth, const rx_denoise_params* params, float* out) {
   if (!ctx || !params) return set_error(nullptr, "rx_denoise: NULL argument"), RX_ERR_ARG;

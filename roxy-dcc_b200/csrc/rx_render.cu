@@ -519,11 +519,12 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
 __global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, const float4* __restrict__ rad,
                              const float4* __restrict__ gn, const float4* __restrict__ ga,
                              float4* __restrict__ acc_r, float4* __restrict__ acc_n, float4* __restrict__ acc_a,
-                             float4* __restrict__ pixels) {
+                             float4* __restrict__ pixels, double* __restrict__ acc64) {
   int fb = *frame_base;
   for (long long pix = blockIdx.x * (long long)blockDim.x + threadIdx.x; pix < K.P;
        pix += (long long)gridDim.x * blockDim.x) {
     float4 a = acc_r[pix], an = acc_n[pix], aa = acc_a[pix];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
     for (int f = 0; f < K.spf; ++f) {
       long long p = (long long)f * K.P + pix;
       float4 s = rad[p];
@@ -532,6 +533,9 @@ __global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, cons
         s.y = fminf(fmaxf(s.y, 0.0f), K.clamp);
         s.z = fminf(fmaxf(s.z, 0.0f), K.clamp);
       }
+      sx += (double)s.x;
+      sy += (double)s.y;
+      sz += (double)s.z;
       float4 g = gn[p], al = ga[p];
       int frame = fb + f;
       if (frame == 0) {
@@ -549,6 +553,12 @@ __global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, cons
     acc_r[pix] = a;
     acc_n[pix] = an;
     acc_a[pix] = aa;
+    if (acc64) {
+      // float64 sums of the clamped samples (reference renders for relMSE)
+      acc64[3 * pix] += sx;
+      acc64[3 * pix + 1] += sy;
+      acc64[3 * pix + 2] += sz;
+    }
     pixels[pix] = make_float4(sqrtf(fminf(a.x, 1.0f)), sqrtf(fminf(a.y, 1.0f)), sqrtf(fminf(a.z, 1.0f)), 0.0f);
   }
 }
@@ -582,6 +592,7 @@ struct Accum {
   int W = 0, H = 0;
   long long P = 0;
   DevBuf<float4> acc_r, acc_n, acc_a, pixels;
+  DevBuf<double> acc64;  // optional float64 radiance sums (3 per pixel)
   DevBuf<int> frame_base;
   DevBuf<unsigned long long> rays;
   int frames = 0;
@@ -644,6 +655,7 @@ int accum_reset(Accum* a) {
   cudaMemsetAsync(a->acc_n.p, 0, a->acc_n.bytes(), st);
   cudaMemsetAsync(a->acc_a.p, 0, a->acc_a.bytes(), st);
   cudaMemsetAsync(a->pixels.p, 0, a->pixels.bytes(), st);
+  if (a->acc64.p) cudaMemsetAsync(a->acc64.p, 0, a->acc64.bytes(), st);
   cudaMemsetAsync(a->frame_base.p, 0, sizeof(int), st);
   cudaMemsetAsync(a->rays.p, 0, sizeof(unsigned long long), st);
   a->frames = 0;
@@ -741,7 +753,7 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   }
   int ablocks = (int)std::min<long long>((K.P + 255) / 256, (long long)ctx->num_sms * 16);
   k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->rad.p, a->gn.p, a->ga.p, a->acc_r.p,
-                                                      a->acc_n.p, a->acc_a.p, a->pixels.p);
+                                                      a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p);
   k_finish<<<1, 1, 0, st>>>(a->counters.p, K.max_depth, a->frame_base.p, a->rays.p, K.spf);
   launches += 2;
   mark(K_OTHER);
@@ -905,6 +917,37 @@ int accum_read(Accum* a, int which, float* host_out) {
   k_pack<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(a->P, src, comp, tmp.p);
   CUDA_TRY(ctx, cudaMemcpyAsync(host_out, tmp.p, tmp.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RX_OK;
+}
+
+int accum_set_f64(Accum* a, int on) {
+  Ctx* ctx = a->ctx;
+  if (on && !a->acc64.p) {
+    if (a->frames != 0)
+      return set_error(ctx, "accum_set_f64: enable float64 sums before the first frame (reset first)"),
+             RX_ERR_ARG;
+    if (!a->acc64.alloc(ctx, 3 * (size_t)a->P))
+      return set_error(ctx, "accum_set_f64: out of device memory"), RX_ERR_CAPACITY;
+    CUDA_TRY(ctx, cudaMemsetAsync(a->acc64.p, 0, a->acc64.bytes(), ctx->stream));
+  } else if (!on) {
+    a->acc64.release();
+  }
+  a->drop_graph();  // k_accumulate's arguments changed
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RX_OK;
+}
+
+int accum_read_f64(Accum* a, double* host_out) {
+  Ctx* ctx = a->ctx;
+  if (!a->acc64.p) return set_error(ctx, "accum_read_f64: float64 sums are not enabled"), RX_ERR_ARG;
+  int fb = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&fb, a->frame_base.p, sizeof(fb), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(host_out, a->acc64.p, a->acc64.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (fb > 0) {
+    double inv = 1.0 / (double)fb;
+    for (size_t i = 0; i < a->acc64.n; ++i) host_out[i] *= inv;
+  }
   return RX_OK;
 }
 

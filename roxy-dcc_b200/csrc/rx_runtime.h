@@ -204,6 +204,8 @@ int accum_info(Accum* a, int* w, int* h, int* frames, long long* rays);
 int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out);
 int accum_set_timing(Accum* a, int on);
 int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
+int accum_set_f64(Accum* a, int on);
+int accum_read_f64(Accum* a, double* host_out);
 
 // Denoise on caller buffers (rx_denoise.cu)
 int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal, const float* albedo,

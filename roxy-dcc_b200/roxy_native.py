@@ -123,6 +123,8 @@ _SIGS = {
     "rx_accum_denoise": ([ctypes.c_void_p, ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_accum_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_accum_last_timing": ([ctypes.c_void_p, _f32p, _f32p, ctypes.c_int, _i32p], ctypes.c_int),
+    "rx_accum_set_f64": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_accum_read_f64": ([ctypes.c_void_p, _f64p], ctypes.c_int),
     "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_denoise_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -467,6 +469,15 @@ class Accumulator:
         self.ctx.check(lib().rx_accum_last_timing(self.h, ctypes.byref(tot), ks, 4, ctypes.byref(nl)))
         return dict(total_ms=tot.value, extend_ms=ks[0], shade_ms=ks[1], connect_ms=ks[2], other_ms=ks[3],
                     launches=nl.value)
+
+    def set_f64(self, on):
+        """Keep float64 sums of the clamped sample radiance (reset first)."""
+        self.ctx.check(lib().rx_accum_set_f64(self.h, int(bool(on))))
+
+    def read_f64(self):
+        out = np.zeros((self.height, self.width, 3), np.float64)
+        self.ctx.check(lib().rx_accum_read_f64(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     def close(self):
         if getattr(self, "h", None) is not None and _LIB is not None:

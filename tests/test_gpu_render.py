@@ -230,3 +230,34 @@ def test_progressive_accumulation_equals_one_shot():
         b.render(ds.native, p, k)
     np.testing.assert_array_equal(a.read(nat.RX_ACC_RADIANCE), b.read(nat.RX_ACC_RADIANCE))
     assert a.info()["rays"] == b.info()["rays"] and b.info()["frames"] == 12
+
+
+def test_float64_reference_accumulation_and_relmse():
+    """float64 sums agree with the float32 running means, a float64 render
+    keeps its f32 outputs unchanged, and relMSE falls roughly as 1/spp."""
+    from rendering.quality import reference_render, rel_mse
+    world = workloads.cornell_box(64, 64)
+    ds = build_device_scene(world)
+    ds.use_lights(False)
+    cam = world.active_camera
+    p = make_params(64, 64, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 8, world._use_sky, 0, 8, 10.0,
+                    list(world._background_color), list(cam.position), list(cam.forward), list(cam.right),
+                    list(cam.up), seed=9)
+    plain = nat.Accumulator(64, 64)
+    plain.render(ds.native, p, 16)
+    acc = nat.Accumulator(64, 64)
+    acc.set_f64(True)
+    acc.render(ds.native, p, 16)
+    np.testing.assert_array_equal(acc.read(nat.RX_ACC_RADIANCE), plain.read(nat.RX_ACC_RADIANCE))
+    m64 = acc.read_f64()
+    np.testing.assert_allclose(m64, acc.read(nat.RX_ACC_RADIANCE), rtol=2e-5, atol=1e-6)
+    with pytest.raises(ValueError, match="before the first frame"):
+        plain.set_f64(True)
+    ref = reference_render(ds.native, p, 1024)
+    errs = []
+    for spp in (4, 16, 64):
+        a = nat.Accumulator(64, 64)
+        a.render(ds.native, p, spp)
+        errs.append(rel_mse(a.read(nat.RX_ACC_RADIANCE), ref))
+    assert errs[0] > errs[1] > errs[2] > 0.0
+    assert 2.0 < errs[0] / errs[1] < 8.0 and 2.0 < errs[1] / errs[2] < 8.0

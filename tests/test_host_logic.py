@@ -220,3 +220,14 @@ def test_renderer_rejects_bad_light_mode():
     with pytest.raises(ValueError):
         RayTracer(w, Image(8, 8), None, adaptive_min_samples=0)
     assert "3" in repr(TaichiRenderer(w, Image(8, 8), None, samples=3))
+
+
+def test_rel_mse_definition():
+    from rendering.quality import rel_mse
+    ref = np.array([[[0.0, 1.0, 2.0]]])
+    x = np.array([[[0.1, 1.0, 1.0]]])
+    want = np.mean([0.01 / 0.01, 0.0, 1.0 / 4.01])
+    assert abs(rel_mse(x, ref) - want) < 1e-12
+    assert rel_mse(ref, ref) == 0.0
+    with pytest.raises(ValueError):
+        rel_mse(np.zeros((2, 2, 3)), np.zeros((2, 3, 3)))

@@ -40,6 +40,7 @@ enum {
 typedef struct rx_ctx rx_ctx;
 typedef struct rx_scene rx_scene;
 typedef struct rx_accum rx_accum;
+typedef struct rx_batch rx_batch;
 
 /* Arguments of one render call: the reference's render_kernel parameters
  * (rendering/taichi/trace.py:239-254) plus the sampling options. */
@@ -215,6 +216,26 @@ int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int 
  * reset accumulator; rx_accum_read_f64 writes the float64 mean (H,W,3). */
 int rx_accum_set_f64(rx_accum* acc, int on);
 int rx_accum_read_f64(rx_accum* acc, double* host_out);
+
+/* Batched rendering: many (scene, accumulator, params, frames) jobs traced
+ * as shared wavefronts, all waves of one call in one CUDA graph.  The
+ * reference renders one scene per TaichiRenderer.render call
+ * (taichi_renderer.py:87-191); a job's result here equals rendering it
+ * alone with rx_render (same random numbers, same accumulation order).
+ * Scenes and accumulators must outlive the batch's use of them; each job
+ * needs its own accumulator.  rx_batch_add writes the job index to *job
+ * (may be NULL).  rx_batch_set_config: paths per wave (>= 1) and the extend
+ * kernel's block size (64, 128 or 256), normally chosen by the autotuner
+ * (rendering/batch.py).  rx_batch_last_stats: device ms of the last render
+ * call, its waves and kernel launches. */
+int rx_batch_create(rx_ctx* ctx, rx_batch** out);
+int rx_batch_destroy(rx_batch* batch);
+int rx_batch_clear(rx_batch* batch);
+int rx_batch_add(rx_batch* batch, rx_scene* scene, rx_accum* acc, const rx_render_params* params, int frames,
+                 int* job);
+int rx_batch_set_config(rx_batch* batch, long long wave_paths, int extend_block);
+int rx_batch_render(rx_batch* batch);
+int rx_batch_last_stats(rx_batch* batch, float* ms, int* waves, int* launches);
 
 /* edge_aware_denoise / a-trous on caller host buffers (denoise.py:23-104):
  * color (H,W,3); normal, albedo (H,W,3) and depth (H,W) may be NULL. */

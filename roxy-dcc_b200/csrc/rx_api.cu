@@ -19,6 +19,10 @@ struct rx_accum {
   rx::Accum* a;
   rx::Ctx* ctx;
 };
+struct rx_batch {
+  rx::Batch* b;
+  rx::Ctx* ctx;
+};
 
 namespace rx {
 
@@ -675,6 +679,62 @@ int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int 
   if (!acc) return RX_ERR_ARG;
   LOCK(acc->ctx);
   return accum_last_timing(acc->a, ms_total, ms_kernels, n_kernels, launches);
+}
+
+int rx_batch_create(rx_ctx* ctx, rx_batch** out) {
+  if (!ctx || !out) return set_error(nullptr, "rx_batch_create: NULL argument"), RX_ERR_ARG;
+  LOCK(&ctx->c);
+  rx_batch* r = new rx_batch();
+  r->b = batch_new(&ctx->c);
+  r->ctx = &ctx->c;
+  *out = r;
+  return RX_OK;
+}
+
+int rx_batch_destroy(rx_batch* b) {
+  if (!b) return RX_OK;
+  Ctx* c = b->ctx;
+  LOCK(c);
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  batch_delete(b->b);
+  delete b;
+  return RX_OK;
+}
+
+int rx_batch_clear(rx_batch* b) {
+  if (!b) return RX_ERR_ARG;
+  LOCK(b->ctx);
+  return batch_clear(b->b);
+}
+
+int rx_batch_add(rx_batch* b, rx_scene* scene, rx_accum* acc, const rx_render_params* params, int frames,
+                 int* job) {
+  if (!b || !scene || !acc || !params) return set_error(b ? b->ctx : nullptr, "rx_batch_add: NULL argument"), RX_ERR_ARG;
+  LOCK(b->ctx);
+  int idx = -1;
+  int rc = batch_add(b->b, &scene->s, acc->a, params, frames, &idx);
+  if (job) *job = idx;
+  return rc;
+}
+
+int rx_batch_set_config(rx_batch* b, long long wave_paths, int extend_block) {
+  if (!b) return RX_ERR_ARG;
+  LOCK(b->ctx);
+  return batch_set_config(b->b, wave_paths, extend_block);
+}
+
+int rx_batch_render(rx_batch* b) {
+  if (!b) return RX_ERR_ARG;
+  LOCK(b->ctx);
+  cudaSetDevice(b->ctx->device);
+  return batch_render(b->b);
+}
+
+int rx_batch_last_stats(rx_batch* b, float* ms, int* waves, int* launches) {
+  if (!b) return RX_ERR_ARG;
+  LOCK(b->ctx);
+  return batch_last_stats(b->b, ms, waves, launches);
 }
 
 int rx_accum_set_f64(rx_accum* acc, int on) {

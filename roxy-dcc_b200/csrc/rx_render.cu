@@ -192,7 +192,89 @@ __device__ __forceinline__ bool light_sample(const Light& L, float ru1, float ru
   return true;
 }
 
+// ------------------------------------------------------------- path sources
+// Where a path's scene, render parameters, pixel and sample index come from.
+// SingleSrc: one scene and one parameter block for the whole wave (kernel
+// parameters).  BatchSrc: a wave made of segments of several jobs (scene +
+// accumulator + parameters); a per-path segment index selects them.
+
+// Paths [path0, path0 + frames * P) of a wave belong to job `job`: its next
+// `frames` frames, counted from the job's frame base at the start of the wave.
+struct WaveSeg {
+  long long path0;
+  long long acc0;  // first accumulate thread of the segment (prefix sum of P)
+  long long P;
+  int frames;
+  int job;
+};
+
+// Accumulation targets of one job (an Accum's buffers).
+struct JobAcc {
+  float4 *acc_r, *acc_n, *acc_a, *pixels;
+  double* acc64;
+  int* frame_base;
+  unsigned long long* rays;
+};
+
+struct SingleSrc {
+  static constexpr bool kBatch = false;
+  DevScene S;
+  RenderK K;
+  __device__ __forceinline__ int seg(long long) const { return 0; }
+  __device__ __forceinline__ DevScene scene(int) const { return S; }
+  __device__ __forceinline__ RenderK params(int) const { return K; }
+  // pixel and sample index of path p (fb: the accumulator's frame base)
+  __device__ __forceinline__ void locate(int, long long p, int fb, uint32_t& pix, uint32_t& smp) const {
+    pix = (uint32_t)(p % K.P);
+    smp = (uint32_t)(fb + (int)(p / K.P));
+  }
+};
+
+struct BatchSrc {
+  static constexpr bool kBatch = true;
+  const int* pseg;  // segment of each path
+  const WaveSeg* segs;
+  const DevScene* scenes;
+  const RenderK* ks;
+  const JobAcc* accs;
+  unsigned long long* job_rays;  // rays traced per job in this wave
+  __device__ __forceinline__ int seg(long long p) const { return __ldg(pseg + p); }
+  __device__ __forceinline__ DevScene scene(int si) const { return scenes[segs[si].job]; }
+  __device__ __forceinline__ RenderK params(int si) const { return ks[segs[si].job]; }
+  __device__ __forceinline__ void locate(int si, long long p, int, uint32_t& pix, uint32_t& smp) const {
+    WaveSeg g = segs[si];
+    long long l = p - g.path0;
+    int fb = *accs[g.job].frame_base;
+    pix = (uint32_t)(l % g.P);
+    smp = (uint32_t)(fb + (int)(l / g.P));
+  }
+};
+
 // -------------------------------------------------------------------- kernels
+// Camera ray and empty path state of path p (pixel px, py; sample `frame`).
+__device__ __forceinline__ void init_path(const RenderK& K, int px, int py, int frame, long long p,
+                                          float4* __restrict__ ray_o, float4* __restrict__ ray_d,
+                                          float4* __restrict__ thr, float4* __restrict__ rad,
+                                          float4* __restrict__ gn, float4* __restrict__ ga) {
+  float3 d = camera_dir(K, px, py, frame);
+  ray_o[p] = make_float4(K.cam_pos.x, K.cam_pos.y, K.cam_pos.z, 1.0f);
+  ray_d[p] = make_float4(d.x, d.y, d.z, 0.0f);
+  thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// Queue position s of a frame -> pixel: 4-row strips walked column by
+// column, so a warp covers an 8 x 4 tile.
+__device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& px, int& py) {
+  long long strip = s / (4LL * K.W);
+  long long r = s - strip * 4LL * K.W;
+  int hs = min(4, K.H - (int)(4 * strip));
+  px = (int)(r / hs);
+  py = (int)(4 * strip + r % hs);
+}
+
 __global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4* __restrict__ ray_o,
                            float4* __restrict__ ray_d, float4* __restrict__ thr, float4* __restrict__ rad,
                            float4* __restrict__ gn, float4* __restrict__ ga, int* __restrict__ q0,
@@ -203,32 +285,53 @@ __global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
     int f = (int)(t / K.P);
     long long s = t - (long long)f * K.P;
-    // 4-row strips walked column by column: a warp covers an 8 x 4 tile
-    long long strip = s / (4LL * K.W);
-    long long r = s - strip * 4LL * K.W;
-    int hs = min(4, K.H - (int)(4 * strip));
-    int px = (int)(r / hs);
-    int py = (int)(4 * strip + r % hs);
-    long long pix = (long long)py * K.W + px;
-    long long p = (long long)f * K.P + pix;
-    float3 d = camera_dir(K, px, py, fb + f);
-    ray_o[p] = make_float4(K.cam_pos.x, K.cam_pos.y, K.cam_pos.z, 1.0f);
-    ray_d[p] = make_float4(d.x, d.y, d.z, 0.0f);
-    thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    int px, py;
+    strip_pixel(K, s, px, py);
+    long long p = (long long)f * K.P + (long long)py * K.W + px;
+    init_path(K, px, py, fb + f, p, ray_o, ray_d, thr, rad, gn, ga);
     q0[t] = (int)p;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)total;
 }
 
-template <bool EXACT>
-#ifndef RX_EXT_MINB
-#define RX_EXT_MINB 1
-#endif
-__global__ void __launch_bounds__(128, RX_EXT_MINB)
-    k_extend(DevScene S, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
+// Segment holding position x of a sorted prefix array (path0 or acc0).
+template <bool ACC>
+__device__ __forceinline__ int find_seg(const WaveSeg* __restrict__ segs, int n_segs, long long x) {
+  int lo = 0, hi = n_segs - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    long long v = ACC ? segs[mid].acc0 : segs[mid].path0;
+    if (v <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_generate_batch(BatchSrc src, int n_segs, long long total, float4* __restrict__ ray_o,
+                                 float4* __restrict__ ray_d, float4* __restrict__ thr, float4* __restrict__ rad,
+                                 float4* __restrict__ gn, float4* __restrict__ ga, int* __restrict__ q0,
+                                 int* __restrict__ pseg, int* __restrict__ counters) {
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
+    int si = find_seg<false>(src.segs, n_segs, t);
+    WaveSeg g = src.segs[si];
+    RenderK K = src.ks[g.job];
+    int fb = *src.accs[g.job].frame_base;
+    long long l = t - g.path0;
+    int f = (int)(l / g.P);
+    int px, py;
+    strip_pixel(K, l - (long long)f * g.P, px, py);
+    long long p = g.path0 + (long long)f * g.P + (long long)py * K.W + px;
+    init_path(K, px, py, fb + f, p, ray_o, ray_d, thr, rad, gn, ga);
+    pseg[p] = si;
+    q0[t] = (int)p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)total;
+}
+
+template <bool EXACT, class Src, int BS>
+__global__ void __launch_bounds__(BS)
+    k_extend(Src src, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
              const float4* __restrict__ ray_d, float4* __restrict__ hits, int sb, const float4* __restrict__ shadow,
              float4* __restrict__ rad, long long shadow_cap, int* err) {
   // Items [0, n): closest hit of bounce b's queue.  Items [n, n + ns): the
@@ -246,22 +349,55 @@ __global__ void __launch_bounds__(128, RX_EXT_MINB)
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
     int i = base + lane;
+    int job = -1, rays_here = 0;
     if (i < n) {
       int p = qin[i];
+      const int si = src.seg(p);
+      const DevScene S = src.scene(si);
+      if constexpr (Src::kBatch) {
+        job = src.segs[si].job;
+        rays_here = 1;
+      }
       float4 o = ray_o[p], d = ray_d[p];
       SceneHit h = scene_closest<EXACT>(S, xyz(o), xyz(d), err);
       int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
       hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
     } else if (i < total) {
+      // A path's shadow rays of one bounce sit in consecutive records; the
+      // first carries their count (the others 0) and this item traces them
+      // all, adding the visible contributions in light order.  Only this
+      // item writes the path's radiance in this launch: no atomics, and the
+      // sum does not depend on scheduling.
       const float4* sp = shadow + 3 * (size_t)(i - n);
-      float4 s0 = sp[0], s1 = sp[1];
-      if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
-        float4 s2 = sp[2];
-        float* r = reinterpret_cast<float*>(rad + __float_as_int(s1.w));
-        atomicAdd(r, s2.x);
-        atomicAdd(r + 1, s2.y);
-        atomicAdd(r + 2, s2.z);
+      const int cnt = min(__float_as_int(sp[2].w), (int)(ns - (i - n)));
+      if (cnt > 0) {
+        const int p = __float_as_int(sp[1].w);
+        const int si = src.seg(p);
+        const DevScene S = src.scene(si);
+        if constexpr (Src::kBatch) {
+          job = src.segs[si].job;
+          rays_here = cnt;
+        }
+        float3 sum = f3(0.0f, 0.0f, 0.0f);
+        bool any = false;
+        for (int k = 0; k < cnt; ++k) {
+          float4 s0 = sp[3 * k], s1 = sp[3 * k + 1];
+          if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
+            sum = any ? sum + xyz(sp[3 * k + 2]) : xyz(sp[3 * k + 2]);
+            any = true;
+          }
+        }
+        if (any) {
+          float4 r = rad[p];
+          rad[p] = make_float4(r.x + sum.x, r.y + sum.y, r.z + sum.z, r.w);
+        }
       }
+    }
+    if constexpr (Src::kBatch) {
+      // rays traced, counted per job (lanes of a warp mostly share one)
+      unsigned m = __match_any_sync(0xffffffffu, job);
+      int tot = __reduce_add_sync(m, rays_here);
+      if (job >= 0 && lane == __ffs(m) - 1) atomicAdd(src.job_rays + job, (unsigned long long)tot);
     }
   }
 }
@@ -278,7 +414,24 @@ __device__ __forceinline__ int warp_append(bool want, int* counter) {
   return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, const int* __restrict__ qin,
+// warp-aggregated append of cnt >= 0 consecutive entries per lane
+__device__ __forceinline__ int warp_append_n(int cnt, int* counter) {
+  const int lane = threadIdx.x & 31;
+  int x = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  int total = __shfl_sync(0xffffffffu, x, 31);
+  int base = 0;
+  if (lane == 0 && total > 0) base = atomicAdd(counter, total);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  return base + x - cnt;
+}
+
+template <class Src>
+__global__ void __launch_bounds__(128) k_shade(Src src, int b, const int* __restrict__ qin,
                                                int* __restrict__ qout, int* counters,
                                                const int* __restrict__ frame_base, float4* __restrict__ ray_o,
                                                float4* __restrict__ ray_d, float4* __restrict__ thr_b,
@@ -286,9 +439,8 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
                                                float4* __restrict__ ga, const float4* __restrict__ hits,
                                                float4* __restrict__ shadow, int* err) {
   const int n = *(volatile int*)&counters[C_Q + b];
-  const int fb = *frame_base;
+  const int fb = frame_base ? *frame_base : 0;
   const int lane = threadIdx.x & 31;
-  const bool last_bounce = (b + 1) >= K.max_depth;
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&counters[C_FS + b], 32);
@@ -296,6 +448,11 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
     if (base >= n) break;
     int i = base + lane;
     bool valid = i < n;
+    // lanes past the end take the first item's job (they write nothing)
+    const int si = src.seg(qin[valid ? i : base]);
+    const DevScene S = src.scene(si);
+    const RenderK K = src.params(si);
+    const bool last_bounce = (b + 1) >= K.max_depth;
     bool alive = false;
     bool do_nee = false;
     float nee_scale = 1.0f;
@@ -310,8 +467,9 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
       float cur_ior = o4.w;
       bool prev_nee = d4.w != 0.0f;
       int code = __float_as_int(h.y);
-      long long pl = p;
-      rng.init((uint32_t)(pl % K.P), (uint32_t)(fb + (int)(pl / K.P)), (uint32_t)b, K.seed);
+      uint32_t pix_id, smp;
+      src.locate(si, p, fb, pix_id, smp);
+      rng.init(pix_id, smp, (uint32_t)b, K.seed);
       float3 add = f3(0.0f, 0.0f, 0.0f);
       bool has_add = false;
       if (code == -1) {
@@ -447,62 +605,88 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
     // own plane); reference_compat samples from the hit point as trace.py
     // does.
     const float3 nee_p = K.compat ? hit_p : hit_p + nrm * 1e-4f;
-    if (K.mode == 0) {
+    // shadow record: (origin, t_max), (dir, path), (contribution, count),
+    // count = number of this path's records starting here (0 on followers)
+    auto write_rec = [&](long long slot, float3 dir, float max_t, float3 val, int count) {
+      float3 so = hit_p + nrm * 1e-4f;
+      float3 c = thr_nee * val;
+      if (nee_scale != 1.0f) c = c * nee_scale;
+      float4* sp = shadow + 3 * (size_t)slot;
+      sp[0] = make_float4(so.x, so.y, so.z, max_t);
+      sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
+      sp[2] = make_float4(c.x, c.y, c.z, __int_as_float(count));
+    };
+    // direct_light_mode "one": one light picked (uniformly in compat mode,
+    // by the alias table otherwise)
+    auto sample_one = [&](float3& dir, float& max_t, float3& val) {
+      int li;
+      float w;
+      if (K.compat) {
+        int cnt = S.n_lights;
+        li = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)cnt), cnt - 1);
+        w = (float)cnt;
+      } else {
+        int nl = S.n_lights;
+        int col = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)nl), nl - 1);
+        li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
+        w = 1.0f / S.lights[li].pick_pdf;
+      }
+      return light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
+                          max_t, val);
+    };
+    // direct_light_mode "all": light li with its own random slots
+    auto sample_li = [&](int li, float3& dir, float& max_t, float3& val) {
+      int s1 = SLOT_ALL_LIGHTS + 4 * li;
+      return light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val);
+    };
+    bool one_light = false;  // warp-uniform: one scene, mode "one"
+    if constexpr (!Src::kBatch) one_light = K.mode == 0;
+    if (one_light) {
       bool emit = false;
       float3 dir = f3(0, 0, 0), val = f3(0, 0, 0);
       float max_t = 0.0f;
-      if (do_nee) {
-        int li;
-        float w;
-        if (K.compat) {
-          int cnt = S.n_lights;
-          li = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)cnt), cnt - 1);
-          w = (float)cnt;
-        } else {
-          int nl = S.n_lights;
-          int col = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)nl), nl - 1);
-          li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
-          w = 1.0f / S.lights[li].pick_pdf;
-        }
-        emit = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
-                            max_t, val);
-      }
+      if (do_nee) emit = sample_one(dir, max_t, val);
       int slot = warp_append(emit, &counters[C_S + b]);
       if (emit) {
-        if (slot < K.shadow_cap) {
-          float3 so = hit_p + nrm * 1e-4f;
-          float3 c = thr_nee * val;
-          if (nee_scale != 1.0f) c = c * nee_scale;
-          float4* sp = shadow + 3 * (size_t)slot;
-          sp[0] = make_float4(so.x, so.y, so.z, max_t);
-          sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
-          sp[2] = make_float4(c.x, c.y, c.z, 0.0f);
-        } else {
-          atomicOr(err, ERR_SHADOW_OVERFLOW);
-        }
+        if (slot < K.shadow_cap) write_rec(slot, dir, max_t, val, 1);
+        else atomicOr(err, ERR_SHADOW_OVERFLOW);
       }
     } else {
-      for (int li = 0; li < S.n_lights; ++li) {
-        bool emit = false;
-        float3 dir = f3(0, 0, 0), val = f3(0, 0, 0);
-        float max_t = 0.0f;
-        if (do_nee) {
-          int s1 = SLOT_ALL_LIGHTS + 4 * li;
-          emit = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val);
-        }
-        int slot = warp_append(emit, &counters[C_S + b]);
-        if (emit) {
-          if (slot < K.shadow_cap) {
-            float3 so = hit_p + nrm * 1e-4f;
-            float3 c = thr_nee * val;
-            if (nee_scale != 1.0f) c = c * nee_scale;
-            float4* sp = shadow + 3 * (size_t)slot;
-            sp[0] = make_float4(so.x, so.y, so.z, max_t);
-            sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
-            sp[2] = make_float4(c.x, c.y, c.z, 0.0f);
-          } else {
-            atomicOr(err, ERR_SHADOW_OVERFLOW);
+      // mode "all" (and batches, whose lanes may differ in mode and light
+      // count): count this path's shadow rays, reserve that many consecutive
+      // records, then sample again (same random numbers) to write them
+      int cnt = 0;
+      float3 dir0 = f3(0, 0, 0), val0 = f3(0, 0, 0);
+      float mt0 = 0.0f;
+      if (do_nee) {
+        if (K.mode == 0) {
+          cnt = sample_one(dir0, mt0, val0) ? 1 : 0;
+        } else {
+          for (int li = 0; li < S.n_lights; ++li) {
+            float3 d, v;
+            float mt;
+            if (sample_li(li, d, mt, v)) ++cnt;
           }
+        }
+      }
+      long long base = warp_append_n(cnt, &counters[C_S + b]);
+      if (cnt > 0) {
+        if (base + cnt <= K.shadow_cap) {
+          if (K.mode == 0) {
+            write_rec(base, dir0, mt0, val0, 1);
+          } else {
+            int k = 0;
+            for (int li = 0; li < S.n_lights && k < cnt; ++li) {
+              float3 d, v;
+              float mt;
+              if (sample_li(li, d, mt, v)) {
+                write_rec(base + k, d, mt, v, k == 0 ? cnt : 0);
+                ++k;
+              }
+            }
+          }
+        } else {
+          atomicOr(err, ERR_SHADOW_OVERFLOW);
         }
       }
     }
@@ -516,50 +700,77 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, RenderK K, int b, con
 
 // trace.py:262-283: clamp, running mean of radiance and first-hit guides,
 // display = sqrt(min(acc, 1)).  Frames of the wave are folded in order.
-__global__ void k_accumulate(RenderK K, const int* __restrict__ frame_base, const float4* __restrict__ rad,
-                             const float4* __restrict__ gn, const float4* __restrict__ ga,
-                             float4* __restrict__ acc_r, float4* __restrict__ acc_n, float4* __restrict__ acc_a,
-                             float4* __restrict__ pixels, double* __restrict__ acc64) {
-  int fb = *frame_base;
+// One pixel: fold `spf` frames (paths path0 + f * P + pix) into the running
+// means, starting at frame index fb.
+__device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, long long P, long long path0,
+                                                 long long pix, const float4* __restrict__ rad,
+                                                 const float4* __restrict__ gn, const float4* __restrict__ ga,
+                                                 const JobAcc& A) {
+  float4 a = A.acc_r[pix], an = A.acc_n[pix], aa = A.acc_a[pix];
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int f = 0; f < spf; ++f) {
+    long long p = path0 + (long long)f * P + pix;
+    float4 s = rad[p];
+    if (clamp > 0.0f) {
+      s.x = fminf(fmaxf(s.x, 0.0f), clamp);
+      s.y = fminf(fmaxf(s.y, 0.0f), clamp);
+      s.z = fminf(fmaxf(s.z, 0.0f), clamp);
+    }
+    sx += (double)s.x;
+    sy += (double)s.y;
+    sz += (double)s.z;
+    float4 g = gn[p], al = ga[p];
+    int frame = fb + f;
+    if (frame == 0) {
+      a = make_float4(s.x, s.y, s.z, 0.0f);
+      an = g;
+      aa = make_float4(al.x, al.y, al.z, 0.0f);
+    } else {
+      float F = (float)frame, F1 = (float)(frame + 1);
+      a = make_float4((a.x * F + s.x) / F1, (a.y * F + s.y) / F1, (a.z * F + s.z) / F1, 0.0f);
+      an = make_float4((an.x * F + g.x) / F1, (an.y * F + g.y) / F1, (an.z * F + g.z) / F1, (an.w * F + g.w) / F1);
+      aa = make_float4((aa.x * F + al.x) / F1, (aa.y * F + al.y) / F1, (aa.z * F + al.z) / F1, 0.0f);
+    }
+  }
+  A.acc_r[pix] = a;
+  A.acc_n[pix] = an;
+  A.acc_a[pix] = aa;
+  if (A.acc64) {
+    // float64 sums of the clamped samples (reference renders for relMSE)
+    A.acc64[3 * pix] += sx;
+    A.acc64[3 * pix + 1] += sy;
+    A.acc64[3 * pix + 2] += sz;
+  }
+  A.pixels[pix] = make_float4(sqrtf(fminf(a.x, 1.0f)), sqrtf(fminf(a.y, 1.0f)), sqrtf(fminf(a.z, 1.0f)), 0.0f);
+}
+
+__global__ void k_accumulate(RenderK K, JobAcc A, const float4* __restrict__ rad, const float4* __restrict__ gn,
+                             const float4* __restrict__ ga) {
+  int fb = *A.frame_base;
   for (long long pix = blockIdx.x * (long long)blockDim.x + threadIdx.x; pix < K.P;
-       pix += (long long)gridDim.x * blockDim.x) {
-    float4 a = acc_r[pix], an = acc_n[pix], aa = acc_a[pix];
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int f = 0; f < K.spf; ++f) {
-      long long p = (long long)f * K.P + pix;
-      float4 s = rad[p];
-      if (K.clamp > 0.0f) {
-        s.x = fminf(fmaxf(s.x, 0.0f), K.clamp);
-        s.y = fminf(fmaxf(s.y, 0.0f), K.clamp);
-        s.z = fminf(fmaxf(s.z, 0.0f), K.clamp);
-      }
-      sx += (double)s.x;
-      sy += (double)s.y;
-      sz += (double)s.z;
-      float4 g = gn[p], al = ga[p];
-      int frame = fb + f;
-      if (frame == 0) {
-        a = make_float4(s.x, s.y, s.z, 0.0f);
-        an = g;
-        aa = make_float4(al.x, al.y, al.z, 0.0f);
-      } else {
-        float F = (float)frame, F1 = (float)(frame + 1);
-        a = make_float4((a.x * F + s.x) / F1, (a.y * F + s.y) / F1, (a.z * F + s.z) / F1, 0.0f);
-        an = make_float4((an.x * F + g.x) / F1, (an.y * F + g.y) / F1, (an.z * F + g.z) / F1,
-                         (an.w * F + g.w) / F1);
-        aa = make_float4((aa.x * F + al.x) / F1, (aa.y * F + al.y) / F1, (aa.z * F + al.z) / F1, 0.0f);
-      }
-    }
-    acc_r[pix] = a;
-    acc_n[pix] = an;
-    acc_a[pix] = aa;
-    if (acc64) {
-      // float64 sums of the clamped samples (reference renders for relMSE)
-      acc64[3 * pix] += sx;
-      acc64[3 * pix + 1] += sy;
-      acc64[3 * pix + 2] += sz;
-    }
-    pixels[pix] = make_float4(sqrtf(fminf(a.x, 1.0f)), sqrtf(fminf(a.y, 1.0f)), sqrtf(fminf(a.z, 1.0f)), 0.0f);
+       pix += (long long)gridDim.x * blockDim.x)
+    accumulate_pixel(K.clamp, K.spf, fb, K.P, 0, pix, rad, gn, ga, A);
+}
+
+__global__ void k_accumulate_batch(BatchSrc src, int n_segs, long long total, const float4* __restrict__ rad,
+                                   const float4* __restrict__ gn, const float4* __restrict__ ga) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int si = find_seg<true>(src.segs, n_segs, t);
+    WaveSeg g = src.segs[si];
+    JobAcc A = src.accs[g.job];
+    accumulate_pixel(src.ks[g.job].clamp, g.frames, *A.frame_base, g.P, g.path0, t - g.acc0, rad, gn, ga, A);
+  }
+}
+
+// After a batch wave: each job's frame base and ray count advance.
+__global__ void k_finish_batch(BatchSrc src, int n_segs) {
+  for (int si = blockIdx.x * blockDim.x + threadIdx.x; si < n_segs; si += gridDim.x * blockDim.x) {
+    WaveSeg g = src.segs[si];
+    const JobAcc& A = src.accs[g.job];
+    *A.frame_base += g.frames;
+    *A.rays += src.job_rays[g.job];
+    src.job_rays[g.job] = 0;
   }
 }
 
@@ -697,14 +908,15 @@ static int blocks_for(Ctx* ctx, const void* fn, int block) {
 
 static void launch_extend(Accum* a, const DevScene& S, const RenderK& K, int b, const int* qin, int sb) {
   Ctx* ctx = a->ctx;
+  SingleSrc src{S, K};
   if (S.exact_slab)
-    k_extend<true><<<a->occ_ext, 128, 0, ctx->stream>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p,
-                                                         a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
-                                                         ctx->d_err);
+    k_extend<true, SingleSrc, 128><<<a->occ_ext, 128, 0, ctx->stream>>>(
+        src, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
+        ctx->d_err);
   else
-    k_extend<false><<<a->occ_ext, 128, 0, ctx->stream>>>(S, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p,
-                                                          a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
-                                                          ctx->d_err);
+    k_extend<false, SingleSrc, 128><<<a->occ_ext, 128, 0, ctx->stream>>>(
+        src, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
+        ctx->d_err);
 }
 
 // Records the launch sequence of one wave on the context stream.  With
@@ -739,9 +951,9 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
     launch_extend(a, S, K, b, qin, sb);
     ++launches;
     mark(K_EXTEND);
-    k_shade<<<a->occ_shade, 128, 0, st>>>(S, K, b, qin, qout, a->counters.p, a->frame_base.p, a->ray_o.p,
-                                           a->ray_d.p, a->thr.p, a->rad.p, a->gn.p, a->ga.p, a->hits.p,
-                                           a->shadow.p, ctx->d_err);
+    k_shade<SingleSrc><<<a->occ_shade, 128, 0, st>>>(SingleSrc{S, K}, b, qin, qout, a->counters.p,
+                                                      a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p,
+                                                      a->gn.p, a->ga.p, a->hits.p, a->shadow.p, ctx->d_err);
     ++launches;
     mark(K_SHADE);
   }
@@ -752,8 +964,8 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
     mark(K_CONNECT);
   }
   int ablocks = (int)std::min<long long>((K.P + 255) / 256, (long long)ctx->num_sms * 16);
-  k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->rad.p, a->gn.p, a->ga.p, a->acc_r.p,
-                                                      a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p);
+  JobAcc A{a->acc_r.p, a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p, a->frame_base.p, a->rays.p};
+  k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, A, a->rad.p, a->gn.p, a->ga.p);
   k_finish<<<1, 1, 0, st>>>(a->counters.p, K.max_depth, a->frame_base.p, a->rays.p, K.spf);
   launches += 2;
   mark(K_OTHER);
@@ -784,8 +996,8 @@ static int ensure_wave_buffers(Accum* a, long long cap, long long shadow_cap) {
     a->shadow_cap = shadow_cap;
   }
   if (!a->occ_ext) {
-    a->occ_ext = blocks_for(ctx, (const void*)k_extend<false>, 128);
-    a->occ_shade = blocks_for(ctx, (const void*)k_shade, 128);
+    a->occ_ext = blocks_for(ctx, (const void*)k_extend<false, SingleSrc, 128>, 128);
+    a->occ_shade = blocks_for(ctx, (const void*)k_shade<SingleSrc>, 128);
   }
   return RX_OK;
 }
@@ -993,6 +1205,302 @@ int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out) {
     CUDA_TRY(ctx, cudaMemcpyAsync(host_out, tmp.p, tmp.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  return RX_OK;
+}
+
+// ------------------------------------------------------------------ batches
+// Many (scene, accumulator, parameters, frames) jobs rendered as shared
+// wavefronts: each wave packs frames of several jobs into one path space, so
+// one extend and one shade launch per bounce serve every scene, short jobs
+// leave the queues early and small images no longer pay a launch sequence
+// each.  All waves of a render call are captured into one CUDA graph.  A
+// job's random numbers are keyed exactly as in a render of its own, so its
+// result does not depend on what it is batched with.
+struct BatchJob {
+  Scene* sc;
+  Accum* acc;
+  rx_render_params p;
+  int frames;
+};
+
+struct PlannedWave {
+  int seg0, nseg;
+  long long paths, acc_threads, shadow;
+  int max_depth;
+};
+
+struct Batch {
+  Ctx* ctx = nullptr;
+  std::vector<BatchJob> jobs;
+  long long wave_paths = 1LL << 25;
+  int ext_block = 128;
+  long long cap = 0, shadow_cap = 0;
+  DevBuf<float4> ray_o, ray_d, thr, rad, gn, ga, hits, shadow;
+  DevBuf<int> q0, q1, counters, pseg;
+  DevBuf<DevScene> d_scenes;
+  DevBuf<RenderK> d_ks;
+  DevBuf<JobAcc> d_accs;
+  DevBuf<unsigned long long> d_job_rays;
+  DevBuf<WaveSeg> d_segs;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<unsigned char> g_key;
+  int g_launches = 0, g_waves = 0;
+  float last_ms = 0.0f;
+  int last_waves = 0, last_launches = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    g_key.clear();
+  }
+  ~Batch() {
+    drop_graph();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+Batch* batch_new(Ctx* ctx) {
+  Batch* b = new Batch();
+  b->ctx = ctx;
+  return b;
+}
+
+void batch_delete(Batch* b) { delete b; }
+
+int batch_clear(Batch* b) {
+  b->jobs.clear();
+  return RX_OK;
+}
+
+int batch_add(Batch* b, Scene* sc, Accum* acc, const rx_render_params* p, int frames, int* job) {
+  Ctx* ctx = b->ctx;
+  if (!sc || !acc || !p || frames < 0) return set_error(ctx, "batch_add: bad arguments"), RX_ERR_ARG;
+  if (sc->ctx != ctx || acc->ctx != ctx) return set_error(ctx, "batch_add: job on another context"), RX_ERR_ARG;
+  if (p->width != acc->W || p->height != acc->H)
+    return set_error(ctx, "batch_add: %dx%d does not match the accumulator %dx%d", p->width, p->height, acc->W,
+                     acc->H),
+           RX_ERR_ARG;
+  if (p->max_depth < 0 || p->max_depth > kMaxBounce - 1)
+    return set_error(ctx, "batch_add: max_depth must be in [0, %d]", kMaxBounce - 1), RX_ERR_ARG;
+  if (p->direct_light_mode != 0 && p->direct_light_mode != 1)
+    return set_error(ctx, "direct_light_mode must be 'one' or 'all'"), RX_ERR_ARG;
+  for (const BatchJob& j : b->jobs)
+    if (j.acc == acc) return set_error(ctx, "batch_add: two jobs share one accumulator"), RX_ERR_ARG;
+  b->jobs.push_back(BatchJob{sc, acc, *p, frames});
+  *job = (int)b->jobs.size() - 1;
+  return RX_OK;
+}
+
+int batch_set_config(Batch* b, long long wave_paths, int ext_block) {
+  if (wave_paths < 1 || wave_paths >= (1LL << 31))
+    return set_error(b->ctx, "batch_set_config: wave_paths out of range"), RX_ERR_ARG;
+  if (ext_block != 64 && ext_block != 128 && ext_block != 256)
+    return set_error(b->ctx, "batch_set_config: extend block must be 64, 128 or 256"), RX_ERR_ARG;
+  if (wave_paths != b->wave_paths || ext_block != b->ext_block) b->drop_graph();
+  b->wave_paths = wave_paths;
+  b->ext_block = ext_block;
+  return RX_OK;
+}
+
+static std::vector<PlannedWave> plan_waves(const Batch* b, std::vector<WaveSeg>& segs) {
+  std::vector<PlannedWave> waves;
+  std::vector<int> rem(b->jobs.size());
+  for (size_t j = 0; j < b->jobs.size(); ++j) rem[j] = b->jobs[j].frames;
+  for (;;) {
+    PlannedWave w{(int)segs.size(), 0, 0, 0, 0, 0};
+    long long left = b->wave_paths;
+    for (size_t j = 0; j < b->jobs.size() && left > 0; ++j) {
+      if (rem[j] == 0) continue;
+      const BatchJob& J = b->jobs[j];
+      long long P = (long long)J.p.width * J.p.height;
+      if (P == 0) {
+        rem[j] = 0;
+        continue;
+      }
+      if (w.nseg > 0 && P > left) continue;
+      int k = (int)std::max<long long>(1, std::min<long long>(rem[j], left / P));
+      segs.push_back(WaveSeg{w.paths, w.acc_threads, P, k, (int)j});
+      ++w.nseg;
+      w.paths += k * P;
+      w.acc_threads += P;
+      left -= k * P;
+      rem[j] -= k;
+      int nl = J.sc->n_lights;
+      w.shadow += k * P * (J.p.direct_light_mode == 1 ? std::max(nl, 1) : 1);
+      w.max_depth = std::max(w.max_depth, J.p.max_depth);
+    }
+    if (w.nseg == 0) break;
+    waves.push_back(w);
+  }
+  return waves;
+}
+
+template <int BS>
+static void launch_extend_batch(Batch* B, const BatchSrc& src, int occ, int b, const int* qin, int sb) {
+  k_extend<false, BatchSrc, BS><<<occ, BS, 0, B->ctx->stream>>>(src, b, qin, B->counters.p, B->ray_o.p, B->ray_d.p,
+                                                               B->hits.p, sb, B->shadow.p, B->rad.p, B->shadow_cap,
+                                                               B->ctx->d_err);
+}
+
+static int batch_ext_blocks(Ctx* ctx, int bs) {
+  if (bs == 64) return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 64>, 64);
+  if (bs == 256) return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 256>, 256);
+  return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 128>, 128);
+}
+
+static void enqueue_batch(Batch* B, const std::vector<PlannedWave>& waves, int* n_launch) {
+  Ctx* ctx = B->ctx;
+  cudaStream_t st = ctx->stream;
+  int occ_ext = batch_ext_blocks(ctx, B->ext_block);
+  int occ_shade = blocks_for(ctx, (const void*)k_shade<BatchSrc>, 128);
+  int launches = 0;
+  for (const PlannedWave& w : waves) {
+    BatchSrc src{B->pseg.p, B->d_segs.p + w.seg0, B->d_scenes.p, B->d_ks.p, B->d_accs.p, B->d_job_rays.p};
+    cudaMemsetAsync(B->counters.p, 0, sizeof(int) * C_N, st);
+    int gblocks = (int)std::min<long long>((w.paths + 255) / 256, (long long)ctx->num_sms * 16);
+    k_generate_batch<<<std::max(gblocks, 1), 256, 0, st>>>(src, w.nseg, w.paths, B->ray_o.p, B->ray_d.p, B->thr.p,
+                                                            B->rad.p, B->gn.p, B->ga.p, B->q0.p, B->pseg.p,
+                                                            B->counters.p);
+    ++launches;
+    auto ext = [&](int b, const int* qin, int sb) {
+      if (B->ext_block == 64) launch_extend_batch<64>(B, src, occ_ext, b, qin, sb);
+      else if (B->ext_block == 256) launch_extend_batch<256>(B, src, occ_ext, b, qin, sb);
+      else launch_extend_batch<128>(B, src, occ_ext, b, qin, sb);
+      ++launches;
+    };
+    for (int b = 0; b < w.max_depth; ++b) {
+      const int* qin = (b & 1) ? B->q1.p : B->q0.p;
+      int* qout = (b & 1) ? B->q0.p : B->q1.p;
+      ext(b, qin, b >= 1 ? b - 1 : -1);
+      k_shade<BatchSrc><<<occ_shade, 128, 0, st>>>(src, b, qin, qout, B->counters.p, nullptr, B->ray_o.p,
+                                                    B->ray_d.p, B->thr.p, B->rad.p, B->gn.p, B->ga.p, B->hits.p,
+                                                    B->shadow.p, ctx->d_err);
+      ++launches;
+    }
+    if (w.max_depth > 0) ext(-1, nullptr, w.max_depth - 1);
+    int ablocks = (int)std::min<long long>((w.acc_threads + 255) / 256, (long long)ctx->num_sms * 16);
+    k_accumulate_batch<<<std::max(ablocks, 1), 256, 0, st>>>(src, w.nseg, w.acc_threads, B->rad.p, B->gn.p,
+                                                              B->ga.p);
+    k_finish_batch<<<(w.nseg + 127) / 128, 128, 0, st>>>(src, w.nseg);
+    launches += 2;
+  }
+  *n_launch = launches;
+}
+
+template <class T>
+static void key_put(std::vector<unsigned char>& k, const T& v) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), p, p + sizeof(T));
+}
+
+int batch_render(Batch* B) {
+  Ctx* ctx = B->ctx;
+  if (B->jobs.empty()) return RX_OK;
+  for (const BatchJob& j : B->jobs) {
+    if (j.sc->n_tris > 0 && j.sc->n_nodes == 0)
+      return set_error(ctx, "batch_render: a scene has triangles but no BVH"), RX_ERR_STATE;
+    int rc = j.sc->upload_palette(ctx);
+    if (rc) return rc;
+  }
+  std::vector<WaveSeg> segs;
+  std::vector<PlannedWave> waves = plan_waves(B, segs);
+  if (waves.empty()) return RX_OK;
+  long long cap = 0, shadow_cap = 0;
+  for (const PlannedWave& w : waves) {
+    cap = std::max(cap, w.paths);
+    shadow_cap = std::max(shadow_cap, w.shadow);
+  }
+  if (cap >= (1LL << 31)) return set_error(ctx, "batch_render: a wave of %lld paths is too large", cap), RX_ERR_CAPACITY;
+  // wave buffers
+  if (cap > B->cap) {
+    B->drop_graph();
+    bool ok = B->ray_o.alloc(ctx, cap) && B->ray_d.alloc(ctx, cap) && B->thr.alloc(ctx, cap) &&
+              B->rad.alloc(ctx, cap) && B->gn.alloc(ctx, cap) && B->ga.alloc(ctx, cap) && B->hits.alloc(ctx, cap) &&
+              B->q0.alloc(ctx, cap) && B->q1.alloc(ctx, cap) && B->pseg.alloc(ctx, cap);
+    if (!ok) {
+      B->cap = 0;
+      return set_error(ctx, "batch_render: out of device memory for %lld wavefront paths", cap), RX_ERR_CAPACITY;
+    }
+    B->cap = cap;
+  }
+  if (shadow_cap > B->shadow_cap) {
+    B->drop_graph();
+    if (!B->shadow.alloc(ctx, (size_t)3 * shadow_cap)) {
+      B->shadow_cap = 0;
+      return set_error(ctx, "batch_render: out of device memory for %lld shadow rays", shadow_cap), RX_ERR_CAPACITY;
+    }
+    B->shadow_cap = shadow_cap;
+  }
+  if (!B->counters.p && !B->counters.alloc(ctx, C_N))
+    return set_error(ctx, "batch_render: out of device memory"), RX_ERR_CAPACITY;
+  // job tables and segments; the captured graph is reused while they match
+  size_t nj = B->jobs.size();
+  std::vector<DevScene> scenes(nj);
+  std::vector<RenderK> ks(nj);
+  std::vector<JobAcc> accs(nj);
+  std::vector<unsigned char> key;
+  for (size_t j = 0; j < nj; ++j) {
+    const BatchJob& J = B->jobs[j];
+    scenes[j] = J.sc->view();
+    ks[j] = make_k(&J.p, J.acc, 0, B->shadow_cap);
+    ks[j].queue_cap = B->cap;
+    Accum* a = J.acc;
+    accs[j] = JobAcc{a->acc_r.p, a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p, a->frame_base.p, a->rays.p};
+    key_put(key, J.sc);
+    key_put(key, J.sc->version);
+    key_put(key, J.acc);
+    key_put(key, a->acc64.p);
+    key_put(key, J.p);
+    key_put(key, J.frames);
+  }
+  key_put(key, B->wave_paths);
+  key_put(key, B->ext_block);
+  key_put(key, B->cap);
+  key_put(key, B->shadow_cap);
+  cudaStream_t st = ctx->stream;
+  bool cached = B->gexec && key == B->g_key;
+  if (!cached) {
+    B->drop_graph();
+    if (!B->d_scenes.alloc(ctx, nj) || !B->d_ks.alloc(ctx, nj) || !B->d_accs.alloc(ctx, nj) ||
+        !B->d_job_rays.alloc(ctx, nj) || !B->d_segs.alloc(ctx, segs.size()))
+      return set_error(ctx, "batch_render: out of device memory for job tables"), RX_ERR_CAPACITY;
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_scenes.p, scenes.data(), sizeof(DevScene) * nj, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_ks.p, ks.data(), sizeof(RenderK) * nj, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_accs.p, accs.data(), sizeof(JobAcc) * nj, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemsetAsync(B->d_job_rays.p, 0, sizeof(unsigned long long) * nj, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(B->d_segs.p, segs.data(), sizeof(WaveSeg) * segs.size(), cudaMemcpyHostToDevice,
+                                  st));
+    cudaGraph_t g;
+    CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int nl = 0;
+    enqueue_batch(B, waves, &nl);
+    CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+    CUDA_TRY(ctx, cudaGraphInstantiate(&B->gexec, g, 0));
+    cudaGraphDestroy(g);
+    B->g_key = key;
+    B->g_launches = nl;
+    B->g_waves = (int)waves.size();
+  }
+  if (!B->e0) {
+    CUDA_TRY(ctx, cudaEventCreate(&B->e0));
+    CUDA_TRY(ctx, cudaEventCreate(&B->e1));
+  }
+  CUDA_TRY(ctx, cudaEventRecord(B->e0, st));
+  CUDA_TRY(ctx, cudaGraphLaunch(B->gexec, st));
+  CUDA_TRY(ctx, cudaEventRecord(B->e1, st));
+  CUDA_TRY(ctx, cudaEventSynchronize(B->e1));
+  CUDA_TRY(ctx, cudaEventElapsedTime(&B->last_ms, B->e0, B->e1));
+  B->last_waves = B->g_waves;
+  B->last_launches = B->g_launches;
+  for (const BatchJob& j : B->jobs) j.acc->frames += j.frames;
+  return check_device_error(ctx);
+}
+
+int batch_last_stats(Batch* B, float* ms, int* waves, int* launches) {
+  if (ms) *ms = B->last_ms;
+  if (waves) *waves = B->last_waves;
+  if (launches) *launches = B->last_launches;
   return RX_OK;
 }
 

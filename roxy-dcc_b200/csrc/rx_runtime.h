@@ -207,6 +207,16 @@ int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernel
 int accum_set_f64(Accum* a, int on);
 int accum_read_f64(Accum* a, double* host_out);
 
+// Batches of jobs rendered as shared wavefronts (rx_render.cu)
+struct Batch;
+Batch* batch_new(Ctx* ctx);
+void batch_delete(Batch* b);
+int batch_clear(Batch* b);
+int batch_add(Batch* b, Scene* sc, Accum* acc, const rx_render_params* p, int frames, int* job);
+int batch_set_config(Batch* b, long long wave_paths, int ext_block);
+int batch_render(Batch* b);
+int batch_last_stats(Batch* b, float* ms, int* waves, int* launches);
+
 // Denoise on caller buffers (rx_denoise.cu)
 int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal, const float* albedo,
                  const float* depth, const rx_denoise_params* dp, float* out);

@@ -124,6 +124,14 @@ _SIGS = {
     "rx_accum_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_accum_last_timing": ([ctypes.c_void_p, _f32p, _f32p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_accum_set_f64": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rx_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_batch_clear": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_batch_add": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(RenderParams), ctypes.c_int,
+                      _i32p], ctypes.c_int),
+    "rx_batch_set_config": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int], ctypes.c_int),
+    "rx_batch_render": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_batch_last_stats": ([ctypes.c_void_p, _f32p, _i32p, _i32p], ctypes.c_int),
     "rx_accum_read_f64": ([ctypes.c_void_p, _f64p], ctypes.c_int),
     "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
@@ -416,6 +424,53 @@ class NativeScene:
     def close(self):
         if getattr(self, "h", None) is not None and _LIB is not None:
             _LIB.rx_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """An rx_batch: jobs (NativeScene, Accumulator, RenderParams, frames)
+    rendered together as shared wavefronts in one CUDA graph."""
+
+    def __init__(self, ctx=None):
+        self.ctx = ctx or context()
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().rx_batch_create(self.ctx.h, ctypes.byref(h)))
+        self.h = h
+        self._keep = []
+
+    def add(self, scene, acc, params, frames):
+        p = type(params).from_buffer_copy(params)
+        job = ctypes.c_int(-1)
+        self.ctx.check(lib().rx_batch_add(self.h, scene.h, acc.h, ctypes.byref(p), int(frames), ctypes.byref(job)))
+        self._keep.append((scene, acc, p))
+        return job.value
+
+    def clear(self):
+        self.ctx.check(lib().rx_batch_clear(self.h))
+        self._keep = []
+
+    def set_config(self, wave_paths, extend_block=128):
+        self.ctx.check(lib().rx_batch_set_config(self.h, int(wave_paths), int(extend_block)))
+
+    def render(self):
+        self.ctx.check(lib().rx_batch_render(self.h))
+
+    def last_stats(self):
+        ms = ctypes.c_float()
+        waves = ctypes.c_int()
+        launches = ctypes.c_int()
+        self.ctx.check(lib().rx_batch_last_stats(self.h, ctypes.byref(ms), ctypes.byref(waves), ctypes.byref(launches)))
+        return dict(ms=ms.value, waves=waves.value, launches=launches.value)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _LIB is not None:
+            _LIB.rx_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -171,6 +171,68 @@ def displaced_icosphere_scene(width=1920, height=1080, subdiv=7, n_spheres=64, s
     return world
 
 
+BOX_COLORS = [(0.73, 0.73, 0.73), (0.65, 0.05, 0.05), (0.12, 0.45, 0.15)]
+
+
+def instanced_box_scene(n_tris, seed, width=256, height=256, n_spheres=16):
+    """One scene of the batched configuration: seeded instances of a unit box
+    (12 triangles each, n_tris // 12 of them, random size, yaw and
+    position) in one IndexedMesh with the Cornell box's three Lambertian
+    albedos as material groups, `n_spheres` Lambertian spheres, a floor quad
+    and a 0.5 x 0.5 emissive quad with emission (17, 12, 4)."""
+    rng = np.random.default_rng(seed)
+    n_box = max(1, n_tris // 12)
+    bp, bf = _box_mesh(1.0, 1.0, 1.0)
+    size = rng.uniform(0.02, 0.12, size=(n_box, 3)) * (1.0 + 3.0 * (n_box < 400))
+    yaw = rng.uniform(0.0, 2.0 * np.pi, n_box)
+    spread = 1.0 + 0.25 * np.log10(n_box)
+    ctr = np.stack([rng.uniform(-spread, spread, n_box), rng.uniform(0.0, 1.2, n_box),
+                    rng.uniform(-spread, spread, n_box)], axis=1)
+    c, s = np.cos(yaw), np.sin(yaw)
+    local = bp[None, :, :] * size[:, None, :]
+    x = c[:, None] * local[:, :, 0] + s[:, None] * local[:, :, 2]
+    z = -s[:, None] * local[:, :, 0] + c[:, None] * local[:, :, 2]
+    pos = np.stack([x, local[:, :, 1], z], axis=2) + ctr[:, None, :]
+    faces = (bf[None, :, :] + 8 * np.arange(n_box, dtype=np.int32)[:, None, None]).reshape(-1, 3)
+    gidx = np.repeat(rng.integers(0, 3, n_box).astype(np.int32), 12)
+    world = World(use_sky=False, background_color=Color(0.0, 0.0, 0.0))
+    world.add_camera(Camera(position=Vec3(0.0, 1.6, 2.6 * spread + 1.0), forward=Vec3(0, -0.45, -1),
+                            up=Vec3(0, 1, 0), fov=40, width=width, height=height))
+    mats = {f"c{k}": Diffuse(Color(*BOX_COLORS[k])) for k in range(3)}
+    mesh = IndexedMesh(pos.reshape(-1, 3), faces, groups=list(mats), tri_group_idx=gidx, build_bvh=False)
+    world.add_object(SceneObject(shapes=[Shape(mesh, mats)], name="boxes"))
+    for i in range(n_spheres):
+        r = float(rng.uniform(0.05, 0.2))
+        p = [float(rng.uniform(-spread, spread)), r, float(rng.uniform(-spread, spread))]
+        world.add_object(SceneObject(shape=Sphere(r), material=Diffuse(Color(*BOX_COLORS[i % 3])),
+                                     translation=Vec3(*p), name=f"sphere{i}"))
+    e = 2.0 * spread
+    fp = np.array([[-e, 0, -e], [e, 0, -e], [e, 0, e], [-e, 0, e]], dtype=np.float64)
+    world.add_object(SceneObject(shapes=[Shape(IndexedMesh(fp, np.array([[0, 2, 1], [0, 3, 2]], np.int32),
+                                                           build_bvh=False), {"default": Diffuse(Color(*BOX_COLORS[0]))})],
+                                 name="floor"))
+    lp = np.array([[-0.25, 2.5, -0.25], [0.25, 2.5, -0.25], [0.25, 2.5, 0.25], [-0.25, 2.5, 0.25]], np.float64)
+    world.add_object(SceneObject(shapes=[Shape(IndexedMesh(lp, np.array([[0, 1, 2], [0, 2, 3]], np.int32),
+                                                           build_bvh=False),
+                                               {"default": Emissive(Color(17.0, 12.0, 4.0), intensity=1.0)})],
+                                 name="light"))
+    return world
+
+
+def batch_specs(n_scenes=64, seed=7, tri_range=(1e3, 2e6), resolutions=(256, 512, 1024), spps=(1, 4, 16, 64),
+                depth_range=(4, 16)):
+    """The batched configuration: per scene a triangle count log-uniform in
+    `tri_range`, a square resolution, spp and max depth drawn by seed."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_scenes):
+        n = int(round(math.exp(rng.uniform(math.log(tri_range[0]), math.log(tri_range[1])))))
+        res = int(rng.choice(resolutions))
+        specs.append(dict(n_tris=n, width=res, height=res, spp=int(rng.choice(spps)),
+                          max_depth=int(rng.integers(depth_range[0], depth_range[1] + 1)), seed=seed * 1000 + i))
+    return specs
+
+
 def camera_params(world, width, height):
     cam = world.active_camera
     return dict(fov_tan=math.tan(math.radians(cam.fov) / 2), aspect=cam.aspect_ratio, cam_pos=list(cam.position),

@@ -222,6 +222,26 @@ def test_renderer_rejects_bad_light_mode():
     assert "3" in repr(TaichiRenderer(w, Image(8, 8), None, samples=3))
 
 
+def test_autotuner_choice_and_batch_specs():
+    import workloads
+    from rendering.batch import choose
+    calls = []
+
+    def measure(c):
+        calls.append(c)
+        return {(1, 64): 3.0, (1, 128): 2.0, (2, 64): 2.5, (2, 128): 4.0}[c]
+
+    best, timings = choose([(1, 64), (1, 128), (2, 64), (2, 128)], measure, repeats=2)
+    assert best == (1, 128) and len(calls) == 8 and len(timings) == 4
+    specs = workloads.batch_specs()
+    assert len(specs) == 64
+    tris = np.array([s["n_tris"] for s in specs])
+    assert tris.min() >= 1000 and tris.max() <= 2_000_000 and 10e6 < tris.sum() < 30e6
+    assert {s["width"] for s in specs} <= {256, 512, 1024} and {s["spp"] for s in specs} <= {1, 4, 16, 64}
+    assert all(4 <= s["max_depth"] <= 16 for s in specs)
+    assert specs == workloads.batch_specs()  # seeded
+
+
 def test_rel_mse_definition():
     from rendering.quality import rel_mse
     ref = np.array([[[0.0, 1.0, 2.0]]])

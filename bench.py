@@ -175,6 +175,10 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
+    if args.workload == "batch":
+        print(json.dumps({"impl": "reference", "unavailable": "the batched workload's baseline is the plain "
+                                                              "one-scene-at-a-time GPU path reported in its own line"}))
+        return 0
     world = _world(args.workload)
     w = WORKLOADS[args.workload]
     vals = []
@@ -372,19 +376,169 @@ def _ray_split(ds, acc, params, w):
     return {"extend_rays": ext}
 
 
+def run_batch(args):
+    """Batched configuration: 64 seeded instanced-box scenes (1k-2M
+    triangles, 256^2-1024^2, 1-64 spp, depth 4-16) rendered as one batch
+    (rx_batch_*, autotuned) against the plain path, which renders the same
+    jobs one scene at a time (rx_render per scene)."""
+    import roxy_native as nat
+    import torch
+    import workloads
+    from rendering.batch import BatchRenderer, Job
+
+    ws, rank, local = _dist()
+    dist = None
+    dev = local if ws > 1 else 0
+    if ws > 1:
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = tdist
+    ctx = nat.context(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", dev))
+    specs = workloads.batch_specs(n_scenes=args.scenes)
+    t0 = time.perf_counter()
+    jobs = [Job(workloads.instanced_box_scene(s["n_tris"], s["seed"], s["width"], s["height"]), s["width"],
+                s["height"], s["spp"], s["max_depth"], direct_light_max_depth=s["max_depth"], seed=s["seed"])
+            for s in specs]
+    br = BatchRenderer(jobs, ctx=ctx)
+    ctx.sync()
+    build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cfg = br.autotune()
+    tune_s = time.perf_counter() - t0
+
+    def timed(fn):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ctx.sync()
+        ev0.record(stream)
+        fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    def reset_all():
+        for j in jobs:
+            j.acc.reset()
+
+    # plain path: one scene at a time, one accumulator per resolution
+    plain_acc = {}
+    for j in jobs:
+        if (j.width, j.height) not in plain_acc:
+            plain_acc[(j.width, j.height)] = nat.Accumulator(j.width, j.height, ctx)
+
+    def plain():
+        rays = 0
+        for j in jobs:
+            a = plain_acc[(j.width, j.height)]
+            a.reset()
+            a.render(j.scene.native, j.params, j.spp)
+            rays += a.info()["rays"]
+        return rays
+
+    for _ in range(args.warmup):
+        reset_all()
+        br.render()
+        plain()
+    if dist:
+        dist.barrier()
+    batch_ms, plain_ms, e2e_ms, rays = [], [], [], 0
+    launches = 0
+    with ClockSampler(dev) as clocks:
+        for _ in range(args.steps):
+            reset_all()
+            batch_ms.append(timed(br.render))
+            launches = br.batch.last_stats()["launches"]
+    rays = sum(j.acc.info()["rays"] for j in jobs)
+    for _ in range(args.steps):
+        plain_ms.append(timed(plain))
+    plain_rays = plain()
+
+    # first previews: one frame of every scene, batched vs one at a time
+    def plain_preview():
+        for j in jobs:
+            a = plain_acc[(j.width, j.height)]
+            a.reset()
+            a.render(j.scene.native, j.params, 1)
+
+    def batch_preview():
+        br.render(frames=1)
+
+    for _ in range(2):
+        reset_all()
+        batch_preview()
+        plain_preview()
+    prev_b, prev_p = [], []
+    for _ in range(args.steps):
+        reset_all()
+        prev_b.append(timed(batch_preview))
+        prev_p.append(timed(plain_preview))
+    # end to end: batch render plus read-back of every display image
+    d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        reset_all()
+        t = time.perf_counter()
+        br.render()
+        d2h = sum(j.acc.read(nat.RX_ACC_DISPLAY).nbytes for j in jobs)
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+    ms = sum(batch_ms) / len(batch_ms)
+    pms = sum(plain_ms) / len(plain_ms)
+    if dist:
+        t = torch.tensor([ms, pms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, pms = float(t[0]), float(t[1])
+    n = len(jobs)
+    if rank == 0:
+        line = {"metric": "scenes/s", "value": n * ws / (ms / 1e3), "unit": "scenes/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator, no dataset)",
+                "config": {"workload": f"{n} instanced-box scenes, {sum(s['n_tris'] for s in specs):,} tris, "
+                                       "256^2-1024^2, 1-64 spp, depth 4-16 (seeded)",
+                           "paths_per_step": sum(j.paths for j in jobs), "parallelism": f"replicas x{ws}",
+                           "scene_build_s": build_s, "autotune_s": tune_s,
+                           "tuned": {"wave_paths": cfg.wave_paths, "extend_block": cfg.extend_block,
+                                     "leaf_size": cfg.leaf_size},
+                           "l2": "wavefront state > L2"},
+                "mrays_per_s": rays * ws / (ms / 1e3) / 1e6,
+                "plain": {"ms_per_step": pms, "scenes_per_s": n * ws / (pms / 1e3),
+                          "mrays_per_s": plain_rays * ws / (pms / 1e3) / 1e6,
+                          "path": "rx_render one scene after another, scenes resident"},
+                "speedup_vs_plain": pms / ms,
+                "preview_1spp": {"batch_ms": sum(prev_b) / len(prev_b), "plain_ms": sum(prev_p) / len(prev_p),
+                                 "batch_scenes_per_s": n * ws / (sum(prev_b) / len(prev_b) / 1e3),
+                                 "plain_scenes_per_s": n * ws / (sum(prev_p) / len(prev_p) / 1e3),
+                                 "speedup": sum(prev_p) / sum(prev_b)},
+                "gpu_launches": launches, "clocks": clocks.summary(),
+                "quality": {"equal_to_plain": "bit-identical images (tests/test_gpu_batch.py), so equal relMSE"},
+                "e2e": {"value": n * ws / (sum(e2e_ms) / len(e2e_ms) / 1e3), "unit": "scenes/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                        "path": "BatchRenderer.render() + read-back of every display image; scenes resident"}}
+        print(json.dumps(line))
+    br.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--scenes", type=int, default=64, help="scenes in the batch workload")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-spp", type=int, default=4096,
                     help="spp of the float64 reference render for relMSE (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -330,7 +330,7 @@ __global__ void k_generate_batch(BatchSrc src, int n_segs, long long total, floa
 }
 
 template <bool EXACT, class Src, int BS>
-__global__ void __launch_bounds__(BS)
+__global__ void __launch_bounds__(BS, Src::kBatch ? 1024 / BS : 1)
     k_extend(Src src, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
              const float4* __restrict__ ray_d, float4* __restrict__ hits, int sb, const float4* __restrict__ shadow,
              float4* __restrict__ rad, long long shadow_cap, int* err) {
@@ -431,7 +431,7 @@ __device__ __forceinline__ int warp_append_n(int cnt, int* counter) {
 }
 
 template <class Src>
-__global__ void __launch_bounds__(128) k_shade(Src src, int b, const int* __restrict__ qin,
+__global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int b, const int* __restrict__ qin,
                                                int* __restrict__ qout, int* counters,
                                                const int* __restrict__ frame_base, float4* __restrict__ ray_o,
                                                float4* __restrict__ ray_d, float4* __restrict__ thr_b,

@@ -24,7 +24,8 @@ enum {
   RX_ERR_CAPACITY = 2,  /* size beyond a limit (the reference asserts)        */
   RX_ERR_CUDA = 3,      /* CUDA runtime error                                 */
   RX_ERR_STATE = 4,     /* call out of order (e.g. render before a BVH)       */
-  RX_ERR_DEVICE = 5     /* a kernel reported an internal error flag           */
+  RX_ERR_DEVICE = 5,    /* a kernel reported an internal error flag           */
+  RX_ERR_TIMEOUT = 6    /* a wait ran out (serving)                           */
 };
 
 enum { RX_BVH_REFERENCE = 0, RX_BVH_LBVH_SAH = 1 };
@@ -236,6 +237,48 @@ int rx_batch_add(rx_batch* batch, rx_scene* scene, rx_accum* acc, const rx_rende
 int rx_batch_set_config(rx_batch* batch, long long wave_paths, int extend_block);
 int rx_batch_render(rx_batch* batch);
 int rx_batch_last_stats(rx_batch* batch, float* ms, int* waves, int* launches);
+
+/* Serving (no reference counterpart: the reference renders one
+ * TaichiRenderer.render call at a time, taichi_renderer.py:87-191).  A host
+ * thread owned by the server admits submitted requests while active slots
+ * and the device-memory budget allow, gives each new request its preview
+ * frames in the next step, then refines admitted requests within a
+ * per-step path budget; every step is one batch of shared wavefronts.
+ * Scenes stay owned by the caller and must outlive their requests; the
+ * server creates and frees each request's accumulator (freed at
+ * rx_serve_release).  Times are seconds since rx_serve_create. */
+typedef struct rx_server rx_server;
+typedef struct {
+  long long hbm_budget;  /* bytes: wave state + accumulators + scenes in use */
+  int max_active;        /* requests rendering at once                        */
+  long long step_paths;  /* paths per serving step (bounds preview latency)   */
+  long long wave_paths;  /* paths per wavefront within a step                 */
+  int extend_block;      /* 64, 128 or 256                                    */
+  int preview_frames;    /* frames of a request's first step                  */
+} rx_serve_config;
+enum { RX_REQ_QUEUED = 0, RX_REQ_ACTIVE = 1, RX_REQ_DONE = 2, RX_REQ_FAILED = 3 };
+typedef struct {
+  int state, frames_done, frames;
+  double t_submit, t_admit, t_preview, t_final; /* -1 until reached */
+  long long bytes;
+} rx_request_info;
+typedef struct {
+  long long steps, admitted, completed, failed;
+  int active, queued, max_active_seen;
+  long long bytes_in_use, max_bytes_in_use;
+  double busy_s, uptime_s;
+} rx_serve_stats;
+int rx_serve_create(rx_ctx* ctx, const rx_serve_config* config, rx_server** out);
+int rx_serve_destroy(rx_server* server);
+int rx_serve_submit(rx_server* server, rx_scene* scene, const rx_render_params* params, int frames, int* request);
+int rx_serve_info(rx_server* server, int request, rx_request_info* out);
+/* until_final 0: wait for the preview; RX_ERR_TIMEOUT after timeout_s */
+int rx_serve_wait(rx_server* server, int request, int until_final, double timeout_s);
+int rx_serve_read(rx_server* server, int request, int which, float* host_out);
+int rx_serve_release(rx_server* server, int request);
+int rx_serve_get_stats(rx_server* server, rx_serve_stats* out);
+/* Device bytes a scene holds (what serving admission charges for it). */
+int rx_scene_device_bytes(rx_scene* scene, long long* bytes);
 
 /* edge_aware_denoise / a-trous on caller host buffers (denoise.py:23-104):
  * color (H,W,3); normal, albedo (H,W,3) and depth (H,W) may be NULL. */

@@ -23,6 +23,10 @@ struct rx_batch {
   rx::Batch* b;
   rx::Ctx* ctx;
 };
+struct rx_server {
+  rx::Server* s;
+  rx::Ctx* ctx;
+};
 
 namespace rx {
 
@@ -735,6 +739,64 @@ int rx_batch_last_stats(rx_batch* b, float* ms, int* waves, int* launches) {
   if (!b) return RX_ERR_ARG;
   LOCK(b->ctx);
   return batch_last_stats(b->b, ms, waves, launches);
+}
+
+int rx_serve_create(rx_ctx* ctx, const rx_serve_config* cfg, rx_server** out) {
+  if (!ctx || !cfg || !out) return set_error(nullptr, "rx_serve_create: NULL argument"), RX_ERR_ARG;
+  if (cfg->hbm_budget <= 0 || cfg->max_active < 1 || cfg->step_paths < 1 || cfg->wave_paths < 1 ||
+      cfg->wave_paths >= (1LL << 31) || cfg->preview_frames < 1 ||
+      (cfg->extend_block != 64 && cfg->extend_block != 128 && cfg->extend_block != 256))
+    return set_error(&ctx->c, "rx_serve_create: bad configuration"), RX_ERR_ARG;
+  rx_server* s = new rx_server();
+  s->s = serve_new(&ctx->c, cfg);
+  s->ctx = &ctx->c;
+  *out = s;
+  return RX_OK;
+}
+
+int rx_serve_destroy(rx_server* s) {
+  if (!s) return RX_OK;
+  serve_delete(s->s);
+  delete s;
+  return RX_OK;
+}
+
+int rx_serve_submit(rx_server* s, rx_scene* scene, const rx_render_params* params, int frames, int* request) {
+  if (!s || !scene || !params || !request) return set_error(s ? s->ctx : nullptr, "rx_serve_submit: NULL argument"),
+                                                    RX_ERR_ARG;
+  return serve_submit(s->s, &scene->s, params, frames, request);
+}
+
+int rx_serve_info(rx_server* s, int request, rx_request_info* out) {
+  if (!s || !out) return RX_ERR_ARG;
+  return serve_info(s->s, request, out);
+}
+
+int rx_serve_wait(rx_server* s, int request, int until_final, double timeout_s) {
+  if (!s) return RX_ERR_ARG;
+  return serve_wait(s->s, request, until_final, timeout_s);
+}
+
+int rx_serve_read(rx_server* s, int request, int which, float* host_out) {
+  if (!s || !host_out) return RX_ERR_ARG;
+  return serve_read(s->s, request, which, host_out);
+}
+
+int rx_serve_release(rx_server* s, int request) {
+  if (!s) return RX_ERR_ARG;
+  return serve_release(s->s, request);
+}
+
+int rx_serve_get_stats(rx_server* s, rx_serve_stats* out) {
+  if (!s || !out) return RX_ERR_ARG;
+  return serve_stats(s->s, out);
+}
+
+int rx_scene_device_bytes(rx_scene* scene, long long* bytes) {
+  if (!scene || !bytes) return RX_ERR_ARG;
+  LOCK(scene->s.ctx);
+  *bytes = (long long)scene_bytes(&scene->s);
+  return RX_OK;
 }
 
 int rx_accum_set_f64(rx_accum* acc, int on) {

@@ -308,6 +308,15 @@ int scene_set_textures(Ctx* c, Scene* s, int n, const int* width, const int* hei
   return RX_OK;
 }
 
+size_t scene_bytes(const Scene* s) {
+  return s->v0b.bytes() + s->v1b.bytes() + s->v2b.bytes() + s->n0b.bytes() + s->n1b.bytes() + s->n2b.bytes() +
+         s->tri_matb.bytes() + s->uvb.bytes() + s->d_tex.bytes() + s->d_texels.bytes() + s->mat_a.bytes() +
+         s->mat_b.bytes() + s->d_objs.bytes() + s->d_lights.bytes() + s->d_alias_prob.bytes() +
+         s->d_alias_idx.bytes() + s->d_nodes.bytes() + s->d_prims.bytes() + s->d_shade.bytes() +
+         s->ref_left.bytes() + s->ref_right.bytes() + s->ref_start.bytes() + s->ref_count.bytes() +
+         s->order.bytes() + s->ref_min.bytes() + s->ref_max.bytes() + s->tmp_codes.bytes();
+}
+
 int scene_get_triangles(Ctx* c, Scene* s, int offset, int n, float* const* rows, int* mat_idx) {
   if (offset < 0 || n < 0 || (long long)offset + n > s->n_tris)
     return set_error(c, "get_triangles: rows [%d, %d) outside the %d present", offset, offset + n, s->n_tris),

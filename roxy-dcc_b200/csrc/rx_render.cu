@@ -1234,6 +1234,7 @@ struct Batch {
   std::vector<BatchJob> jobs;
   long long wave_paths = 1LL << 25;
   int ext_block = 128;
+  bool use_graph = true;
   long long cap = 0, shadow_cap = 0;
   DevBuf<float4> ray_o, ray_d, thr, rad, gn, ga, hits, shadow;
   DevBuf<int> q0, q1, counters, pseg;
@@ -1276,7 +1277,10 @@ int batch_clear(Batch* b) {
 int batch_add(Batch* b, Scene* sc, Accum* acc, const rx_render_params* p, int frames, int* job) {
   Ctx* ctx = b->ctx;
   if (!sc || !acc || !p || frames < 0) return set_error(ctx, "batch_add: bad arguments"), RX_ERR_ARG;
-  if (sc->ctx != ctx || acc->ctx != ctx) return set_error(ctx, "batch_add: job on another context"), RX_ERR_ARG;
+  // scenes may come from another context of the same device (built on its
+  // stream, which its builders synchronise); accumulators are this context's
+  if (sc->ctx->device != ctx->device || acc->ctx != ctx)
+    return set_error(ctx, "batch_add: job on another device or context"), RX_ERR_ARG;
   if (p->width != acc->W || p->height != acc->H)
     return set_error(ctx, "batch_add: %dx%d does not match the accumulator %dx%d", p->width, p->height, acc->W,
                      acc->H),
@@ -1459,7 +1463,7 @@ int batch_render(Batch* B) {
   key_put(key, B->cap);
   key_put(key, B->shadow_cap);
   cudaStream_t st = ctx->stream;
-  bool cached = B->gexec && key == B->g_key;
+  bool cached = B->use_graph && B->gexec && key == B->g_key;
   if (!cached) {
     B->drop_graph();
     if (!B->d_scenes.alloc(ctx, nj) || !B->d_ks.alloc(ctx, nj) || !B->d_accs.alloc(ctx, nj) ||
@@ -1471,23 +1475,34 @@ int batch_render(Batch* B) {
     CUDA_TRY(ctx, cudaMemsetAsync(B->d_job_rays.p, 0, sizeof(unsigned long long) * nj, st));
     CUDA_TRY(ctx, cudaMemcpyAsync(B->d_segs.p, segs.data(), sizeof(WaveSeg) * segs.size(), cudaMemcpyHostToDevice,
                                   st));
-    cudaGraph_t g;
-    CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int nl = 0;
-    enqueue_batch(B, waves, &nl);
-    CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
-    CUDA_TRY(ctx, cudaGraphInstantiate(&B->gexec, g, 0));
-    cudaGraphDestroy(g);
-    B->g_key = key;
-    B->g_launches = nl;
-    B->g_waves = (int)waves.size();
+    if (B->use_graph) {
+      cudaGraph_t g;
+      CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int nl = 0;
+      enqueue_batch(B, waves, &nl);
+      CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+      CUDA_TRY(ctx, cudaGraphInstantiate(&B->gexec, g, 0));
+      cudaGraphDestroy(g);
+      B->g_key = key;
+      B->g_launches = nl;
+      B->g_waves = (int)waves.size();
+    }
   }
   if (!B->e0) {
     CUDA_TRY(ctx, cudaEventCreate(&B->e0));
     CUDA_TRY(ctx, cudaEventCreate(&B->e1));
   }
   CUDA_TRY(ctx, cudaEventRecord(B->e0, st));
-  CUDA_TRY(ctx, cudaGraphLaunch(B->gexec, st));
+  if (B->use_graph) {
+    CUDA_TRY(ctx, cudaGraphLaunch(B->gexec, st));
+  } else {
+    // job sets that change every call (serving): launch directly
+    int nl = 0;
+    enqueue_batch(B, waves, &nl);
+    CUDA_TRY(ctx, cudaGetLastError());
+    B->g_launches = nl;
+    B->g_waves = (int)waves.size();
+  }
   CUDA_TRY(ctx, cudaEventRecord(B->e1, st));
   CUDA_TRY(ctx, cudaEventSynchronize(B->e1));
   CUDA_TRY(ctx, cudaEventElapsedTime(&B->last_ms, B->e0, B->e1));
@@ -1495,6 +1510,23 @@ int batch_render(Batch* B) {
   B->last_launches = B->g_launches;
   for (const BatchJob& j : B->jobs) j.acc->frames += j.frames;
   return check_device_error(ctx);
+}
+
+void batch_use_graph(Batch* B, bool on) {
+  if (!on) B->drop_graph();
+  B->use_graph = on;
+}
+
+size_t accum_bytes(const Accum* a) {
+  return a->acc_r.bytes() + a->acc_n.bytes() + a->acc_a.bytes() + a->pixels.bytes() + a->acc64.bytes() +
+         a->ray_o.bytes() + a->ray_d.bytes() + a->thr.bytes() + a->rad.bytes() + a->gn.bytes() + a->ga.bytes() +
+         a->hits.bytes() + a->shadow.bytes() + a->q0.bytes() + a->q1.bytes() + a->dn0.bytes() + a->dn1.bytes() +
+         a->dn_out.bytes() + 64;
+}
+
+size_t batch_bytes(const Batch* B) {
+  return B->ray_o.bytes() + B->ray_d.bytes() + B->thr.bytes() + B->rad.bytes() + B->gn.bytes() + B->ga.bytes() +
+         B->hits.bytes() + B->shadow.bytes() + B->q0.bytes() + B->q1.bytes() + B->pseg.bytes();
 }
 
 int batch_last_stats(Batch* B, float* ms, int* waves, int* launches) {

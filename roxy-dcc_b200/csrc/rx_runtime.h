@@ -216,6 +216,23 @@ int batch_add(Batch* b, Scene* sc, Accum* acc, const rx_render_params* p, int fr
 int batch_set_config(Batch* b, long long wave_paths, int ext_block);
 int batch_render(Batch* b);
 int batch_last_stats(Batch* b, float* ms, int* waves, int* launches);
+void batch_use_graph(Batch* b, bool on);
+
+// Serving loop (rx_serve.cu)
+struct Server;
+Server* serve_new(Ctx* ctx, const rx_serve_config* cfg);
+void serve_delete(Server* s);
+int serve_submit(Server* s, Scene* sc, const rx_render_params* p, int frames, int* id);
+int serve_info(Server* s, int id, rx_request_info* out);
+int serve_wait(Server* s, int id, int until_final, double timeout_s);
+int serve_read(Server* s, int id, int which, float* host_out);
+int serve_release(Server* s, int id);
+int serve_stats(Server* s, rx_serve_stats* out);
+
+// device bytes held by each object (serving admission)
+size_t accum_bytes(const Accum* a);
+size_t batch_bytes(const Batch* b);
+size_t scene_bytes(const Scene* s);
 
 // Denoise on caller buffers (rx_denoise.cu)
 int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal, const float* albedo,

@@ -1,0 +1,116 @@
+"""Render serving with continuous batching (rx_serve_*).
+
+A RenderServer owns a native serving loop on its own host thread: requests
+(a resident scene, render parameters, a frame count) are admitted as active
+slots and the device-memory budget allow, each gets a preview in the next
+step and is then refined within a per-step path budget, and every step
+traces all admitted requests together as one batch of wavefronts.  Scenes
+and BVHs stay resident; each request's accumulator lives until release().
+
+poisson_run() drives a server with Poisson arrivals and reports latency to
+the first preview and to the final image (p50 / p99) beside throughput.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+import roxy_native as nat
+
+STATE_NAMES = {nat.RX_REQ_QUEUED: "queued", nat.RX_REQ_ACTIVE: "active", nat.RX_REQ_DONE: "done",
+               nat.RX_REQ_FAILED: "failed"}
+
+
+class RenderServer:
+    def __init__(self, hbm_budget=150e9, max_active=256, step_paths=1 << 25, wave_paths=1 << 25, extend_block=128,
+                 preview_frames=1, ctx=None):
+        self.ctx = ctx or nat.context()
+        cfg = nat.ServeConfig(int(hbm_budget), int(max_active), int(step_paths), int(wave_paths), int(extend_block),
+                              int(preview_frames))
+        h = ctypes.c_void_p()
+        self.ctx.check(nat.lib().rx_serve_create(self.ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self._meta = {}
+
+    def submit(self, scene, params, frames):
+        """Queue a request; returns its id.  `scene`: NativeScene (kept
+        alive by the server object until release)."""
+        rid = ctypes.c_int(-1)
+        p = type(params).from_buffer_copy(params)
+        self.ctx.check(nat.lib().rx_serve_submit(self.h, scene.h, ctypes.byref(p), int(frames), ctypes.byref(rid)))
+        self._meta[rid.value] = (scene, p.width, p.height)
+        return rid.value
+
+    def info(self, rid):
+        out = nat.RequestInfo()
+        self.ctx.check(nat.lib().rx_serve_info(self.h, int(rid), ctypes.byref(out)))
+        return {"state": STATE_NAMES[out.state], "frames_done": out.frames_done, "frames": out.frames,
+                "t_submit": out.t_submit, "t_admit": out.t_admit, "t_preview": out.t_preview, "t_final": out.t_final,
+                "bytes": out.bytes}
+
+    def wait(self, rid, final=True, timeout=60.0):
+        self.ctx.check(nat.lib().rx_serve_wait(self.h, int(rid), int(bool(final)), float(timeout)))
+
+    def read(self, rid, which=nat.RX_ACC_DISPLAY):
+        _, w, h = self._meta[rid]
+        shape = (h, w) if which == nat.RX_ACC_DEPTH else (h, w, 3)
+        out = np.zeros(shape, np.float32)
+        self.ctx.check(nat.lib().rx_serve_read(self.h, int(rid), int(which), nat.fptr(out)))
+        return out
+
+    def release(self, rid):
+        self.ctx.check(nat.lib().rx_serve_release(self.h, int(rid)))
+        self._meta.pop(rid, None)
+
+    def stats(self):
+        s = nat.ServeStats()
+        self.ctx.check(nat.lib().rx_serve_get_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in nat.ServeStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and nat._LIB is not None:
+            nat._LIB.rx_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else float("nan")
+
+
+def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0):
+    """Submit `requests` (list of (NativeScene, RenderParams, frames)) with
+    exponential inter-arrival times of mean 1/rate, wait for all, release
+    them, and return latency and throughput figures in seconds."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=len(requests))
+    ids = []
+    t_start = time.perf_counter()
+    t_next = t_start
+    for (scene, params, frames), gap in zip(requests, gaps):
+        t_next += gap
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(server.submit(scene, params, frames))
+    infos = []
+    for rid in ids:
+        server.wait(rid, final=True, timeout=timeout)
+        infos.append(server.info(rid))
+        if read_final:
+            server.read(rid)
+        server.release(rid)
+    t_end = time.perf_counter()
+    prev = [i["t_preview"] - i["t_submit"] for i in infos]
+    fin = [i["t_final"] - i["t_submit"] for i in infos]
+    first = min(i["t_submit"] for i in infos)
+    last = max(i["t_final"] for i in infos)
+    return {"requests": len(ids), "rate": rate, "preview_p50_ms": 1e3 * percentile(prev, 50),
+            "preview_p99_ms": 1e3 * percentile(prev, 99), "final_p50_ms": 1e3 * percentile(fin, 50),
+            "final_p99_ms": 1e3 * percentile(fin, 99), "throughput_rps": len(ids) / max(last - first, 1e-9),
+            "wall_s": t_end - t_start}

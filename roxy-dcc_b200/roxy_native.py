@@ -15,10 +15,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # ROXY_CUDA_LIB selects another build of the library (e.g. an installed copy)
 LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
-SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu"]
+SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu",
+           "rx_serve.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
 
-RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE = range(6)
+RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE, RX_ERR_TIMEOUT = range(7)
+RX_REQ_QUEUED, RX_REQ_ACTIVE, RX_REQ_DONE, RX_REQ_FAILED = range(4)
 RX_BVH_REFERENCE, RX_BVH_LBVH_SAH = 0, 1
 RX_ACC_RADIANCE, RX_ACC_NORMAL, RX_ACC_ALBEDO, RX_ACC_DEPTH, RX_ACC_DISPLAY = range(5)
 
@@ -46,6 +48,24 @@ class RenderParams(ctypes.Structure):
         ("sample_clamp", ctypes.c_float), ("reference_compat", ctypes.c_int), ("seed", ctypes.c_uint32),
         ("wave_paths", ctypes.c_int),
     ]
+
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_longlong), ("max_active", ctypes.c_int), ("step_paths", ctypes.c_longlong),
+                ("wave_paths", ctypes.c_longlong), ("extend_block", ctypes.c_int), ("preview_frames", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("frames_done", ctypes.c_int), ("frames", ctypes.c_int),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_preview", ctypes.c_double),
+                ("t_final", ctypes.c_double), ("bytes", ctypes.c_longlong)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("admitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("active", ctypes.c_int), ("queued", ctypes.c_int),
+                ("max_active_seen", ctypes.c_int), ("bytes_in_use", ctypes.c_longlong),
+                ("max_bytes_in_use", ctypes.c_longlong), ("busy_s", ctypes.c_double), ("uptime_s", ctypes.c_double)]
 
 
 class DenoiseParams(ctypes.Structure):
@@ -133,6 +153,16 @@ _SIGS = {
     "rx_batch_render": ([ctypes.c_void_p], ctypes.c_int),
     "rx_batch_last_stats": ([ctypes.c_void_p, _f32p, _i32p, _i32p], ctypes.c_int),
     "rx_accum_read_f64": ([ctypes.c_void_p, _f64p], ctypes.c_int),
+    "rx_serve_create": ([ctypes.c_void_p, ctypes.POINTER(ServeConfig), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rx_serve_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_serve_submit": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(RenderParams), ctypes.c_int, _i32p],
+                        ctypes.c_int),
+    "rx_serve_info": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(RequestInfo)], ctypes.c_int),
+    "rx_serve_wait": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double], ctypes.c_int),
+    "rx_serve_read": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p], ctypes.c_int),
+    "rx_serve_release": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_serve_get_stats": ([ctypes.c_void_p, ctypes.POINTER(ServeStats)], ctypes.c_int),
+    "rx_scene_device_bytes": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_denoise_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -199,6 +229,8 @@ class Context:
             msg = msg.decode() if msg else f"error {rc}"
             if rc == RX_ERR_ARG:
                 raise ValueError(msg)
+            if rc == RX_ERR_TIMEOUT:
+                raise TimeoutError(msg)
             if rc == RX_ERR_CAPACITY:
                 raise AssertionError(msg)
             raise RxError(rc, msg)
@@ -324,6 +356,11 @@ class NativeScene:
         mat = np.empty(n, np.int32)
         self.ctx.check(lib().rx_scene_get_triangles(self.h, int(offset), n, *[fptr(a) for a in out], iptr(mat)))
         return dict(zip(("v0", "v1", "v2", "n0", "n1", "n2"), out), mat_idx=mat)
+
+    def device_bytes(self):
+        n = ctypes.c_longlong()
+        self.ctx.check(lib().rx_scene_device_bytes(self.h, ctypes.byref(n)))
+        return n.value
 
     def set_materials(self, mat_type, albedo, roughness, ior, emission):
         t = i32(mat_type)

@@ -175,9 +175,9 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    if args.workload == "batch":
-        print(json.dumps({"impl": "reference", "unavailable": "the batched workload's baseline is the plain "
-                                                              "one-scene-at-a-time GPU path reported in its own line"}))
+    if args.workload in ("batch", "serve"):
+        print(json.dumps({"impl": "reference", "unavailable": "the batched and serving workloads' baseline is the "
+                                                              "plain one-scene-at-a-time GPU path in their own line"}))
         return 0
     world = _world(args.workload)
     w = WORKLOADS[args.workload]
@@ -523,14 +523,82 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Serving configuration: Poisson arrivals at swept rates; each request
+    renders one of four displaced-icosphere scenes (the large-mesh
+    generator, seeds 2024-2027, resident on the device) at a resolution
+    from {256^2, 512^2, 1024^2} and spp from {1, 4, 16, 64}, max depth 12.
+    The batched server (continuous batching, 150 GB admission budget, 1-spp
+    preview first) is compared with the plain path: the same server with
+    one active request at a time.  Every rate uses the same seeded request
+    list (the first N of one draw)."""
+    import roxy_native as nat
+    import workloads
+    from rendering.batch import Job
+    from rendering.serving import RenderServer, poisson_run
+
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    ctx = nat.context(0)
+    t0 = time.perf_counter()
+    pool = [Job(workloads.displaced_icosphere_scene(64, 64, seed=2024 + k), 64, 64, 1, 12).prepare(ctx=ctx)
+            for k in range(4)]
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(99)
+    all_reqs = []
+    for _ in range(args.max_requests):
+        base = pool[int(rng.integers(0, len(pool)))]
+        res = int(rng.choice([256, 512, 1024]))
+        spp = int(rng.choice([1, 4, 16, 64]))
+        j = Job(base.world, res, res, spp, 12, scene=base.scene, seed=int(rng.integers(0, 1 << 30))).prepare(ctx=ctx)
+        all_reqs.append((j.scene.native, j.params, j.spp))
+    rates = [float(r) for r in args.rates.split(",")]
+    rows = []
+    for rate in rates:
+        n = int(min(max(rate * args.duration, 20), args.max_requests))
+        reqs = all_reqs[:n]
+        row = {"rate_rps": rate, "requests": n}
+        for name, kw in (("batched", dict(max_active=1024, step_paths=1 << 23)),
+                         ("plain", dict(max_active=1, step_paths=1 << 40))):
+            srv = RenderServer(hbm_budget=150e9, wave_paths=1 << 25, preview_frames=1, ctx=ctx, **kw)
+            poisson_run(srv, all_reqs[-8:], rate=rate, seed=1)  # warm
+            st0 = srv.stats()
+            with ClockSampler(0) as clocks:
+                r = poisson_run(srv, reqs, rate=rate, seed=2)
+            st = srv.stats()
+            srv.close()
+            row[name] = {k: r[k] for k in ("preview_p50_ms", "preview_p99_ms", "final_p50_ms", "final_p99_ms",
+                                           "throughput_rps")}
+            row[name].update(max_active=st["max_active_seen"], max_gb=st["max_bytes_in_use"] / 1e9,
+                             steps=st["steps"] - st0["steps"], busy_s=st["busy_s"] - st0["busy_s"],
+                             clocks=clocks.summary())
+        rows.append(row)
+    top = rows[-1]
+    line = {"metric": "requests/s", "value": top["batched"]["throughput_rps"], "unit": "requests/s", "n_gpus": 1,
+            "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": "Poisson arrivals, 4 resident displaced-icosphere scenes (327,680 tris + 64 "
+                                   "spheres), 256^2-1024^2, 1-64 spp, depth 12, 150 GB budget, 1-spp preview",
+                       "scene_build_s": build_s, "rates_rps": rates},
+            "sweep": rows,
+            "speedup_vs_plain_at_top_rate": top["batched"]["throughput_rps"] / top["plain"]["throughput_rps"],
+            "preview_p99_ms_at_top_rate": top["batched"]["preview_p99_ms"]}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS) + ["batch", "serve"])
     ap.add_argument("--scenes", type=int, default=64, help="scenes in the batch workload")
+    ap.add_argument("--rates", default="10,50,100,200,500", help="serve workload: arrival rates (req/s)")
+    ap.add_argument("--duration", type=float, default=3.0, help="serve workload: seconds of arrivals per rate")
+    ap.add_argument("--max-requests", type=int, default=600, help="serve workload: requests per rate at most")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-spp", type=int, default=4096,
                     help="spp of the float64 reference render for relMSE (0: skip)")
@@ -539,6 +607,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -127,6 +127,16 @@ int rx_ctx_create(int device, rx_ctx** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->c.num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) {
+    // stream-ordered allocations keep freed memory in the device pool, so
+    // accumulators and wave state of later requests reuse it without new
+    // mappings
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      unsigned long long keep = ~0ULL;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   if (e == cudaSuccess) e = cudaMalloc(&c->c.d_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->c.d_err, 0, sizeof(int));
   if (e != cudaSuccess) {

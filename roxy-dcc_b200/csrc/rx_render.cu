@@ -1512,6 +1512,33 @@ int batch_render(Batch* B) {
   return check_device_error(ctx);
 }
 
+int batch_reserve(Batch* B, long long cap) {
+  Ctx* ctx = B->ctx;
+  if (cap > B->cap) {
+    B->drop_graph();
+    bool ok = B->ray_o.alloc(ctx, cap) && B->ray_d.alloc(ctx, cap) && B->thr.alloc(ctx, cap) &&
+              B->rad.alloc(ctx, cap) && B->gn.alloc(ctx, cap) && B->ga.alloc(ctx, cap) && B->hits.alloc(ctx, cap) &&
+              B->q0.alloc(ctx, cap) && B->q1.alloc(ctx, cap) && B->pseg.alloc(ctx, cap);
+    if (!ok) {
+      B->cap = 0;
+      return set_error(ctx, "batch_reserve: out of device memory for %lld wavefront paths", cap), RX_ERR_CAPACITY;
+    }
+    B->cap = cap;
+  }
+  if (cap > B->shadow_cap) {
+    B->drop_graph();
+    if (!B->shadow.alloc(ctx, (size_t)3 * cap)) {
+      B->shadow_cap = 0;
+      return set_error(ctx, "batch_reserve: out of device memory for %lld shadow rays", cap), RX_ERR_CAPACITY;
+    }
+    B->shadow_cap = cap;
+  }
+  if (!B->counters.p && !B->counters.alloc(ctx, C_N))
+    return set_error(ctx, "batch_reserve: out of device memory"), RX_ERR_CAPACITY;
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RX_OK;
+}
+
 void batch_use_graph(Batch* B, bool on) {
   if (!on) B->drop_graph();
   B->use_graph = on;

@@ -217,6 +217,7 @@ int batch_set_config(Batch* b, long long wave_paths, int ext_block);
 int batch_render(Batch* b);
 int batch_last_stats(Batch* b, float* ms, int* waves, int* launches);
 void batch_use_graph(Batch* b, bool on);
+int batch_reserve(Batch* b, long long cap);
 
 // Serving loop (rx_serve.cu)
 struct Server;

@@ -200,9 +200,16 @@ Server* serve_new(Ctx* ctx, const rx_serve_config* cfg) {
   S->batch = batch_new(ctx);
   batch_use_graph(S->batch, false);
   batch_set_config(S->batch, cfg->wave_paths, cfg->extend_block);
-  // the shared wave state is reserved up front
-  S->used = wave_need(std::min(cfg->wave_paths, std::max(cfg->step_paths, (long long)1)));
+  // the shared wave state is reserved up front and allocated now, so the
+  // first requests do not wait for it
+  long long cap = std::min(cfg->wave_paths, std::max(cfg->step_paths, (long long)1));
+  S->used = wave_need(cap);
   S->max_used = S->used;
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    batch_reserve(S->batch, cap);
+  }
   S->th = std::thread(serve_loop, S);
   return S;
 }

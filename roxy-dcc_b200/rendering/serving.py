@@ -85,32 +85,55 @@ def percentile(xs, q):
 
 def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0):
     """Submit `requests` (list of (NativeScene, RenderParams, frames)) with
-    exponential inter-arrival times of mean 1/rate, wait for all, release
-    them, and return latency and throughput figures in seconds."""
+    exponential inter-arrival times of mean 1/rate.  A second thread plays
+    the client that waits for each final image, reads it if asked and
+    releases the request as soon as it is done, while arrivals continue.
+    Returns latency and throughput figures."""
+    import queue
+    import threading
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, size=len(requests))
-    ids = []
+    ids = queue.Queue()
+    infos, errors = [], []
+
+    def collect():
+        for _ in range(len(requests)):
+            rid = ids.get()
+            if rid is None:
+                return
+            try:
+                server.wait(rid, final=True, timeout=timeout)
+                infos.append(server.info(rid))
+                if read_final:
+                    server.read(rid)
+                server.release(rid)
+            except Exception as e:  # re-raised after the run
+                errors.append(e)
+
+    th = threading.Thread(target=collect, daemon=True)
+    th.start()
     t_start = time.perf_counter()
     t_next = t_start
-    for (scene, params, frames), gap in zip(requests, gaps):
-        t_next += gap
-        delay = t_next - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(server.submit(scene, params, frames))
-    infos = []
-    for rid in ids:
-        server.wait(rid, final=True, timeout=timeout)
-        infos.append(server.info(rid))
-        if read_final:
-            server.read(rid)
-        server.release(rid)
+    try:
+        for (scene, params, frames), gap in zip(requests, gaps):
+            t_next += gap
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.put(server.submit(scene, params, frames))
+    except Exception:
+        ids.put(None)
+        th.join()
+        raise
+    th.join()
+    if errors:
+        raise errors[0]
     t_end = time.perf_counter()
     prev = [i["t_preview"] - i["t_submit"] for i in infos]
     fin = [i["t_final"] - i["t_submit"] for i in infos]
     first = min(i["t_submit"] for i in infos)
     last = max(i["t_final"] for i in infos)
-    return {"requests": len(ids), "rate": rate, "preview_p50_ms": 1e3 * percentile(prev, 50),
+    return {"requests": len(infos), "rate": rate, "preview_p50_ms": 1e3 * percentile(prev, 50),
             "preview_p99_ms": 1e3 * percentile(prev, 99), "final_p50_ms": 1e3 * percentile(fin, 50),
-            "final_p99_ms": 1e3 * percentile(fin, 99), "throughput_rps": len(ids) / max(last - first, 1e-9),
+            "final_p99_ms": 1e3 * percentile(fin, 99), "throughput_rps": len(infos) / max(last - first, 1e-9),
             "wall_s": t_end - t_start}

@@ -255,6 +255,8 @@ typedef struct {
   long long wave_paths;  /* paths per wavefront within a step                 */
   int extend_block;      /* 64, 128 or 256                                    */
   int preview_frames;    /* frames of a request's first step                  */
+  long long pool_prewarm; /* bytes mapped into the device allocation pool at
+                             start, so admitting requests later maps none    */
 } rx_serve_config;
 enum { RX_REQ_QUEUED = 0, RX_REQ_ACTIVE = 1, RX_REQ_DONE = 2, RX_REQ_FAILED = 3 };
 typedef struct {

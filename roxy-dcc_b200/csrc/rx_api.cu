@@ -754,7 +754,7 @@ int rx_batch_last_stats(rx_batch* b, float* ms, int* waves, int* launches) {
 int rx_serve_create(rx_ctx* ctx, const rx_serve_config* cfg, rx_server** out) {
   if (!ctx || !cfg || !out) return set_error(nullptr, "rx_serve_create: NULL argument"), RX_ERR_ARG;
   if (cfg->hbm_budget <= 0 || cfg->max_active < 1 || cfg->step_paths < 1 || cfg->wave_paths < 1 ||
-      cfg->wave_paths >= (1LL << 31) || cfg->preview_frames < 1 ||
+      cfg->wave_paths >= (1LL << 31) || cfg->preview_frames < 1 || cfg->pool_prewarm < 0 ||
       (cfg->extend_block != 64 && cfg->extend_block != 128 && cfg->extend_block != 256))
     return set_error(&ctx->c, "rx_serve_create: bad configuration"), RX_ERR_ARG;
   rx_server* s = new rx_server();

@@ -209,6 +209,16 @@ Server* serve_new(Ctx* ctx, const rx_serve_config* cfg) {
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     batch_reserve(S->batch, cap);
+    // map memory into the stream-ordered pool now (the context keeps freed
+    // pool memory), so admitting many requests later allocates accumulators
+    // from memory that is already mapped
+    long long warm = std::min(cfg->pool_prewarm, cfg->hbm_budget - S->used);
+    if (warm > 0) {
+      void* p = nullptr;
+      if (cudaMallocAsync(&p, (size_t)warm, ctx->stream) == cudaSuccess) cudaFreeAsync(p, ctx->stream);
+      else cudaGetLastError();
+      cudaStreamSynchronize(ctx->stream);
+    }
   }
   S->th = std::thread(serve_loop, S);
   return S;

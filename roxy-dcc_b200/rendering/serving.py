@@ -23,10 +23,12 @@ STATE_NAMES = {nat.RX_REQ_QUEUED: "queued", nat.RX_REQ_ACTIVE: "active", nat.RX_
 
 class RenderServer:
     def __init__(self, hbm_budget=150e9, max_active=256, step_paths=1 << 25, wave_paths=1 << 25, extend_block=128,
-                 preview_frames=1, ctx=None):
+                 preview_frames=1, pool_prewarm=None, ctx=None):
         self.ctx = ctx or nat.context()
+        if pool_prewarm is None:
+            pool_prewarm = min(hbm_budget / 8, 16e9)
         cfg = nat.ServeConfig(int(hbm_budget), int(max_active), int(step_paths), int(wave_paths), int(extend_block),
-                              int(preview_frames))
+                              int(preview_frames), int(pool_prewarm))
         h = ctypes.c_void_p()
         self.ctx.check(nat.lib().rx_serve_create(self.ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

@@ -52,7 +52,8 @@ class RenderParams(ctypes.Structure):
 
 class ServeConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_longlong), ("max_active", ctypes.c_int), ("step_paths", ctypes.c_longlong),
-                ("wave_paths", ctypes.c_longlong), ("extend_block", ctypes.c_int), ("preview_frames", ctypes.c_int)]
+                ("wave_paths", ctypes.c_longlong), ("extend_block", ctypes.c_int), ("preview_frames", ctypes.c_int),
+                ("pool_prewarm", ctypes.c_longlong)]
 
 
 class RequestInfo(ctypes.Structure):

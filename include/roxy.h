@@ -282,6 +282,66 @@ int rx_serve_get_stats(rx_server* server, rx_serve_stats* out);
 /* Device bytes a scene holds (what serving admission charges for it). */
 int rx_scene_device_bytes(rx_scene* scene, long long* bytes);
 
+/* Learned denoiser kernels (no reference counterpart; the reference's only
+ * denoiser is edge_aware_denoise, denoise.py:23-104).  BF16 tensor-core 3x3
+ * convolutions (stride 1, zero padding 1) with FP32 accumulation on NHWC
+ * device tensors, and the element-wise layers of the network around them.
+ * All pointers are device pointers; `stream` NULL means the context's
+ * stream.  Activations are viewed through a channel stride and offset (a
+ * concatenation is a wider tensor); channel counts are multiples of 16,
+ * strides and offsets multiples of 8.  Weights: [Cout][3][3][Cin] bf16. */
+typedef struct {
+  int N, H, W;            /* images, height, width                    */
+  int Cin, Cout;          /* input / output channels                  */
+  int x_cstride, x_coff;  /* input view: channel stride and offset    */
+  int y_cstride, y_coff;  /* output view                              */
+} rx_conv_desc;
+/* y = act(conv(x, w) + bias); relu != 0 applies max(., 0); y32 (optional)
+ * receives the same values in float32 */
+int rx_conv_bf16_fwd(rx_ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y,
+                     float* y32, int relu, void* stream);
+/* dx = gradient of the input for output gradient dy (in the y view);
+ * w_rot: Cout*9*Cin bf16 of scratch the caller provides */
+int rx_conv_bf16_bwd_data(rx_ctx* ctx, const rx_conv_desc* d, const void* dy, const void* w, void* w_rot, void* dx,
+                          void* stream);
+/* dw += gradient of the weights (float32 [Cout][3][3][Cin]); dbias (optional) += bias gradient */
+int rx_conv_bf16_bwd_weight(rx_ctx* ctx, const rx_conv_desc* d, const void* dy, const void* x, float* dw,
+                            float* dbias, void* stream);
+enum { RX_DN_COPY = 0, RX_DN_RELU_MASK = 1, RX_DN_POOL = 2, RX_DN_POOL_BWD = 3, RX_DN_UP = 4, RX_DN_UP_BWD = 5 };
+/* One element-wise layer from view a to view b (bf16, NHWC):
+ *   COPY       b[..c] = a (flag: b += a), C channels, N x H x W pixels
+ *   RELU_MASK  b = 0 where a <= 0 (a: a ReLU's output, b: its gradient)
+ *   POOL       2x2 average, a is H x W, b is H/2 x W/2
+ *   POOL_BWD   a is the H/2 x W/2 gradient, b (H x W) = a / 4 (flag: +=)
+ *   UP         nearest 2x, a is H x W, b is 2H x 2W
+ *   UP_BWD     a is the 2H x 2W gradient, b (H x W) = sum of 4 children */
+typedef struct {
+  int kind, N, H, W, C;
+  const void* a;
+  int a_stride, a_off;
+  void* b;
+  int b_stride, b_off;
+  int flag;
+} rx_dn_op;
+int rx_dn_layer(rx_ctx* ctx, const rx_dn_op* op, void* stream);
+/* 16-channel bf16 network input (log1p radiance, albedo, normal,
+ * depth/(1+depth), zeros) from float32 planes of P pixels; base (optional,
+ * float32 P x 3) receives log1p(radiance), the image the network corrects */
+int rx_dn_features(rx_ctx* ctx, long long P, const float* radiance, const float* albedo, const float* normal,
+                   const float* depth, void* out, float* base, void* stream);
+/* L1 loss of y + base (first 3 channels of y32; base optional) against the
+ * log1p target (P,3): *loss += sum |y + base - t|; grad (bf16, grad_stride
+ * channels) = sign(y + base - t) * scale */
+int rx_dn_l1_loss(rx_ctx* ctx, long long P, const float* y32, int y_stride, const float* base, const float* target,
+                  float scale, void* grad, int grad_stride, float* loss, void* stream);
+/* radiance (P,3) = max(expm1(y + base), 0) (base optional) */
+int rx_dn_output(rx_ctx* ctx, long long P, const float* y32, int y_stride, const float* base, float* out,
+                 void* stream);
+/* Adam step `step` (1-based) on n float32 parameters; writes their bf16
+ * copy p16 (optional) and clears g */
+int rx_dn_adam(rx_ctx* ctx, long long n, float* p, float* g, float* m, float* v, void* p16, float lr, float b1,
+               float b2, float eps, int step, void* stream);
+
 /* edge_aware_denoise / a-trous on caller host buffers (denoise.py:23-104):
  * color (H,W,3); normal, albedo (H,W,3) and depth (H,W) may be NULL. */
 int rx_denoise(rx_ctx* ctx, int height, int width, const float* color, const float* normal, const float* albedo,

@@ -802,6 +802,66 @@ int rx_serve_get_stats(rx_server* s, rx_serve_stats* out) {
   return serve_stats(s->s, out);
 }
 
+static cudaStream_t pick_stream(rx_ctx* ctx, void* stream) {
+  return stream ? (cudaStream_t)stream : ctx->c.stream;
+}
+
+int rx_conv_bf16_fwd(rx_ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y,
+                     float* y32, int relu, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return conv_fwd(&ctx->c, d, x, w, bias, y, y32, relu, pick_stream(ctx, stream));
+}
+
+int rx_conv_bf16_bwd_data(rx_ctx* ctx, const rx_conv_desc* d, const void* dy, const void* w, void* w_rot, void* dx,
+                          void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return conv_bwd_data(&ctx->c, d, dy, w, w_rot, dx, pick_stream(ctx, stream));
+}
+
+int rx_conv_bf16_bwd_weight(rx_ctx* ctx, const rx_conv_desc* d, const void* dy, const void* x, float* dw,
+                            float* dbias, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return conv_bwd_weight(&ctx->c, d, dy, x, dw, dbias, pick_stream(ctx, stream));
+}
+
+int rx_dn_layer(rx_ctx* ctx, const rx_dn_op* op, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return dn_op(&ctx->c, op, pick_stream(ctx, stream));
+}
+
+int rx_dn_features(rx_ctx* ctx, long long P, const float* radiance, const float* albedo, const float* normal,
+                   const float* depth, void* out, float* base, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return dn_features(&ctx->c, P, radiance, albedo, normal, depth, out, base, pick_stream(ctx, stream));
+}
+
+int rx_dn_l1_loss(rx_ctx* ctx, long long P, const float* y32, int y_stride, const float* base, const float* target,
+                  float scale, void* grad, int grad_stride, float* loss, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return dn_l1_loss(&ctx->c, P, y32, y_stride, base, target, scale, grad, grad_stride, loss,
+                    pick_stream(ctx, stream));
+}
+
+int rx_dn_output(rx_ctx* ctx, long long P, const float* y32, int y_stride, const float* base, float* out,
+                 void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return dn_output(&ctx->c, P, y32, y_stride, base, out, pick_stream(ctx, stream));
+}
+
+int rx_dn_adam(rx_ctx* ctx, long long n, float* p, float* g, float* m, float* v, void* p16, float lr, float b1,
+               float b2, float eps, int step, void* stream) {
+  if (!ctx) return RX_ERR_ARG;
+  cudaSetDevice(ctx->c.device);
+  return dn_adam(&ctx->c, n, p, g, m, v, p16, lr, b1, b2, eps, step, pick_stream(ctx, stream));
+}
+
 int rx_scene_device_bytes(rx_scene* scene, long long* bytes) {
   if (!scene || !bytes) return RX_ERR_ARG;
   LOCK(scene->s.ctx);

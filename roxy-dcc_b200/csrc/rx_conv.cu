@@ -1,0 +1,621 @@
+// BF16 tensor-core kernels of the learned denoiser: 3x3 convolutions
+// (forward, gradient of the input, gradient of the weights) as implicit
+// GEMMs with FP32 accumulation, and the small element-wise layers around
+// them (2x2 average pool, nearest 2x upsample, channel copies for the skip
+// concatenations, ReLU masks, loss, Adam).
+//
+// Layout: activations NHWC bf16, read and written through a channel stride
+// and offset so that a concatenated buffer is just a wider tensor;
+// weights [Cout][3][3][Cin] bf16 (K = tap * Cin + ci), biases fp32.
+// Channel counts are multiples of 16.
+//
+// Tensor-core path: tiles staged in shared memory by cp.async (16-byte
+// copies, zero-filled outside the image), fragments loaded with ldmatrix
+// and multiplied with mma.sync m16n8k16 bf16 -> f32.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "rx_internal.cuh"
+#include "rx_runtime.h"
+
+namespace rx {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// 16-byte global -> shared copy; `valid` false writes zeros (no bytes read)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem),
+               "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// ------------------------------------------------------------- forward conv
+// y[p][co] = act(bias[co] + sum_{tap, ci} x[p + off(tap)][ci] * w[co][tap][ci])
+// GEMM: M = pixels (64 per block), N = output channels (BN per block),
+// K = 9 taps x Cin, BK channels per stage.  4 warps as 2 (M) x 2 (N).
+template <int BN, int BK>
+__global__ void __launch_bounds__(128) k_conv_fwd(rx_conv_desc d, const bf16* __restrict__ x,
+                                                  const bf16* __restrict__ w, const float* __restrict__ bias,
+                                                  bf16* __restrict__ y, float* __restrict__ y32, int relu) {
+  constexpr int BM = 64, LDS = BK + 8;
+  constexpr int KC = BK / 8;              // 16-byte chunks per row
+  constexpr int A_PER = BM * KC / 128;    // A chunks per thread
+  constexpr int B_CH = BN * KC;           // B chunks per stage
+  constexpr int NT = BN / 16;             // n8 tiles per warp
+  __shared__ __align__(16) bf16 sA[2][BM][LDS];
+  __shared__ __align__(16) bf16 sB[2][BN][LDS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const long long HW = (long long)d.H * d.W;
+  const long long P = (long long)d.N * HW;
+  const long long m0 = (long long)blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  const int CB = d.Cin / BK;
+  const int KT = 9 * CB;
+
+  int a_row[A_PER], a_kc[A_PER], a_y[A_PER], a_x[A_PER];
+  long long a_img[A_PER];
+  bool a_ok[A_PER];
+#pragma unroll
+  for (int i = 0; i < A_PER; ++i) {
+    int c = tid + i * 128;
+    a_row[i] = c / KC;
+    a_kc[i] = c % KC;
+    long long pix = m0 + a_row[i];
+    a_ok[i] = pix < P;
+    long long n = a_ok[i] ? pix / HW : 0;
+    long long r = a_ok[i] ? pix - n * HW : 0;
+    a_img[i] = n * HW;
+    a_y[i] = (int)(r / d.W);
+    a_x[i] = (int)(r % d.W);
+  }
+
+  auto load = [&](int kt, int buf) {
+    int tap = kt / CB, c0 = (kt % CB) * BK;
+    int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+    for (int i = 0; i < A_PER; ++i) {
+      int yy = a_y[i] + dy, xx = a_x[i] + dx;
+      bool ok = a_ok[i] && yy >= 0 && yy < d.H && xx >= 0 && xx < d.W;
+      const bf16* src =
+          ok ? x + (a_img[i] + (long long)yy * d.W + xx) * d.x_cstride + d.x_coff + c0 + a_kc[i] * 8 : x;
+      cp_async16(&sA[buf][a_row[i]][a_kc[i] * 8], src, ok);
+    }
+    for (int c = tid; c < B_CH; c += 128) {
+      int row = c / KC, kc = c % KC;
+      int co = n0 + row;
+      bool ok = co < d.Cout;
+      const bf16* src = ok ? w + ((long long)co * 9 + tap) * d.Cin + c0 + kc * 8 : w;
+      cp_async16(&sB[buf][row][kc * 8], src, ok);
+    }
+  };
+
+  float acc[2][NT][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
+
+  load(0, 0);
+  cp_async_commit();
+  for (int kt = 0; kt < KT; ++kt) {
+    int buf = kt & 1;
+    if (kt + 1 < KT) load(kt + 1, buf ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < BK / 16; ++ks) {
+      uint32_t af[2][4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+        ldsm_x4(af[mi], &sA[buf][wm * 32 + mi * 16 + (lane & 15)][ks * 16 + (lane >> 4) * 8]);
+#pragma unroll
+      for (int nj = 0; nj < NT / 2; ++nj) {
+        uint32_t bfr[4];
+        ldsm_x4(bfr, &sB[buf][wn * (BN / 2) + nj * 16 + (lane & 7) + (lane >> 4) * 8][ks * 16 + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          mma_bf16(acc[mi][2 * nj], af[mi], bfr[0], bfr[1]);
+          mma_bf16(acc[mi][2 * nj + 1], af[mi], bfr[2], bfr[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        long long m = m0 + wm * 32 + mi * 16 + g + h * 8;
+        int co = n0 + wn * (BN / 2) + ni * 8 + 2 * t;
+        if (m >= P || co >= d.Cout) continue;
+        float v0 = acc[mi][ni][2 * h], v1 = acc[mi][ni][2 * h + 1];
+        if (bias) {
+          v0 += bias[co];
+          v1 += bias[co + 1];
+        }
+        if (relu) {
+          v0 = fmaxf(v0, 0.0f);
+          v1 = fmaxf(v1, 0.0f);
+        }
+        *reinterpret_cast<__nv_bfloat162*>(y + m * d.y_cstride + d.y_coff + co) = __floats2bfloat162_rn(v0, v1);
+        if (y32) {
+          y32[m * d.y_cstride + d.y_coff + co] = v0;
+          y32[m * d.y_cstride + d.y_coff + co + 1] = v1;
+        }
+      }
+}
+
+// ------------------------------------------------------- weight gradient
+// dw[co][tap][ci] += sum_p dy[p][co] * x[p + off(tap)][ci]
+// GEMM: M = output channels (64), N = input channels (64), K = pixels
+// (32 per stage, `pix_per_block` per block, split-K with atomics).
+__global__ void __launch_bounds__(128) k_conv_wgrad(rx_conv_desc d, const bf16* __restrict__ dy,
+                                                    const bf16* __restrict__ x, float* __restrict__ dw,
+                                                    int pix_per_block) {
+  constexpr int BM = 64, BN = 64, BK = 32, LDA = BM + 8, LDB = BN + 8;
+  __shared__ __align__(16) bf16 sA[2][BK][LDA];
+  __shared__ __align__(16) bf16 sB[2][BK][LDB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const long long HW = (long long)d.H * d.W;
+  const long long P = (long long)d.N * HW;
+  const int tap = blockIdx.z;
+  const int dyo = tap / 3 - 1, dxo = tap % 3 - 1;
+  const int co_blocks = (d.Cout + BM - 1) / BM;
+  const int co0 = (blockIdx.y % co_blocks) * BM;
+  const int ci0 = (blockIdx.y / co_blocks) * BN;
+  const long long p_begin = (long long)blockIdx.x * pix_per_block;
+  const long long p_end = P < p_begin + pix_per_block ? P : p_begin + pix_per_block;
+  const int KT = (int)((p_end - p_begin + BK - 1) / BK);
+
+  auto load = [&](int kt, int buf) {
+    long long pb = p_begin + (long long)kt * BK;
+    // 32 pixels x 8 chunks of dy and of x: 256 chunks each, 2 per thread
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      int c = tid + i * 128;
+      int r = c >> 3, kc = c & 7;
+      long long p = pb + r;
+      bool pok = p < p_end;
+      int co = co0 + kc * 8;
+      bool ok = pok && co < d.Cout;
+      const bf16* src = ok ? dy + p * d.y_cstride + d.y_coff + co : dy;
+      cp_async16(&sA[buf][r][kc * 8], src, ok);
+      long long n = pok ? p / HW : 0;
+      long long rem = pok ? p - n * HW : 0;
+      int yy = (int)(rem / d.W) + dyo, xx = (int)(rem % d.W) + dxo;
+      int ci = ci0 + kc * 8;
+      bool okx = pok && ci < d.Cin && yy >= 0 && yy < d.H && xx >= 0 && xx < d.W;
+      const bf16* srcx = okx ? x + (n * HW + (long long)yy * d.W + xx) * d.x_cstride + d.x_coff + ci : x;
+      cp_async16(&sB[buf][r][kc * 8], srcx, okx);
+    }
+  };
+
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.0f;
+
+  if (KT > 0) {
+    load(0, 0);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < KT; ++kt) {
+    int buf = kt & 1;
+    if (kt + 1 < KT) load(kt + 1, buf ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < BK / 16; ++ks) {
+      const int j = lane >> 3, r = lane & 7;
+      uint32_t af[2][4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+        ldsm_x4_t(af[mi], &sA[buf][ks * 16 + r + (j >> 1) * 8][wm * 32 + mi * 16 + (j & 1) * 8]);
+#pragma unroll
+      for (int nj = 0; nj < 2; ++nj) {
+        uint32_t bfr[4];
+        ldsm_x4_t(bfr, &sB[buf][ks * 16 + r + (j & 1) * 8][wn * 32 + nj * 16 + (j >> 1) * 8]);
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          mma_bf16(acc[mi][2 * nj], af[mi], bfr[0], bfr[1]);
+          mma_bf16(acc[mi][2 * nj + 1], af[mi], bfr[2], bfr[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        int co = co0 + wm * 32 + mi * 16 + g + h * 8;
+        int ci = ci0 + wn * 32 + ni * 8 + 2 * t;
+        if (co >= d.Cout || ci >= d.Cin) continue;
+        float* dst = dw + ((long long)co * 9 + tap) * d.Cin + ci;
+        atomicAdd(dst, acc[mi][ni][2 * h]);
+        atomicAdd(dst + 1, acc[mi][ni][2 * h + 1]);
+      }
+}
+
+// dbias[co] += sum_p dy[p][co]
+__global__ void k_bias_grad(rx_conv_desc d, const bf16* __restrict__ dy, float* __restrict__ db, int pix_per_block) {
+  const long long P = (long long)d.N * d.H * d.W;
+  long long p0 = (long long)blockIdx.x * pix_per_block;
+  long long p1 = P < p0 + pix_per_block ? P : p0 + pix_per_block;
+  for (int co = threadIdx.x; co < d.Cout; co += blockDim.x) {
+    float s = 0.0f;
+    for (long long p = p0; p < p1; ++p) s += __bfloat162float(dy[p * d.y_cstride + d.y_coff + co]);
+    atomicAdd(db + co, s);
+  }
+}
+
+// w_rot[ci][tap][co] = w[co][8 - tap][ci]: the weights of the input-gradient
+// convolution (a 3x3 convolution of dy with the flipped, transposed kernel)
+__global__ void k_rot_weights(int Cout, int Cin, const bf16* __restrict__ w, bf16* __restrict__ wr) {
+  long long n = (long long)Cout * 9 * Cin;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    int ci = (int)(i % Cin);
+    int tap = (int)((i / Cin) % 9);
+    int co = (int)(i / ((long long)Cin * 9));
+    wr[((long long)ci * 9 + (8 - tap)) * Cout + co] = w[i];
+  }
+}
+
+// ------------------------------------------------------------ element-wise
+// Every element-wise kernel walks (pixel, channel) of an NHWC view
+// (stride, offset) with a grid-stride loop.
+#define RX_EW_LOOP(count) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (count); i += (long long)gridDim.x * blockDim.x)
+
+// dst = src (channels [0, C) of each view); accumulate: dst += src
+__global__ void k_copy_ch(long long P, int C, const bf16* __restrict__ src, int s_stride, int s_off,
+                          bf16* __restrict__ dst, int d_stride, int d_off, int accumulate) {
+  RX_EW_LOOP(P * C) {
+    long long p = i / C;
+    int c = (int)(i % C);
+    float v = __bfloat162float(src[p * s_stride + s_off + c]);
+    bf16* o = dst + p * d_stride + d_off + c;
+    if (accumulate) v += __bfloat162float(*o);
+    *o = __float2bfloat16_rn(v);
+  }
+}
+
+// g = y > 0 ? g : 0  (gradient through a ReLU whose output is y)
+__global__ void k_relu_mask(long long P, int C, const bf16* __restrict__ yv, int y_stride, int y_off,
+                            bf16* __restrict__ g, int g_stride, int g_off) {
+  RX_EW_LOOP(P * C) {
+    long long p = i / C;
+    int c = (int)(i % C);
+    if (!(__bfloat162float(yv[p * y_stride + y_off + c]) > 0.0f)) g[p * g_stride + g_off + c] = __float2bfloat16_rn(0.0f);
+  }
+}
+
+// 2x2 average pool (H, W even): out (N, H/2, W/2, C)
+__global__ void k_pool2(int N, int H, int W, int C, const bf16* __restrict__ x, int x_stride, int x_off,
+                        bf16* __restrict__ y, int y_stride, int y_off) {
+  int h2 = H / 2, w2 = W / 2;
+  RX_EW_LOOP((long long)N * h2 * w2 * C) {
+    int c = (int)(i % C);
+    long long q = i / C;
+    int xo = (int)(q % w2), yo = (int)((q / w2) % h2);
+    long long n = q / ((long long)w2 * h2);
+    long long b = (n * H + 2 * yo) * W + 2 * xo;
+    float s = __bfloat162float(x[b * x_stride + x_off + c]) + __bfloat162float(x[(b + 1) * x_stride + x_off + c]) +
+              __bfloat162float(x[(b + W) * x_stride + x_off + c]) +
+              __bfloat162float(x[(b + W + 1) * x_stride + x_off + c]);
+    y[q * y_stride + y_off + c] = __float2bfloat16_rn(0.25f * s);
+  }
+}
+
+// gradient of the pool: each input pixel gets a quarter of its output's
+// gradient; accumulate adds to dx
+__global__ void k_pool2_bwd(int N, int H, int W, int C, const bf16* __restrict__ dy, int dy_stride, int dy_off,
+                            bf16* __restrict__ dx, int dx_stride, int dx_off, int accumulate) {
+  RX_EW_LOOP((long long)N * H * W * C) {
+    int c = (int)(i % C);
+    long long p = i / C;
+    int xx = (int)(p % W), yy = (int)((p / W) % H);
+    long long n = p / ((long long)W * H);
+    long long q = (n * (H / 2) + yy / 2) * (W / 2) + xx / 2;
+    float v = 0.25f * __bfloat162float(dy[q * dy_stride + dy_off + c]);
+    bf16* o = dx + p * dx_stride + dx_off + c;
+    if (accumulate) v += __bfloat162float(*o);
+    *o = __float2bfloat16_rn(v);
+  }
+}
+
+// nearest 2x upsample: out (N, 2H, 2W, C) from x (N, H, W, C)
+__global__ void k_up2(int N, int H, int W, int C, const bf16* __restrict__ x, int x_stride, int x_off,
+                      bf16* __restrict__ y, int y_stride, int y_off) {
+  RX_EW_LOOP((long long)N * 4 * H * W * C) {
+    int c = (int)(i % C);
+    long long p = i / C;
+    int xx = (int)(p % (2 * W)), yy = (int)((p / (2 * W)) % (2 * H));
+    long long n = p / (4LL * W * H);
+    long long q = (n * H + yy / 2) * W + xx / 2;
+    y[p * y_stride + y_off + c] = x[q * x_stride + x_off + c];
+  }
+}
+
+// gradient of the upsample: sum of the four children
+__global__ void k_up2_bwd(int N, int H, int W, int C, const bf16* __restrict__ dy, int dy_stride, int dy_off,
+                          bf16* __restrict__ dx, int dx_stride, int dx_off) {
+  RX_EW_LOOP((long long)N * H * W * C) {
+    int c = (int)(i % C);
+    long long q = i / C;
+    int xx = (int)(q % W), yy = (int)((q / W) % H);
+    long long n = q / ((long long)W * H);
+    long long b = (n * 2 * H + 2 * yy) * 2 * W + 2 * xx;
+    long long w2 = 2LL * W;
+    float s = __bfloat162float(dy[b * dy_stride + dy_off + c]) + __bfloat162float(dy[(b + 1) * dy_stride + dy_off + c]) +
+              __bfloat162float(dy[(b + w2) * dy_stride + dy_off + c]) +
+              __bfloat162float(dy[(b + w2 + 1) * dy_stride + dy_off + c]);
+    dx[q * dx_stride + dx_off + c] = __float2bfloat16_rn(s);
+  }
+}
+
+// Network input: 16 channels (log1p radiance, albedo, normal, depth/(1+depth),
+// six zeros) from float32 (P, 3) planes; base (optional) receives the
+// float32 log1p radiance the network's output is added to.
+__global__ void k_features(long long P, const float* __restrict__ rad, const float* __restrict__ alb,
+                           const float* __restrict__ nrm, const float* __restrict__ dep, bf16* __restrict__ out,
+                           float* __restrict__ base) {
+  RX_EW_LOOP(P) {
+    float f[16];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      f[k] = log1pf(fmaxf(rad[3 * i + k], 0.0f));
+      f[3 + k] = alb[3 * i + k];
+      f[6 + k] = nrm[3 * i + k];
+      if (base) base[3 * i + k] = f[k];
+    }
+    float dd = fmaxf(dep[i], 0.0f);
+    f[9] = dd / (1.0f + dd);
+#pragma unroll
+    for (int k = 10; k < 16; ++k) f[k] = 0.0f;
+    __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + 16 * i);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+  }
+}
+
+// L1 loss in log1p space of y + base (base optional) against target t
+// (P, 3): sum |y + base - t| into *loss, gradient sign(.) * scale into g
+// (bf16, channel stride gs; pad channels 3..gs-1 zero)
+__global__ void k_l1_loss(long long P, const float* __restrict__ y32, int y_stride, const float* __restrict__ base,
+                          const float* __restrict__ t, float scale, bf16* __restrict__ g, int gs,
+                          float* __restrict__ loss) {
+  float s = 0.0f;
+  RX_EW_LOOP(P) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float dlt = (y32[i * y_stride + k] + (base ? base[3 * i + k] : 0.0f)) - t[3 * i + k];
+      s += fabsf(dlt);
+      g[i * gs + k] = __float2bfloat16_rn(dlt > 0.0f ? scale : (dlt < 0.0f ? -scale : 0.0f));
+    }
+    for (int k = 3; k < gs; ++k) g[i * gs + k] = __float2bfloat16_rn(0.0f);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, s);
+}
+
+// radiance = max(expm1(y + base), 0) from the head's first three channels
+__global__ void k_output(long long P, const float* __restrict__ y32, int y_stride, const float* __restrict__ base,
+                         float* __restrict__ out) {
+  RX_EW_LOOP(P) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      out[3 * i + k] = fmaxf(expm1f(y32[i * y_stride + k] + (base ? base[3 * i + k] : 0.0f)), 0.0f);
+  }
+}
+
+// Adam (Kingma and Ba, 2015) on float32 master weights; writes the bf16
+// copy the convolutions read and clears the gradient
+__global__ void k_adam(long long n, float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, bf16* __restrict__ p16, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  RX_EW_LOOP(n) {
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.0f - b1) * gi;
+    float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+    if (p16) p16[i] = __float2bfloat16_rn(pi);
+    g[i] = 0.0f;
+  }
+}
+
+static int ew_blocks(Ctx* ctx, long long n) {
+  return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)ctx->num_sms * 32));
+}
+
+static bool conv_ok(const rx_conv_desc* d) {
+  return d && d->N > 0 && d->H > 0 && d->W > 0 && d->Cin > 0 && d->Cout > 0 && d->Cin % 16 == 0 &&
+         d->Cout % 16 == 0 && d->x_cstride % 8 == 0 && d->x_coff % 8 == 0 && d->y_cstride % 8 == 0 &&
+         d->y_coff % 8 == 0 && d->x_coff + d->Cin <= d->x_cstride && d->y_coff + d->Cout <= d->y_cstride;
+}
+
+int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
+             int relu, cudaStream_t st) {
+  if (!conv_ok(d) || !x || !w || !y)
+    return set_error(ctx, "conv_bf16_fwd: bad descriptor (channels multiples of 16, strides of 8)"), RX_ERR_ARG;
+  long long P = (long long)d->N * d->H * d->W;
+  dim3 grid((unsigned)((P + 63) / 64), 1);
+  const bf16* xb = static_cast<const bf16*>(x);
+  const bf16* wb = static_cast<const bf16*>(w);
+  bf16* yb = static_cast<bf16*>(y);
+  bool bk32 = d->Cin % 32 == 0;
+  if (d->Cout >= 128) {
+    grid.y = (unsigned)((d->Cout + 127) / 128);
+    if (bk32) k_conv_fwd<128, 32><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+    else k_conv_fwd<128, 16><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+  } else if (d->Cout > 32) {
+    grid.y = (unsigned)((d->Cout + 63) / 64);
+    if (bk32) k_conv_fwd<64, 32><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+    else k_conv_fwd<64, 16><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+  } else {
+    grid.y = (unsigned)((d->Cout + 31) / 32);
+    if (bk32) k_conv_fwd<32, 32><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+    else k_conv_fwd<32, 16><<<grid, 128, 0, st>>>(*d, xb, wb, bias, yb, y32, relu);
+  }
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+int conv_bwd_data(Ctx* ctx, const rx_conv_desc* d, const void* dy, const void* w, void* w_rot, void* dx,
+                  cudaStream_t st) {
+  if (!conv_ok(d) || !dy || !w || !w_rot || !dx) return set_error(ctx, "conv_bf16_bwd_data: bad arguments"), RX_ERR_ARG;
+  long long nw = (long long)d->Cout * 9 * d->Cin;
+  k_rot_weights<<<ew_blocks(ctx, nw), 256, 0, st>>>(d->Cout, d->Cin, static_cast<const bf16*>(w),
+                                                   static_cast<bf16*>(w_rot));
+  CUDA_TRY(ctx, cudaGetLastError());
+  // dx = conv(dy, w_rot): input channels Cout (read from the y view), output Cin (the x view)
+  rx_conv_desc t = *d;
+  t.Cin = d->Cout;
+  t.Cout = d->Cin;
+  t.x_cstride = d->y_cstride;
+  t.x_coff = d->y_coff;
+  t.y_cstride = d->x_cstride;
+  t.y_coff = d->x_coff;
+  return conv_fwd(ctx, &t, dy, w_rot, nullptr, dx, nullptr, 0, st);
+}
+
+int conv_bwd_weight(Ctx* ctx, const rx_conv_desc* d, const void* dy, const void* x, float* dw, float* db,
+                    cudaStream_t st) {
+  if (!conv_ok(d) || !dy || !x || !dw) return set_error(ctx, "conv_bf16_bwd_weight: bad arguments"), RX_ERR_ARG;
+  long long P = (long long)d->N * d->H * d->W;
+  // enough pixel chunks to fill the GPU with every (tap, channel block)
+  int cb = ((d->Cout + 63) / 64) * ((d->Cin + 63) / 64);
+  long long want = (long long)ctx->num_sms * 4 / std::max(1, 9 * cb) + 1;
+  int ppb = (int)std::max<long long>(256, ((P + want - 1) / want + 31) / 32 * 32);
+  dim3 grid((unsigned)((P + ppb - 1) / ppb), (unsigned)cb, 9);
+  k_conv_wgrad<<<grid, 128, 0, st>>>(*d, static_cast<const bf16*>(dy), static_cast<const bf16*>(x), dw, ppb);
+  CUDA_TRY(ctx, cudaGetLastError());
+  if (db) {
+    int bppb = 4096;
+    k_bias_grad<<<(unsigned)((P + bppb - 1) / bppb), 128, 0, st>>>(*d, static_cast<const bf16*>(dy), db, bppb);
+    CUDA_TRY(ctx, cudaGetLastError());
+  }
+  return RX_OK;
+}
+
+int dn_op(Ctx* ctx, const rx_dn_op* o, cudaStream_t st) {
+  if (!o) return set_error(ctx, "dn_op: NULL"), RX_ERR_ARG;
+  const bf16* a = static_cast<const bf16*>(o->a);
+  bf16* b = static_cast<bf16*>(o->b);
+  long long P = (long long)o->N * o->H * o->W;
+  switch (o->kind) {
+    case RX_DN_COPY:
+      k_copy_ch<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(P, o->C, a, o->a_stride, o->a_off, b, o->b_stride, o->b_off,
+                                                         o->flag);
+      break;
+    case RX_DN_RELU_MASK:
+      k_relu_mask<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(P, o->C, a, o->a_stride, o->a_off, b, o->b_stride,
+                                                           o->b_off);
+      break;
+    case RX_DN_POOL:
+      if (o->H % 2 || o->W % 2) return set_error(ctx, "dn_op: pool needs even H and W"), RX_ERR_ARG;
+      k_pool2<<<ew_blocks(ctx, P / 4 * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                           o->b_stride, o->b_off);
+      break;
+    case RX_DN_POOL_BWD:
+      if (o->H % 2 || o->W % 2) return set_error(ctx, "dn_op: pool needs even H and W"), RX_ERR_ARG;
+      k_pool2_bwd<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                           o->b_stride, o->b_off, o->flag);
+      break;
+    case RX_DN_UP:
+      k_up2<<<ew_blocks(ctx, 4 * P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                         o->b_stride, o->b_off);
+      break;
+    case RX_DN_UP_BWD:
+      k_up2_bwd<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                         o->b_stride, o->b_off);
+      break;
+    default:
+      return set_error(ctx, "dn_op: unknown kind %d", o->kind), RX_ERR_ARG;
+  }
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+int dn_features(Ctx* ctx, long long P, const float* rad, const float* alb, const float* nrm, const float* dep,
+                void* out, float* base, cudaStream_t st) {
+  if (P <= 0 || !rad || !alb || !nrm || !dep || !out) return set_error(ctx, "dn_features: bad arguments"), RX_ERR_ARG;
+  k_features<<<ew_blocks(ctx, P), 256, 0, st>>>(P, rad, alb, nrm, dep, static_cast<bf16*>(out), base);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+int dn_l1_loss(Ctx* ctx, long long P, const float* y32, int y_stride, const float* base, const float* target,
+               float scale, void* grad, int grad_stride, float* loss, cudaStream_t st) {
+  if (P <= 0 || !y32 || !target || !grad || !loss || y_stride < 3 || grad_stride < 3)
+    return set_error(ctx, "dn_l1_loss: bad arguments"), RX_ERR_ARG;
+  k_l1_loss<<<ew_blocks(ctx, P), 256, 0, st>>>(P, y32, y_stride, base, target, scale, static_cast<bf16*>(grad),
+                                               grad_stride, loss);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+int dn_output(Ctx* ctx, long long P, const float* y32, int y_stride, const float* base, float* out,
+              cudaStream_t st) {
+  if (P <= 0 || !y32 || !out || y_stride < 3) return set_error(ctx, "dn_output: bad arguments"), RX_ERR_ARG;
+  k_output<<<ew_blocks(ctx, P), 256, 0, st>>>(P, y32, y_stride, base, out);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+int dn_adam(Ctx* ctx, long long n, float* p, float* g, float* m, float* v, void* p16, float lr, float b1, float b2,
+            float eps, int step, cudaStream_t st) {
+  if (n <= 0 || !p || !g || !m || !v || step < 1) return set_error(ctx, "dn_adam: bad arguments"), RX_ERR_ARG;
+  float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  k_adam<<<ew_blocks(ctx, n), 256, 0, st>>>(n, p, g, m, v, static_cast<bf16*>(p16), lr, b1, b2, eps, c1, c2);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
+}  // namespace rx

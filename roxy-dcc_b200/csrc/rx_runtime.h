@@ -230,6 +230,23 @@ int serve_read(Server* s, int id, int which, float* host_out);
 int serve_release(Server* s, int id);
 int serve_stats(Server* s, rx_serve_stats* out);
 
+// Learned denoiser kernels (rx_conv.cu)
+int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
+             int relu, cudaStream_t st);
+int conv_bwd_data(Ctx* ctx, const rx_conv_desc* d, const void* dy, const void* w, void* w_rot, void* dx,
+                  cudaStream_t st);
+int conv_bwd_weight(Ctx* ctx, const rx_conv_desc* d, const void* dy, const void* x, float* dw, float* db,
+                    cudaStream_t st);
+int dn_op(Ctx* ctx, const rx_dn_op* o, cudaStream_t st);
+int dn_features(Ctx* ctx, long long P, const float* rad, const float* alb, const float* nrm, const float* dep,
+                void* out, float* base, cudaStream_t st);
+int dn_l1_loss(Ctx* ctx, long long P, const float* y32, int y_stride, const float* base, const float* target,
+               float scale, void* grad, int grad_stride, float* loss, cudaStream_t st);
+int dn_output(Ctx* ctx, long long P, const float* y32, int y_stride, const float* base, float* out,
+              cudaStream_t st);
+int dn_adam(Ctx* ctx, long long n, float* p, float* g, float* m, float* v, void* p16, float lr, float b1, float b2,
+            float eps, int step, cudaStream_t st);
+
 // device bytes held by each object (serving admission)
 size_t accum_bytes(const Accum* a);
 size_t batch_bytes(const Batch* b);

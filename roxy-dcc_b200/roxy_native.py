@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
 SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu",
-           "rx_serve.cu"]
+           "rx_serve.cu", "rx_conv.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
 
 RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE, RX_ERR_TIMEOUT = range(7)
@@ -67,6 +67,20 @@ class ServeStats(ctypes.Structure):
                 ("failed", ctypes.c_longlong), ("active", ctypes.c_int), ("queued", ctypes.c_int),
                 ("max_active_seen", ctypes.c_int), ("bytes_in_use", ctypes.c_longlong),
                 ("max_bytes_in_use", ctypes.c_longlong), ("busy_s", ctypes.c_double), ("uptime_s", ctypes.c_double)]
+
+
+class ConvDesc(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("N", "H", "W", "Cin", "Cout", "x_cstride", "x_coff", "y_cstride",
+                                             "y_coff")]
+
+
+class DnOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("N", ctypes.c_int), ("H", ctypes.c_int), ("W", ctypes.c_int),
+                ("C", ctypes.c_int), ("a", ctypes.c_void_p), ("a_stride", ctypes.c_int), ("a_off", ctypes.c_int),
+                ("b", ctypes.c_void_p), ("b_stride", ctypes.c_int), ("b_off", ctypes.c_int), ("flag", ctypes.c_int)]
+
+
+RX_DN_COPY, RX_DN_RELU_MASK, RX_DN_POOL, RX_DN_POOL_BWD, RX_DN_UP, RX_DN_UP_BWD = range(6)
 
 
 class DenoiseParams(ctypes.Structure):
@@ -164,6 +178,19 @@ _SIGS = {
     "rx_serve_release": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_serve_get_stats": ([ctypes.c_void_p, ctypes.POINTER(ServeStats)], ctypes.c_int),
     "rx_scene_device_bytes": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "rx_conv_bf16_fwd": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "rx_conv_bf16_bwd_data": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc)] + [ctypes.c_void_p] * 5, ctypes.c_int),
+    "rx_conv_bf16_bwd_weight": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc)] + [ctypes.c_void_p] * 5, ctypes.c_int),
+    "rx_dn_layer": ([ctypes.c_void_p, ctypes.POINTER(DnOp), ctypes.c_void_p], ctypes.c_int),
+    "rx_dn_features": ([ctypes.c_void_p, ctypes.c_longlong] + [ctypes.c_void_p] * 7, ctypes.c_int),
+    "rx_dn_l1_loss": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                       ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                       ctypes.c_void_p], ctypes.c_int),
+    "rx_dn_output": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                      ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rx_dn_adam": ([ctypes.c_void_p, ctypes.c_longlong] + [ctypes.c_void_p] * 5 + [ctypes.c_float] * 4 +
+                   [ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "rx_denoise": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_denoise_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

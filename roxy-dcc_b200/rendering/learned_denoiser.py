@@ -131,7 +131,10 @@ class Denoiser:
         return nat.ConvDesc(N, H, W, cin, cout, xs, xo, ys, yo)
 
     def _stream(self):
-        return ctypes.c_void_p(_torch().cuda.current_stream(self.dev).cuda_stream)
+        # torch's default stream has handle 0; the library would read NULL as
+        # its own (non-blocking) stream, so name the legacy default stream (1)
+        h = _torch().cuda.current_stream(self.dev).cuda_stream
+        return ctypes.c_void_p(h or 1)
 
     def _conv(self, name, N, H, W, x, xs, xo, y, ys, yo, y32=None):
         _, cin, cout, relu = next(L for L in LAYERS if L[0] == name)
@@ -297,6 +300,154 @@ def render_views(scene_world, device_scene, views, size, spp, max_depth=12, seed
     return {k: np.stack(v) for k, v in out.items()}
 
 
+WEIGHTS = __file__.rsplit("/", 1)[0] + "/denoiser_weights.npz"
+
+
+def save_weights(net, path):
+    """Weights as bf16 bit patterns (what inference reads), biases float32."""
+    out = {}
+    for name, _, _, _ in LAYERS:
+        w = net.w32[name].cpu().numpy().astype(np.float32)
+        out[f"{name}.w16"] = (w.view(np.uint32) + 0x7FFF + ((w.view(np.uint32) >> 16) & 1) >> 16).astype(np.uint16)
+        out[f"{name}.b"] = net.b32[name].cpu().numpy()
+    np.savez_compressed(path, **out)
+
+
+def load_weights(path=WEIGHTS):
+    d = np.load(path)
+    out = {}
+    for name, _, _, _ in LAYERS:
+        out[f"{name}.w"] = (d[f"{name}.w16"].astype(np.uint32) << 16).view(np.float32)
+        out[f"{name}.b"] = d[f"{name}.b"]
+    return out
+
+
+def make_training_set(scene_seeds=(3001, 3002, 3003, 3004), views_per_scene=48, size=256, spp_in=4, spp_ref=256,
+                      seed=5):
+    """Noisy / reference pairs rendered from orbiting cameras over scenes of
+    the large-mesh generator (other seeds than the evaluation scene).
+    Returns float32 numpy arrays: radiance, albedo, normal, depth (V, S, S,
+    3|1) of the noisy renders and target (V, S, S, 3) = log1p(reference)."""
+    import workloads
+    from rendering.taichi.extractor import build_device_scene
+    parts = {k: [] for k in ("radiance", "albedo", "normal", "depth", "target")}
+    for k, s in enumerate(scene_seeds):
+        world = workloads.displaced_icosphere_scene(size, size, seed=s)
+        ds = build_device_scene(world)
+        ds.use_lights(False)
+        views = orbit_views(views_per_scene, seed + k)
+        noisy = render_views(world, ds, views, size, spp_in, seed=1000 * k + 17)
+        ref = render_views(world, ds, views, size, spp_ref, seed=1000 * k + 500000, ref=True)
+        for key in ("radiance", "albedo", "normal", "depth"):
+            parts[key].append(noisy[key])
+        parts["target"].append(np.log1p(np.maximum(ref["radiance"], 0.0)).astype(np.float32))
+    return {k: np.concatenate(v) for k, v in parts.items()}
+
+
+def train(net, data, steps=3000, batch=16, crop=128, lr=2e-3, seed=0, log_every=250):
+    """Adam on random crops (with flips) of the training set held on the
+    device; the learning rate decays by a cosine to 5 % of `lr`.  Returns the
+    loss history (mean L1 in log1p space per logged step)."""
+    torch = _torch()
+    dev = net.dev
+    T = {k: torch.from_numpy(v).to(dev) for k, v in data.items()}
+    V, S = T["radiance"].shape[:2]
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    acc = 0.0
+    for it in range(steps):
+        idx = torch.randint(0, V, (batch,), generator=g)
+        oy = torch.randint(0, S - crop + 1, (1,), generator=g).item() // 4 * 4
+        ox = torch.randint(0, S - crop + 1, (1,), generator=g).item() // 4 * 4
+        flip = torch.randint(0, 4, (1,), generator=g).item()
+
+        def pick(t):
+            c = t[idx.to(dev), oy:oy + crop, ox:ox + crop]
+            if flip & 1:
+                c = torch.flip(c, (2,))
+            if flip & 2:
+                c = torch.flip(c, (1,))
+            return c.contiguous()
+
+        # normals are world-space guides: mirrored crops keep them as rendered
+        rad, alb, nrm, dep, tgt = (pick(T[k]) for k in ("radiance", "albedo", "normal", "depth", "target"))
+        cur = lr * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * it / max(steps, 1))))
+        loss = net.train_step(rad, alb, nrm, dep, tgt, lr=cur)
+        acc += float(loss) / (3 * batch * crop * crop)
+        if (it + 1) % log_every == 0:
+            hist.append(acc / log_every)
+            acc = 0.0
+    return hist
+
+
+def evaluate(net, world, width=1920, height=1080, spp=4, ref_spp=4096, max_depth=12, seed=77):
+    """relMSE of the noisy render, the 5-pass a-trous filter and the learned
+    denoiser against a float64 `ref_spp` render of the same view; plus the
+    learned denoiser's inference time (CUDA events, mean of 10 after 3)."""
+    torch = _torch()
+    from rendering.quality import reference_render, rel_mse
+    from rendering.taichi.extractor import build_device_scene
+    from rendering.taichi.trace import make_params
+    cam = world.active_camera
+    ds = build_device_scene(world)
+    ds.use_lights(False)
+    p = make_params(width, height, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, max_depth,
+                    int(world._use_sky), 0, 1, 10.0, list(world._background_color), list(cam.position),
+                    list(cam.forward), list(cam.right), list(cam.up), seed=seed)
+    ref = reference_render(ds.native, p, ref_spp)
+    acc = nat.Accumulator(width, height)
+    acc.render(ds.native, p, spp)
+    noisy = acc.read(nat.RX_ACC_RADIANCE)
+    dp = nat.DenoiseParams(1, 5, 0.08, 0.35, 0.20, 1.0, 1.0, 1, 1, 1, 0)
+    atrous = acc.denoise(dp)
+    dev = net.dev
+    planes = [torch.from_numpy(acc.read(w)).to(dev)[None] for w in
+              (nat.RX_ACC_RADIANCE, nat.RX_ACC_ALBEDO, nat.RX_ACC_NORMAL)]
+    dep = torch.from_numpy(acc.read(nat.RX_ACC_DEPTH)).to(dev)[None, ..., None].contiguous()
+    out = net.denoise(*planes, dep)
+    for _ in range(3):
+        net.denoise(*planes, dep)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        net.denoise(*planes, dep)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    learned = out[0].cpu().numpy()
+    flops = 2.0 * macs_per_pixel() * width * height
+    return {"relmse_noisy": rel_mse(noisy, ref), "relmse_atrous": rel_mse(atrous, ref),
+            "relmse_learned": rel_mse(learned, ref), "spp": spp, "ref_spp": ref_spp, "infer_ms": ms,
+            "infer_tflops": flops / (ms / 1e3) / 1e12, "flops_per_frame": flops}
+
+
+def main():
+    """Train on renderer-generated pairs and write the weights file."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--views", type=int, default=48)
+    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--eval", action="store_true")
+    args = ap.parse_args()
+    t0 = time.time()
+    data = make_training_set(views_per_scene=args.views)
+    t_data = time.time() - t0
+    net = Denoiser(seed=0)
+    t0 = time.time()
+    hist = train(net, data, steps=args.steps)
+    t_train = time.time() - t0
+    save_weights(net, args.out)
+    res = {"pairs": int(data["radiance"].shape[0]), "data_s": t_data, "train_s": t_train, "loss": hist}
+    if args.eval:
+        import workloads
+        net2 = Denoiser(weights=load_weights(args.out))
+        res["eval"] = evaluate(net2, workloads.displaced_icosphere_scene())
+    print(json.dumps(res))
+
+
 def orbit_views(n, seed, radius=(2.4, 3.6)):
     """Seeded camera positions around the scene's centre, looking at it."""
     rng = np.random.default_rng(seed)
@@ -309,3 +460,7 @@ def orbit_views(n, seed, radius=(2.4, 3.6)):
         at = rng.normal(0.0, 0.25, 3).tolist()
         views.append((pos, at))
     return views
+
+
+if __name__ == "__main__":
+    main()

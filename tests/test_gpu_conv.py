@@ -24,7 +24,8 @@ def _p(t):
 
 
 def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    # torch's default stream (handle 0) is the legacy default stream, handle 1
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
 
 
 def _close(got, ref, frac=2e-2):

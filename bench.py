@@ -175,7 +175,7 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    if args.workload in ("batch", "serve"):
+    if args.workload in ("batch", "serve", "denoiser"):
         print(json.dumps({"impl": "reference", "unavailable": "the batched and serving workloads' baseline is the "
                                                               "plain one-scene-at-a-time GPU path in their own line"}))
         return 0
@@ -523,6 +523,45 @@ def run_batch(args):
     return 0
 
 
+def run_denoiser(args):
+    """Learned-denoiser configuration: the committed weights (trained on
+    renderer-generated 4-spp / 256-spp pairs of other large-mesh scenes)
+    denoise a 4-spp 1920x1080 render of the benchmark scene; relMSE of the
+    noisy image, the 5-pass a-trous filter and the learned denoiser against a
+    float64 4096-spp render; inference timed with CUDA events."""
+    import roxy_native as nat
+    import workloads
+    from rendering.learned_denoiser import Denoiser, evaluate, load_weights
+
+    ws, rank, local = _dist()
+    if rank != 0:
+        return 0
+    nat.context(0)
+    net = Denoiser(weights=load_weights())
+    with ClockSampler(0) as clocks:
+        r = evaluate(net, workloads.displaced_icosphere_scene(), ref_spp=args.ref_spp or 4096)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    line = {"metric": "frames/s", "value": 1e3 / r["infer_ms"], "unit": "frames/s", "n_gpus": 1, "steps": 10,
+            "warmup": 3, "ms_per_step": r["infer_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": "learned denoiser, 3-level U-Net 32/64/128, 1920x1080 4-spp render of the "
+                                   "displaced-icosphere scene", "flops_per_frame": r["flops_per_frame"]},
+            "roofline": {"bound": "tensor", "kernel": "k_conv_fwd (all layers of one inference)",
+                         "achieved": r["infer_tflops"], "peak": peak, "unit": "TFLOP/s",
+                         "frac": r["infer_tflops"] / peak,
+                         "peak_source": "measured" if "bf16_tflops" in peaks else "fallback", "traffic": None},
+            "quality": {k: r[k] for k in ("relmse_noisy", "relmse_atrous", "relmse_learned", "spp", "ref_spp")},
+            "clocks": clocks.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 def run_serve(args):
     """Serving configuration: Poisson arrivals at swept rates; each request
     renders one of four displaced-icosphere scenes (the large-mesh
@@ -594,7 +633,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--workload", default="icosphere", choices=sorted(WORKLOADS) + ["batch", "serve", "denoiser"])
     ap.add_argument("--scenes", type=int, default=64, help="scenes in the batch workload")
     ap.add_argument("--rates", default="10,50,100,200,500", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="serve workload: seconds of arrivals per rate")
@@ -609,6 +648,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "denoiser":
+        return run_denoiser(args)
     return run_ours(args)
 
 

@@ -81,7 +81,7 @@ int rx_device_count(int* out);
 int rx_ctx_create(int device, rx_ctx** out);
 int rx_ctx_destroy(rx_ctx* ctx);
 const char* rx_last_error(const rx_ctx* ctx);
-int rx_ctx_sync(rx_ctx* ctx);
+int rx_ctx_sync(rx_ctx* ctx);       /* waits for the device; reports kernel error flags */
 void* rx_ctx_stream(rx_ctx* ctx); /* the cudaStream_t the library launches on */
 
 /* Scene state.  Replaces the module-global fields written by extract_scene
@@ -300,6 +300,12 @@ typedef struct {
  * receives the same values in float32 */
 int rx_conv_bf16_fwd(rx_ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y,
                      float* y32, int relu, void* stream);
+/* Forward convolutions with 16, 32, 64 or 128 output channels run on the
+ * fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
+ * memory); other shapes and impl = 1 use the mma.sync kernel.  A kernel
+ * whose internal wait runs out raises the device error flag, reported by
+ * rx_ctx_sync. */
+int rx_conv_set_impl(rx_ctx* ctx, int impl);
 /* dx = gradient of the input for output gradient dy (in the y view);
  * w_rot: Cout*9*Cin bf16 of scratch the caller provides */
 int rx_conv_bf16_bwd_data(rx_ctx* ctx, const rx_conv_desc* d, const void* dy, const void* w, void* w_rot, void* dx,

@@ -160,7 +160,22 @@ int rx_ctx_destroy(rx_ctx* ctx) {
 
 int rx_ctx_sync(rx_ctx* ctx) {
   if (!ctx) return RX_ERR_ARG;
-  CUDA_TRY(&ctx->c, cudaStreamSynchronize(ctx->c.stream));
+  LOCK(&ctx->c);
+  cudaSetDevice(ctx->c.device);
+  CUDA_TRY(&ctx->c, cudaDeviceSynchronize());
+  // error bits a kernel raised (a bounded wait that ran out, an overflow)
+  int e = 0;
+  CUDA_TRY(&ctx->c, cudaMemcpy(&e, ctx->c.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CUDA_TRY(&ctx->c, cudaMemset(ctx->c.d_err, 0, sizeof(int)));
+    return set_error(&ctx->c, "device error flags 0x%x", e), RX_ERR_DEVICE;
+  }
+  return RX_OK;
+}
+
+int rx_conv_set_impl(rx_ctx* ctx, int impl) {
+  if (!ctx || (impl != 0 && impl != 1)) return set_error(ctx ? &ctx->c : nullptr, "rx_conv_set_impl: 0 or 1"), RX_ERR_ARG;
+  ctx->c.conv_impl = impl;
   return RX_OK;
 }
 

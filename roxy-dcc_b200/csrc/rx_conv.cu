@@ -179,6 +179,205 @@ __global__ void __launch_bounds__(128) k_conv_fwd(rx_conv_desc d, const bf16* __
       }
 }
 
+// ------------------------------------------- forward conv on tcgen05 (UMMA)
+// One CTA computes 128 consecutive pixels of one image row (the MMA's M)
+// for all COUT output channels (its N), accumulating in tensor memory.
+// Per chunk of 32 input channels it stages, with cp.async, a halo of 3 rows
+// x 130 pixels and the 9 taps' weights in shared memory in the canonical
+// K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes): channel
+// chunk planes [kc][row][pixel][8 channels] and [tap][kc][co][8].  A tap's
+// A operand is then the same descriptor with its start moved by whole
+// pixels, so the halo is loaded once for all 9 taps.  One thread issues
+// 9 taps x 2 K-steps of tcgen05.mma (kind::f16, BF16 in, FP32 accumulate)
+// per chunk and commits them to the chunk buffer's mbarrier; two buffers
+// overlap the next chunk's copies with the current MMAs.
+namespace tc {
+constexpr int TILE = 128, HALO_W = TILE + 2, KCH = 4;  // 4 chunks of 8 channels = 32
+constexpr int HALO_BYTES = KCH * 3 * HALO_W * 16;      // 24960
+constexpr unsigned long long kSpinCycles = 4000000000ull;  // ~2 s at 1.9 GHz
+
+__host__ __device__ constexpr int stage_bytes(int cout) { return HALO_BYTES + 9 * KCH * cout * 16; }
+
+// K-major, no-swizzle shared-memory matrix descriptor (Blackwell version 1)
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M=128
+__host__ __device__ constexpr uint32_t idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  unsigned long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > kSpinCycles) return false;
+  }
+}
+}  // namespace tc
+
+template <int COUT>
+__global__ void __launch_bounds__(128, 1) k_conv_fwd_tc(rx_conv_desc d, const bf16* __restrict__ x,
+                                                        const bf16* __restrict__ w, const float* __restrict__ bias,
+                                                        bf16* __restrict__ y, float* __restrict__ y32, int relu,
+                                                        int* err) {
+  constexpr int SB = tc::stage_bytes(COUT);
+  constexpr int TCOLS = COUT < 32 ? 32 : COUT;  // tensor-memory columns (power of two >= 32)
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int x0 = blockIdx.x * tc::TILE, yrow = blockIdx.y, n = blockIdx.z;
+  const int nch = (d.Cin + 31) / 32;
+
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int b = 0; b < 2; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  auto load = [&](int ch, int buf) {
+    unsigned char* base = smem + buf * SB;
+    const int c0 = ch * 32;
+    // halo: chunk index ((r * HALO_W + px) * KCH + kc); 16 bytes each
+    for (int c = tid; c < 3 * tc::HALO_W * tc::KCH; c += 128) {
+      int kc = c % tc::KCH, rp = c / tc::KCH;
+      int px = rp % tc::HALO_W, r = rp / tc::HALO_W;
+      int yy = yrow + r - 1, xx = x0 + px - 1, ci = c0 + kc * 8;
+      bool ok = yy >= 0 && yy < d.H && xx >= 0 && xx < d.W && ci < d.Cin;
+      const bf16* src = ok ? x + (((long long)n * d.H + yy) * d.W + xx) * d.x_cstride + d.x_coff + ci : x;
+      cp_async16(base + ((kc * 3 + r) * tc::HALO_W + px) * 16, src, ok);
+    }
+    // weights: chunk index ((co * 9 + tap) * KCH + kc)
+    unsigned char* wb = base + tc::HALO_BYTES;
+    for (int c = tid; c < COUT * 9 * tc::KCH; c += 128) {
+      int kc = c % tc::KCH, ct = c / tc::KCH;
+      int tap = ct % 9, co = ct / 9;
+      int ci = c0 + kc * 8;
+      bool ok = co < d.Cout && ci < d.Cin;
+      const bf16* src = ok ? w + ((long long)co * 9 + tap) * d.Cin + ci : w;
+      cp_async16(wb + ((tap * tc::KCH + kc) * COUT + co) * 16, src, ok);
+    }
+  };
+
+  load(0, 0);
+  cp_async_commit();
+  bool ok_all = true;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < nch) {
+      const int nb = (ch + 1) & 1;
+      if (ch + 1 >= 2) {
+        // the MMAs of chunk ch - 1 read buffer nb: wait for their commit
+        if (!tc::mbar_wait(smem_u32(&bars[nb]), (uint32_t)(((ch - 1) >> 1) & 1))) abort_flag = 1;
+      }
+      __syncthreads();
+      if (abort_flag) {
+        ok_all = false;
+        break;
+      }
+      load(ch + 1, nb);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    // copies visible to the tensor cores (async proxy) before the MMAs
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t hb = smem_u32(smem + buf * SB);
+      const uint32_t wb = hb + tc::HALO_BYTES;
+      constexpr uint32_t ID = tc::idesc(COUT);
+#pragma unroll 1
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+        for (int k2 = 0; k2 < 2; ++k2) {
+          uint64_t ad = tc::desc(hb + (((2 * k2) * 3 + dy) * tc::HALO_W + dx) * 16, 3 * tc::HALO_W * 16, 128);
+          uint64_t bd = tc::desc(wb + ((tap * tc::KCH + 2 * k2) * COUT) * 16, COUT * 16, 128);
+          uint32_t acc = (ch > 0 || tap > 0 || k2 > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+              "l"(ad), "l"(bd), "r"(ID), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                       smem_u32(&bars[buf]))
+                   : "memory");
+    }
+  }
+  if (ok_all) {
+    const int last = nch - 1;
+    if (!tc::mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1))) ok_all = false;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (ok_all) {
+    // accumulator row = pixel (warp's 32 lanes), columns = output channels
+    const int xx = x0 + warp * 32 + lane;
+    const long long m = ((long long)n * d.H + yrow) * d.W + xx;
+#pragma unroll 1
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (xx < d.W && c0 < d.Cout) {
+        float v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          v[k] = __uint_as_float(r[k]) + (bias ? bias[c0 + k] : 0.0f);
+          if (relu) v[k] = fmaxf(v[k], 0.0f);
+        }
+        uint4 pk[2];
+        uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+          pw[k] = *reinterpret_cast<uint32_t*>(&h);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(y + m * d.y_cstride + d.y_coff + c0);
+        dst[0] = pk[0];
+        dst[1] = pk[1];
+        if (y32) {
+#pragma unroll
+          for (int k = 0; k < 16; ++k) y32[m * d.y_cstride + d.y_coff + c0 + k] = v[k];
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicOr(err, ERR_BAD_NODE);
+  }
+  cp_async_wait<0>();
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
 // ------------------------------------------------------- weight gradient
 // dw[co][tap][ci] += sum_p dy[p][co] * x[p + off(tap)][ci]
 // GEMM: M = output channels (64), N = input channels (64), K = pixels
@@ -480,10 +679,37 @@ static bool conv_ok(const rx_conv_desc* d) {
          d->y_coff % 8 == 0 && d->x_coff + d->Cin <= d->x_cstride && d->y_coff + d->Cout <= d->y_cstride;
 }
 
+template <int COUT>
+static int launch_tc(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                     float* y32, int relu, cudaStream_t st) {
+  constexpr int smem = 2 * tc::stage_bytes(COUT);
+  static int attr_dev = -1;
+  if (attr_dev != ctx->device) {
+    CUDA_TRY(ctx, cudaFuncSetAttribute(k_conv_fwd_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_dev = ctx->device;
+  }
+  dim3 grid((unsigned)((d->W + tc::TILE - 1) / tc::TILE), (unsigned)d->H, (unsigned)d->N);
+  k_conv_fwd_tc<COUT><<<grid, 128, smem, st>>>(*d, x, w, bias, y, y32, relu, ctx->d_err);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return RX_OK;
+}
+
 int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
              int relu, cudaStream_t st) {
   if (!conv_ok(d) || !x || !w || !y)
     return set_error(ctx, "conv_bf16_fwd: bad descriptor (channels multiples of 16, strides of 8)"), RX_ERR_ARG;
+  if (ctx->conv_impl == 0 && d->H <= 65535 && d->N <= 65535) {
+    const bf16* xb = static_cast<const bf16*>(x);
+    const bf16* wb = static_cast<const bf16*>(w);
+    bf16* yb = static_cast<bf16*>(y);
+    switch (d->Cout) {
+      case 16: return launch_tc<16>(ctx, d, xb, wb, bias, yb, y32, relu, st);
+      case 32: return launch_tc<32>(ctx, d, xb, wb, bias, yb, y32, relu, st);
+      case 64: return launch_tc<64>(ctx, d, xb, wb, bias, yb, y32, relu, st);
+      case 128: return launch_tc<128>(ctx, d, xb, wb, bias, yb, y32, relu, st);
+      default: break;
+    }
+  }
   long long P = (long long)d->N * d->H * d->W;
   dim3 grid((unsigned)((P + 63) / 64), 1);
   const bf16* xb = static_cast<const bf16*>(x);

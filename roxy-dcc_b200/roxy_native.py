@@ -180,6 +180,7 @@ _SIGS = {
     "rx_scene_device_bytes": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "rx_conv_bf16_fwd": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "rx_conv_set_impl": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_conv_bf16_bwd_data": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc)] + [ctypes.c_void_p] * 5, ctypes.c_int),
     "rx_conv_bf16_bwd_weight": ([ctypes.c_void_p, ctypes.POINTER(ConvDesc)] + [ctypes.c_void_p] * 5, ctypes.c_int),
     "rx_dn_layer": ([ctypes.c_void_p, ctypes.POINTER(DnOp), ctypes.c_void_p], ctypes.c_int),

@@ -49,8 +49,17 @@ CASES = [  # N, H, W, Cin, Cout, x_stride, x_off, y_stride, y_off, relu
 ]
 
 
-@pytest.mark.parametrize("N,H,W,Cin,Cout,xs,xo,ys,yo,relu", CASES)
-def test_conv_fwd_and_grads_match_torch(N, H, W, Cin, Cout, xs, xo, ys, yo, relu):
+@pytest.fixture(params=[0, 1], ids=["tcgen05", "mma_sync"])
+def impl(request):
+    ctx = _ctx()
+    ctx.check(nat.lib().rx_conv_set_impl(ctx.h, request.param))
+    yield request.param
+    ctx.check(nat.lib().rx_ctx_sync(ctx.h))  # no kernel raised its error flag
+    ctx.check(nat.lib().rx_conv_set_impl(ctx.h, 0))
+
+
+@pytest.mark.parametrize("N,H,W,Cin,Cout,xs,xo,ys,yo,relu", CASES + [(1, 3, 300, 32, 64, 32, 0, 64, 0, 1)])
+def test_conv_fwd_and_grads_match_torch(N, H, W, Cin, Cout, xs, xo, ys, yo, relu, impl):
     ctx = _ctx()
     g = torch.Generator(device="cuda").manual_seed(N * 1000 + H)
     dev = "cuda"
@@ -163,6 +172,29 @@ def _torch_net(net, x16, base, target):
     P = x.shape[0] * x.shape[2] * x.shape[3]
     (loss / (3 * P)).backward()
     return float(loss), {k: (v[0].grad, v[1].grad) for k, v in params.items()}
+
+
+def test_tcgen05_and_mma_sync_convolutions_agree():
+    """The two forward kernels on the same operands: same values up to the
+    order of their float32 sums (and the bf16 rounding of the output)."""
+    ctx = _ctx()
+    L = nat.lib()
+    g = torch.Generator(device="cuda").manual_seed(21)
+    for (Cin, Cout, H, W) in ((16, 32, 33, 257), (96, 32, 20, 128), (64, 128, 9, 200), (32, 16, 5, 130)):
+        x = torch.randn((2, H, W, Cin), generator=g, device="cuda").to(torch.bfloat16)
+        w = (torch.randn((Cout, 9, Cin), generator=g, device="cuda") / np.sqrt(9 * Cin)).to(torch.bfloat16)
+        b = torch.randn(Cout, generator=g, device="cuda")
+        d = nat.ConvDesc(2, H, W, Cin, Cout, Cin, 0, Cout, 0)
+        outs = []
+        for impl_ in (0, 1):
+            ctx.check(L.rx_conv_set_impl(ctx.h, impl_))
+            y = torch.zeros((2, H, W, Cout), dtype=torch.bfloat16, device="cuda")
+            y32 = torch.zeros((2, H, W, Cout), dtype=torch.float32, device="cuda")
+            ctx.check(L.rx_conv_bf16_fwd(ctx.h, ctypes.byref(d), _p(x), _p(w), _p(b), _p(y), _p(y32), 0, _stream()))
+            outs.append(y32)
+        ctx.check(L.rx_conv_set_impl(ctx.h, 0))
+        ctx.check(L.rx_ctx_sync(ctx.h))
+        assert float((outs[0] - outs[1]).abs().max()) <= 1e-3 * float(outs[1].abs().max()), (Cin, Cout)
 
 
 def test_network_loss_and_gradients_match_torch():

@@ -302,9 +302,11 @@ int rx_conv_bf16_fwd(rx_ctx* ctx, const rx_conv_desc* d, const void* x, const vo
                      float* y32, int relu, void* stream);
 /* Forward convolutions with 16, 32, 64 or 128 output channels run on the
  * fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
- * memory); other shapes and impl = 1 use the mma.sync kernel.  A kernel
- * whose internal wait runs out raises the device error flag, reported by
- * rx_ctx_sync. */
+ * memory): impl = 0 uses the persistent kernel (weights resident in shared
+ * memory) where the layer's weights and two halos fit, else the streaming
+ * one; impl = 2 uses the streaming one only; impl = 1 and other shapes use
+ * the mma.sync kernel.  A kernel whose internal wait runs out raises the
+ * device error flag, reported by rx_ctx_sync. */
 int rx_conv_set_impl(rx_ctx* ctx, int impl);
 /* dx = gradient of the input for output gradient dy (in the y view);
  * w_rot: Cout*9*Cin bf16 of scratch the caller provides */

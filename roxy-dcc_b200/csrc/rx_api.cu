@@ -174,7 +174,7 @@ int rx_ctx_sync(rx_ctx* ctx) {
 }
 
 int rx_conv_set_impl(rx_ctx* ctx, int impl) {
-  if (!ctx || (impl != 0 && impl != 1)) return set_error(ctx ? &ctx->c : nullptr, "rx_conv_set_impl: 0 or 1"), RX_ERR_ARG;
+  if (!ctx || impl < 0 || impl > 2) return set_error(ctx ? &ctx->c : nullptr, "rx_conv_set_impl: 0, 1 or 2"), RX_ERR_ARG;
   ctx->c.conv_impl = impl;
   return RX_OK;
 }

@@ -378,6 +378,209 @@ __global__ void __launch_bounds__(128, 1) k_conv_fwd_tc(rx_conv_desc d, const bf
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
+// Persistent row-strip variant for layers whose weights fit in shared
+// memory beside a ring of input rows.  The weights are loaded once per CTA.
+// Each CTA owns a contiguous range of 128-pixel row tiles ordered with the
+// row fastest, so consecutive tiles are vertically adjacent and share two of
+// their three input rows: the input is a ring of S row slots
+// [slot][kc][pixel][8] (130 pixels, all input channels) into which rows are
+// copied S - 2 rows ahead of the MMAs; every input row is read once per
+// strip instead of three times.  Two tensor-memory accumulators let row
+// y's MMAs run while row y-1's epilogue reads its accumulator.
+namespace tc {
+__host__ __device__ constexpr int row_bytes(int cin) { return HALO_W * cin * 2; }
+__host__ __device__ constexpr int weights_bytes(int cin, int cout) { return 9 * cin * cout * 2; }
+}  // namespace tc
+
+// cp.async.wait_group with a run-time count (0..3; larger waits for 3)
+__device__ __forceinline__ void cp_async_wait_n(int n) {
+  switch (n) {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    default: cp_async_wait<3>(); break;
+  }
+}
+
+template <int COUT>
+__global__ void __launch_bounds__(128, 1) k_conv_fwd_ring(rx_conv_desc d, const bf16* __restrict__ x,
+                                                          const bf16* __restrict__ w, const float* __restrict__ bias,
+                                                          bf16* __restrict__ y, float* __restrict__ y32, int relu,
+                                                          int S, long long per_cta, int* err) {
+  constexpr int TCOLS = 2 * COUT < 32 ? 32 : 2 * COUT;  // two accumulators
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int KC = d.Cin / 8, L = S - 2;
+  const int RB = tc::row_bytes(d.Cin);
+  unsigned char* wsm = smem;                                  // [tap][kc][co][8]
+  unsigned char* rsm = smem + tc::weights_bytes(d.Cin, COUT);  // S x [kc][px][8]
+  const int xt = (d.W + tc::TILE - 1) / tc::TILE;
+  const long long total = (long long)d.N * xt * d.H;  // row tiles, row fastest
+  long long u = (long long)blockIdx.x * per_cta;
+  const long long uend = u + per_cta < total ? u + per_cta : total;
+
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int b = 0; b < 2; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  // weights once (they join the first row's copy group): chunk ((co * 9 + tap) * KC + kc)
+  for (int c = tid; c < COUT * 9 * KC; c += 128) {
+    int kc = c % KC, ct = c / KC;
+    int tap = ct % 9, co = ct / 9;
+    const bf16* src = w + ((long long)co * 9 + tap) * d.Cin + kc * 8;
+    cp_async16(wsm + ((tap * KC + kc) * COUT + co) * 16, src, co < d.Cout);
+  }
+  auto slot_of = [&](int r) { return (r + S) % S; };  // r >= -1
+  auto load_row = [&](int n, int x0, int r) {
+    unsigned char* base = rsm + slot_of(r) * RB;
+    const bool row_ok = r >= 0 && r < d.H;
+    const long long rbase = ((long long)n * d.H + r) * d.W;
+    for (int c = tid; c < tc::HALO_W * KC; c += 128) {
+      int kc = c % KC, px = c / KC;
+      int xx = x0 + px - 1;
+      bool ok = row_ok && xx >= 0 && xx < d.W;
+      const bf16* src = ok ? x + (rbase + xx) * d.x_cstride + d.x_coff + kc * 8 : x;
+      cp_async16(base + (kc * tc::HALO_W + px) * 16, src, ok);
+    }
+  };
+  auto issue = [&](int yy, int buf) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t rb = smem_u32(rsm);
+    const uint32_t wb = smem_u32(wsm);
+    const uint32_t acc_t = tmem + (uint32_t)(buf * COUT);
+    constexpr uint32_t ID = tc::idesc(COUT);
+    int first = 1;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dy = tap / 3, dx = tap % 3;
+      const uint32_t sb = rb + (uint32_t)(slot_of(yy + dy - 1) * RB);
+#pragma unroll 1
+      for (int kc0 = 0; kc0 < KC; kc0 += 2) {
+        uint64_t ad = tc::desc(sb + (kc0 * tc::HALO_W + dx) * 16, tc::HALO_W * 16, 128);
+        uint64_t bd = tc::desc(wb + ((tap * KC + kc0) * COUT) * 16, COUT * 16, 128);
+        uint32_t acc = first ? 0u : 1u;
+        first = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(acc_t),
+            "l"(ad), "l"(bd), "r"(ID), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     smem_u32(&bars[buf]))
+                 : "memory");
+  };
+  auto epilogue = [&](int n, int yr, int x0, int buf) {
+    const int xx = x0 + warp * 32 + lane;
+    const long long m = ((long long)n * d.H + yr) * d.W + xx;
+#pragma unroll 1
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * COUT + c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (xx < d.W) {
+        float v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          v[k] = __uint_as_float(r[k]) + (bias ? bias[c0 + k] : 0.0f);
+          if (relu) v[k] = fmaxf(v[k], 0.0f);
+        }
+        uint4 pk[2];
+        uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+          pw[k] = *reinterpret_cast<uint32_t*>(&h);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(y + m * d.y_cstride + d.y_coff + c0);
+        dst[0] = pk[0];
+        dst[1] = pk[1];
+        if (y32) {
+          float4* d32 = reinterpret_cast<float4*>(y32 + m * d.y_cstride + d.y_coff + c0);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) d32[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+        }
+      }
+    }
+  };
+
+  int i = 0;  // row tiles whose MMAs this CTA has issued
+  bool ok_all = true;
+  while (u < uend) {
+    // one segment: consecutive rows [ylo, yhi) of one column of tiles
+    const long long col = u / d.H;
+    const int ylo = (int)(u - col * d.H);
+    const int yhi = (int)((long long)ylo + (uend - u) < d.H ? (long long)ylo + (uend - u) : d.H);
+    const int n = (int)(col / xt), x0 = (int)(col % xt) * tc::TILE;
+    for (int k = 0; k <= L; ++k) {  // rows ylo-1 .. ylo+L-1, one copy group each
+      if (ylo - 1 + k <= yhi) load_row(n, x0, ylo - 1 + k);
+      cp_async_commit();
+    }
+    for (int yy = ylo; yy < yhi; ++yy, ++i) {
+      const int buf = i & 1;
+      cp_async_wait_n(L - 2);  // rows up to yy + 1 have landed
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads();
+      if (tid == 0) issue(yy, buf);
+      if (yy > ylo) {
+        // row yy-1: MMAs done -> its accumulator and row yy-2's slot are free
+        if (!tc::mbar_wait(smem_u32(&bars[buf ^ 1]), (uint32_t)(((i - 1) >> 1) & 1))) abort_flag = 1;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        if (abort_flag) {
+          // this row's MMAs were issued: give them a bounded wait before
+          // the tensor memory is released
+          tc::mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i >> 1) & 1));
+          ok_all = false;
+          break;
+        }
+      }
+      if (yy + L <= yhi) load_row(n, x0, yy + L);
+      cp_async_commit();
+      if (yy > ylo) {
+        epilogue(n, yy - 1, x0, buf ^ 1);
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      }
+    }
+    if (!ok_all) break;
+    const int last = i - 1;
+    if (!tc::mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1))) {
+      ok_all = false;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    epilogue(n, yhi - 1, x0, last & 1);
+    cp_async_wait<0>();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    u += yhi - ylo;
+  }
+  if (!ok_all && tid == 0) atomicOr(err, ERR_BAD_NODE);
+  cp_async_wait<0>();
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
 // ------------------------------------------------------- weight gradient
 // dw[co][tap][ci] += sum_p dy[p][co] * x[p + off(tap)][ci]
 // GEMM: M = output channels (64), N = input channels (64), K = pixels
@@ -694,14 +897,70 @@ static int launch_tc(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16*
   return RX_OK;
 }
 
+// Row-strip kernel when the weights and a ring of at least 4 input rows fit
+// in shared memory (6 rows where they fit: copies 4 rows ahead); returns 1
+// if it launched.
+template <int COUT>
+static int launch_ring(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                       float* y32, int relu, cudaStream_t st, int* rc) {
+  const int limit = 232448 - 256;  // opt-in shared memory per block, less the static part
+  const int wbytes = tc::weights_bytes(d->Cin, COUT), rbytes = tc::row_bytes(d->Cin);
+  if (wbytes + 4 * rbytes > limit || (y32 && ((uintptr_t)y32 & 15))) return 0;
+  const int S = std::min(6, (limit - wbytes) / rbytes);
+  const int smem = wbytes + S * rbytes;
+  static int attr_dev = -1;
+  if (attr_dev != ctx->device) {
+    if (cudaFuncSetAttribute(k_conv_fwd_ring<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    attr_dev = ctx->device;
+  }
+  // resident CTAs per SM from shared memory (the kernel's 128 B of static
+  // shared memory plus the per-block reservation), capped so that every
+  // resident CTA gets its tensor memory
+  int smem_sm = 0, reserved = 0;
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, ctx->device);
+  constexpr int tcols = 2 * COUT < 32 ? 32 : 2 * COUT;
+  int per_sm = smem_sm / (smem + 128 + reserved);
+  per_sm = std::max(1, std::min(std::min(per_sm, 512 / tcols), 16));
+  const long long total = (long long)d->N * d->H * ((d->W + tc::TILE - 1) / tc::TILE);
+  const long long want = std::min<long long>(total, (long long)ctx->num_sms * per_sm);
+  const long long per_cta = (total + want - 1) / want;
+  const int grid = (int)((total + per_cta - 1) / per_cta);
+  k_conv_fwd_ring<COUT><<<grid, 128, smem, st>>>(*d, x, w, bias, y, y32, relu, S, per_cta, ctx->d_err);
+  cudaError_t e = cudaGetLastError();
+  *rc = e == cudaSuccess ? RX_OK : (set_error(ctx, "conv_bf16_fwd: %s", cudaGetErrorString(e)), RX_ERR_CUDA);
+  return 1;
+}
+
 int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
              int relu, cudaStream_t st) {
   if (!conv_ok(d) || !x || !w || !y)
     return set_error(ctx, "conv_bf16_fwd: bad descriptor (channels multiples of 16, strides of 8)"), RX_ERR_ARG;
-  if (ctx->conv_impl == 0 && d->H <= 65535 && d->N <= 65535) {
+  if (ctx->conv_impl != 1 && d->H <= 65535 && d->N <= 65535) {
     const bf16* xb = static_cast<const bf16*>(x);
     const bf16* wb = static_cast<const bf16*>(w);
     bf16* yb = static_cast<bf16*>(y);
+    int rc = RX_OK;
+    switch (ctx->conv_impl == 0 ? d->Cout : 0) {
+      case 16:
+        if (launch_ring<16>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
+        break;
+      case 32:
+        if (launch_ring<32>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
+        break;
+      case 64:
+        if (launch_ring<64>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
+        break;
+      case 128:
+        if (launch_ring<128>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
+        break;
+      default:
+        break;
+    }
     switch (d->Cout) {
       case 16: return launch_tc<16>(ctx, d, xb, wb, bias, yb, y32, relu, st);
       case 32: return launch_tc<32>(ctx, d, xb, wb, bias, yb, y32, relu, st);

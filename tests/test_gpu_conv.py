@@ -49,7 +49,7 @@ CASES = [  # N, H, W, Cin, Cout, x_stride, x_off, y_stride, y_off, relu
 ]
 
 
-@pytest.fixture(params=[0, 1], ids=["tcgen05", "mma_sync"])
+@pytest.fixture(params=[0, 1, 2], ids=["tcgen05", "mma_sync", "tcgen05_streaming"])
 def impl(request):
     ctx = _ctx()
     ctx.check(nat.lib().rx_conv_set_impl(ctx.h, request.param))
@@ -175,18 +175,21 @@ def _torch_net(net, x16, base, target):
 
 
 def test_tcgen05_and_mma_sync_convolutions_agree():
-    """The two forward kernels on the same operands: same values up to the
-    order of their float32 sums (and the bf16 rounding of the output)."""
+    """The forward kernels on the same operands (persistent and streaming
+    tcgen05, then mma.sync): same values up to the order of their float32
+    sums (and the bf16 rounding of the output)."""
     ctx = _ctx()
     L = nat.lib()
     g = torch.Generator(device="cuda").manual_seed(21)
-    for (Cin, Cout, H, W) in ((16, 32, 33, 257), (96, 32, 20, 128), (64, 128, 9, 200), (32, 16, 5, 130)):
+    for (Cin, Cout, H, W) in ((16, 32, 33, 257), (96, 32, 20, 128), (64, 128, 9, 200), (32, 16, 5, 130),
+                              (64, 64, 70, 300), (192, 64, 6, 129), (32, 32, 128, 512), (96, 32, 600, 256),
+                              (96, 64, 20, 140)):
         x = torch.randn((2, H, W, Cin), generator=g, device="cuda").to(torch.bfloat16)
         w = (torch.randn((Cout, 9, Cin), generator=g, device="cuda") / np.sqrt(9 * Cin)).to(torch.bfloat16)
         b = torch.randn(Cout, generator=g, device="cuda")
         d = nat.ConvDesc(2, H, W, Cin, Cout, Cin, 0, Cout, 0)
         outs = []
-        for impl_ in (0, 1):
+        for impl_ in (0, 2, 1):
             ctx.check(L.rx_conv_set_impl(ctx.h, impl_))
             y = torch.zeros((2, H, W, Cout), dtype=torch.bfloat16, device="cuda")
             y32 = torch.zeros((2, H, W, Cout), dtype=torch.float32, device="cuda")
@@ -194,7 +197,9 @@ def test_tcgen05_and_mma_sync_convolutions_agree():
             outs.append(y32)
         ctx.check(L.rx_conv_set_impl(ctx.h, 0))
         ctx.check(L.rx_ctx_sync(ctx.h))
-        assert float((outs[0] - outs[1]).abs().max()) <= 1e-3 * float(outs[1].abs().max()), (Cin, Cout)
+        scale = float(outs[2].abs().max())
+        assert float((outs[0] - outs[2]).abs().max()) <= 1e-3 * scale, (Cin, Cout)
+        assert float((outs[1] - outs[2]).abs().max()) <= 1e-3 * scale, (Cin, Cout)
 
 
 def test_network_loss_and_gradients_match_torch():

@@ -300,13 +300,15 @@ typedef struct {
  * receives the same values in float32 */
 int rx_conv_bf16_fwd(rx_ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y,
                      float* y32, int relu, void* stream);
-/* Forward convolutions with 16, 32, 64 or 128 output channels run on the
- * fifth-generation tensor cores (tcgen05.mma, accumulators in tensor
- * memory): impl = 0 uses the persistent kernel (weights resident in shared
- * memory) where the layer's weights and two halos fit, else the streaming
- * one; impl = 2 uses the streaming one only; impl = 1 and other shapes use
- * the mma.sync kernel.  A kernel whose internal wait runs out raises the
- * device error flag, reported by rx_ctx_sync. */
+/* Forward convolution kernels.  impl = 0 (default): the warp-specialised
+ * tcgen05 kernel (weights resident in shared memory, a ring of input rows,
+ * accumulators in tensor memory) for every layer whose weights fit beside
+ * four input rows in at most two output-channel groups, the mma.sync
+ * kernel for the others.  impl = 1: mma.sync only.  impl = 2: the streaming
+ * tcgen05 kernel (one 128-pixel row tile per CTA, weights staged per
+ * 32-channel chunk) for 16, 32, 64 or 128 output channels, mma.sync for
+ * other shapes.  A kernel whose internal wait runs out raises the device
+ * error flag, reported by rx_ctx_sync. */
 int rx_conv_set_impl(rx_ctx* ctx, int impl);
 /* dx = gradient of the input for output gradient dy (in the y view);
  * w_rot: Cout*9*Cin bf16 of scratch the caller provides */

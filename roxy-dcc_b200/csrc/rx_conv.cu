@@ -378,20 +378,6 @@ __global__ void __launch_bounds__(128, 1) k_conv_fwd_tc(rx_conv_desc d, const bf
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
-// Persistent row-strip variant for layers whose weights fit in shared
-// memory beside a ring of input rows.  The weights are loaded once per CTA.
-// Each CTA owns a contiguous range of 128-pixel row tiles ordered with the
-// row fastest, so consecutive tiles are vertically adjacent and share two of
-// their three input rows: the input is a ring of S row slots
-// [slot][kc][pixel][8] (130 pixels, all input channels) into which rows are
-// copied S - 2 rows ahead of the MMAs; every input row is read once per
-// strip instead of three times.  Two tensor-memory accumulators let row
-// y's MMAs run while row y-1's epilogue reads its accumulator.
-namespace tc {
-__host__ __device__ constexpr int row_bytes(int cin) { return HALO_W * cin * 2; }
-__host__ __device__ constexpr int weights_bytes(int cin, int cout) { return 9 * cin * cout * 2; }
-}  // namespace tc
-
 // cp.async.wait_group with a run-time count (0..3; larger waits for 3)
 __device__ __forceinline__ void cp_async_wait_n(int n) {
   switch (n) {
@@ -402,182 +388,327 @@ __device__ __forceinline__ void cp_async_wait_n(int n) {
   }
 }
 
-template <int COUT>
-__global__ void __launch_bounds__(128, 1) k_conv_fwd_ring(rx_conv_desc d, const bf16* __restrict__ x,
-                                                          const bf16* __restrict__ w, const float* __restrict__ bias,
-                                                          bf16* __restrict__ y, float* __restrict__ y32, int relu,
-                                                          int S, long long per_cta, int* err) {
-  constexpr int TCOLS = 2 * COUT < 32 ? 32 : 2 * COUT;  // two accumulators
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long bars[2];
+// --------------------------------------- forward conv, warp-specialised
+// Persistent row-strip kernel for layers whose weights fit in shared memory
+// beside a ring of input rows.  The weights are loaded once per CTA.  Each
+// CTA owns a contiguous range of 128-pixel row tiles ordered with the row
+// fastest, so consecutive tiles are vertically adjacent and share two of
+// their three input rows: the input is a ring of S row slots [slot][kc]
+// [pixel][8] (130 pixels, all input channels), and every input row is read
+// once per strip instead of three times.  Three jobs run in separate warps
+// that hand work to one another through mbarriers, so that copies, MMAs
+// and epilogues of different rows overlap:
+//   warps 5-6: producers.  Each input row of the strip (130 pixels, zero
+//     outside the image) is copied with coalesced 16-byte cp.async into a
+//     ring slot [kc][130 px x 16 B]; once a row's copies have landed the 64
+//     producers make them visible to the tensor cores (proxy fence) and
+//     arrive on `full[slot]`; a slot is refilled after `empty[slot]`.
+//   warp 4 (one thread): MMA issuer.  Output row y reads the slots of rows
+//     y-1, y, y+1; it accumulates into one of two tensor-memory buffers,
+//     commits to `acc_full[buf]`, and releases row y-1's slot (its last
+//     reader) with a commit to `empty`.
+//   warps 0-3: epilogue.  Warp w reads tensor-memory lanes 32 w .. 32 w + 31
+//     (its 32 pixels), adds the bias, applies ReLU, stores bf16 (and fp32),
+//     then arrives on `acc_empty[buf]`.
+// Output channels may be split into G groups of NG (blockIdx.x % G) when
+// all the weights do not fit in shared memory beside the ring; the G CTAs
+// of a strip run side by side and share its input rows through L2.
+// Every wait is bounded: a wait that runs out (or sees another role give
+// up) raises the shared abort flag, the roles stop, outstanding copies and
+// MMAs are waited for (bounded), the device error flag is set.
+namespace tc {
+constexpr int PLANE = HALO_W * 16;  // one 8-channel chunk of one row
+__host__ __device__ constexpr int slot_bytes(int cin) { return (cin / 8) * PLANE; }
+__host__ __device__ constexpr int weights_bytes(int cin, int cout) { return 9 * cin * cout * 2; }
+constexpr int kMaxSlots = 8;
+}  // namespace tc
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// single-thread bounded wait; gives up when the abort flag is raised
+__device__ __forceinline__ bool mbar_wait_abortable(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  const unsigned long long t0 = clock64();
+  for (;;) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > tc::kSpinCycles) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+
+// whole-warp bounded wait with a warp-uniform outcome
+__device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  const unsigned long long t0 = clock64();
+  for (;;) {
+    const bool ok = mbar_try(bar, parity);
+    if (__all_sync(0xffffffffu, ok)) return true;
+    const bool stop = *abort_flag || clock64() - t0 > tc::kSpinCycles;
+    if (__any_sync(0xffffffffu, stop)) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+}
+
+template <int NG>
+__global__ void __launch_bounds__(224, 1) k_conv_fwd_ws(rx_conv_desc d, const bf16* __restrict__ x,
+                                                        const bf16* __restrict__ w, const float* __restrict__ bias,
+                                                        bf16* __restrict__ y, float* __restrict__ y32, int relu,
+                                                        int S, int G, long long per_cta, int* err) {
+  constexpr int TCOLS = 2 * NG < 32 ? 32 : 2 * NG;  // two accumulators
+  constexpr int kProducers = 64;                     // warps 5 and 6
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long full[tc::kMaxSlots], empty[tc::kMaxSlots];
+  __shared__ __align__(8) unsigned long long acc_full[2], acc_empty[2], mma_done;
   __shared__ uint32_t tmem_base;
-  __shared__ int abort_flag;
+  __shared__ volatile int abort_flag;
+  __shared__ float sbias[NG];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int KC = d.Cin / 8, L = S - 2;
-  const int RB = tc::row_bytes(d.Cin);
-  unsigned char* wsm = smem;                                  // [tap][kc][co][8]
-  unsigned char* rsm = smem + tc::weights_bytes(d.Cin, COUT);  // S x [kc][px][8]
+  const int KC = d.Cin / 8;
+  const int SB = tc::slot_bytes(d.Cin);
+  unsigned char* smem = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
+  unsigned char* wsm = smem;                                 // [tap][kc][co][8]
+  unsigned char* rsm = smem + tc::weights_bytes(d.Cin, NG);  // S x [kc][PLANE]
+  const int grp = blockIdx.x % G;
   const int xt = (d.W + tc::TILE - 1) / tc::TILE;
   const long long total = (long long)d.N * xt * d.H;  // row tiles, row fastest
-  long long u = (long long)blockIdx.x * per_cta;
-  const long long uend = u + per_cta < total ? u + per_cta : total;
+  const long long u0 = (long long)(blockIdx.x / G) * per_cta;
+  const long long uend = u0 + per_cta < total ? u0 + per_cta : total;
 
   if (tid == 0) {
     abort_flag = 0;
-    for (int b = 0; b < 2; ++b)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[b])));
+    for (int s = 0; s < S; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full[s])), "r"(kProducers));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&acc_full[b])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(smem_u32(&acc_empty[b])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mma_done)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
+  for (int c = tid; c < NG; c += blockDim.x) sbias[c] = bias ? bias[grp * NG + c] : 0.0f;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
                  "r"(TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
+  // this group's weights, once: chunk ((co * 9 + tap) * KC + kc) -> [tap][kc][co][8]
+  for (int c = tid; c < NG * 9 * KC; c += blockDim.x) {
+    int kc = c % KC, ct = c / KC;
+    int tap = ct % 9, co = ct / 9;
+    const bf16* src = w + ((long long)(grp * NG + co) * 9 + tap) * d.Cin + kc * 8;
+    cp_async16(wsm + ((tap * KC + kc) * NG + co) * 16, src, true);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  // weights once (they join the first row's copy group): chunk ((co * 9 + tap) * KC + kc)
-  for (int c = tid; c < COUT * 9 * KC; c += 128) {
-    int kc = c % KC, ct = c / KC;
-    int tap = ct % 9, co = ct / 9;
-    const bf16* src = w + ((long long)co * 9 + tap) * d.Cin + kc * 8;
-    cp_async16(wsm + ((tap * KC + kc) * COUT + co) * 16, src, co < d.Cout);
-  }
-  auto slot_of = [&](int r) { return (r + S) % S; };  // r >= -1
-  auto load_row = [&](int n, int x0, int r) {
-    unsigned char* base = rsm + slot_of(r) * RB;
-    const bool row_ok = r >= 0 && r < d.H;
-    const long long rbase = ((long long)n * d.H + r) * d.W;
-    for (int c = tid; c < tc::HALO_W * KC; c += 128) {
-      int kc = c % KC, px = c / KC;
-      int xx = x0 + px - 1;
-      bool ok = row_ok && xx >= 0 && xx < d.W;
-      const bf16* src = ok ? x + (rbase + xx) * d.x_cstride + d.x_coff + kc * 8 : x;
-      cp_async16(base + (kc * tc::HALO_W + px) * 16, src, ok);
-    }
-  };
-  auto issue = [&](int yy, int buf) {
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t rb = smem_u32(rsm);
-    const uint32_t wb = smem_u32(wsm);
-    const uint32_t acc_t = tmem + (uint32_t)(buf * COUT);
-    constexpr uint32_t ID = tc::idesc(COUT);
-    int first = 1;
-#pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-      const int dy = tap / 3, dx = tap % 3;
-      const uint32_t sb = rb + (uint32_t)(slot_of(yy + dy - 1) * RB);
-#pragma unroll 1
-      for (int kc0 = 0; kc0 < KC; kc0 += 2) {
-        uint64_t ad = tc::desc(sb + (kc0 * tc::HALO_W + dx) * 16, tc::HALO_W * 16, 128);
-        uint64_t bd = tc::desc(wb + ((tap * KC + kc0) * COUT) * 16, COUT * 16, 128);
-        uint32_t acc = first ? 0u : 1u;
-        first = 0;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(acc_t),
-            "l"(ad), "l"(bd), "r"(ID), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-      }
-    }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                     smem_u32(&bars[buf]))
-                 : "memory");
-  };
-  auto epilogue = [&](int n, int yr, int x0, int buf) {
-    const int xx = x0 + warp * 32 + lane;
-    const long long m = ((long long)n * d.H + yr) * d.W + xx;
-#pragma unroll 1
-    for (int c0 = 0; c0 < COUT; c0 += 16) {
-      uint32_t r[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * COUT + c0)));
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (xx < d.W) {
-        float v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          v[k] = __uint_as_float(r[k]) + (bias ? bias[c0 + k] : 0.0f);
-          if (relu) v[k] = fmaxf(v[k], 0.0f);
-        }
-        uint4 pk[2];
-        uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-          pw[k] = *reinterpret_cast<uint32_t*>(&h);
-        }
-        uint4* dst = reinterpret_cast<uint4*>(y + m * d.y_cstride + d.y_coff + c0);
-        dst[0] = pk[0];
-        dst[1] = pk[1];
-        if (y32) {
-          float4* d32 = reinterpret_cast<float4*>(y32 + m * d.y_cstride + d.y_coff + c0);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) d32[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-        }
-      }
-    }
-  };
-
-  int i = 0;  // row tiles whose MMAs this CTA has issued
-  bool ok_all = true;
-  while (u < uend) {
-    // one segment: consecutive rows [ylo, yhi) of one column of tiles
-    const long long col = u / d.H;
-    const int ylo = (int)(u - col * d.H);
-    const int yhi = (int)((long long)ylo + (uend - u) < d.H ? (long long)ylo + (uend - u) : d.H);
-    const int n = (int)(col / xt), x0 = (int)(col % xt) * tc::TILE;
-    for (int k = 0; k <= L; ++k) {  // rows ylo-1 .. ylo+L-1, one copy group each
-      if (ylo - 1 + k <= yhi) load_row(n, x0, ylo - 1 + k);
-      cp_async_commit();
-    }
-    for (int yy = ylo; yy < yhi; ++yy, ++i) {
-      const int buf = i & 1;
-      cp_async_wait_n(L - 2);  // rows up to yy + 1 have landed
+  if (warp >= 5) {
+    // ------------------------------------------------ producers (cp.async)
+    // consecutive threads copy consecutive 16-byte chunks of a pixel row,
+    // so each warp request is coalesced; a row is signalled `lag` rows
+    // after it was issued, once its copies have landed
+    const int ptid = tid - 5 * 32;
+    const int lag = S - 3 < 2 ? S - 3 : 2;
+    auto signal = [&](int q) {
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncthreads();
-      if (tid == 0) issue(yy, buf);
-      if (yy > ylo) {
-        // row yy-1: MMAs done -> its accumulator and row yy-2's slot are free
-        if (!tc::mbar_wait(smem_u32(&bars[buf ^ 1]), (uint32_t)(((i - 1) >> 1) & 1))) abort_flag = 1;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        __syncthreads();
-        if (abort_flag) {
-          // this row's MMAs were issued: give them a bounded wait before
-          // the tensor memory is released
-          tc::mbar_wait(smem_u32(&bars[buf]), (uint32_t)((i >> 1) & 1));
-          ok_all = false;
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&full[q % S])) : "memory");
+    };
+    int k = 0;  // rows issued
+    bool ok = true;
+    for (long long u = u0; u < uend && ok;) {
+      const long long col = u / d.H;
+      const int ylo = (int)(u - col * d.H);
+      const int yhi = (int)((long long)ylo + (uend - u) < d.H ? (long long)ylo + (uend - u) : d.H);
+      const int n = (int)(col / xt), x0 = (int)(col % xt) * tc::TILE;
+      for (int r = ylo - 1; r <= yhi; ++r, ++k) {
+        const int s = (int)(k % S);
+        if (!mbar_wait_warp(smem_u32(&empty[s]), (uint32_t)(((k / S) & 1) ^ 1), &abort_flag)) {
+          ok = false;
           break;
         }
+        unsigned char* base = rsm + s * SB;
+        const bool row_ok = r >= 0 && r < d.H;
+        const long long rbase = ((long long)n * d.H + r) * d.W;
+        for (int c = ptid; c < tc::HALO_W * KC; c += kProducers) {
+          const int kc = c % KC, px = c / KC;
+          const int xx = x0 + px - 1;
+          const bool in = row_ok && xx >= 0 && xx < d.W;
+          const bf16* src = in ? x + (rbase + xx) * d.x_cstride + d.x_coff + kc * 8 : x;
+          cp_async16(base + kc * tc::PLANE + px * 16, src, in);
+        }
+        cp_async_commit();
+        if (k >= lag) {
+          cp_async_wait_n(lag);
+          signal(k - lag);
+        }
       }
-      if (yy + L <= yhi) load_row(n, x0, yy + L);
-      cp_async_commit();
-      if (yy > ylo) {
-        epilogue(n, yy - 1, x0, buf ^ 1);
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      }
+      u += yhi - ylo;
     }
-    if (!ok_all) break;
-    const int last = i - 1;
-    if (!tc::mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1))) {
-      ok_all = false;
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    epilogue(n, yhi - 1, x0, last & 1);
     cp_async_wait<0>();
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    u += yhi - ylo;
+    if (ok)
+      for (int q = k > lag ? k - lag : 0; q < k; ++q) signal(q);
+  } else if (warp == 4) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t rb = smem_u32(rsm), wb = smem_u32(wsm);
+      constexpr uint32_t ID = tc::idesc(NG);
+      // descriptor words (K-major, no swizzle): SBO 128 B and version 1 in
+      // the high word; LBO = one plane (A) or NG x 16 B (B) in the low word
+      constexpr uint32_t desc_hi = (128u >> 4) | (1u << 14);
+      const uint32_t a_lbo = (uint32_t)(tc::PLANE >> 4) << 16;
+      const uint32_t b_lo0 = (wb >> 4) | ((uint32_t)NG << 16);
+      int kb = 0;  // ring index of the segment's first row (ylo - 1)
+      int i = 0;         // output rows issued
+      bool ok = true;
+      for (long long u = u0; u < uend && ok;) {
+        const long long col = u / d.H;
+        const int ylo = (int)(u - col * d.H);
+        const int yhi = (int)((long long)ylo + (uend - u) < d.H ? (long long)ylo + (uend - u) : d.H);
+        const int nrows = yhi - ylo;
+        for (int yy = ylo; yy < yhi; ++yy, ++i) {
+          const int kr = kb + (yy - ylo);  // ring index of row yy - 1
+          int slot[3];
+          for (int q = 0; q < 3; ++q) {
+            slot[q] = (kr + q) % S;
+            if (ok) ok = mbar_wait_abortable(smem_u32(&full[slot[q]]), (uint32_t)(((kr + q) / S) & 1), &abort_flag);
+          }
+          const int b = i & 1;
+          if (ok) ok = mbar_wait_abortable(smem_u32(&acc_empty[b]), (uint32_t)(((i >> 1) & 1) ^ 1), &abort_flag);
+          if (!ok) break;
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t acc_t = tmem + (uint32_t)(b * NG);
+          // The issue loop runs on one thread, so its integer work sets
+          // the MMA rate: descriptors are stepped, not rebuilt.  Low words
+          // hold (address >> 4) | (LBO >> 4) << 16; a byte offset of 16 k
+          // adds k.  A: next chunk pair +2 planes, next tap column +1
+          // pixel; B walks [tap][kc][co] in order, 2 NG x 16 B per step.
+          uint32_t b_lo = b_lo0;
+          uint32_t acc = 0u;
+#pragma unroll 1
+          for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap % 3;
+            uint32_t a_lo = ((rb + (uint32_t)(slot[dy] * SB)) >> 4) + (uint32_t)dx + a_lbo;
+#pragma unroll 2
+            for (int kc0 = 0; kc0 < KC; kc0 += 2) {
+              const uint64_t ad = ((uint64_t)desc_hi << 32) | a_lo;
+              const uint64_t bd = ((uint64_t)desc_hi << 32) | b_lo;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(acc_t),
+                  "l"(ad), "l"(bd), "r"(ID), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+              acc = 1u;
+              a_lo += 2 * (tc::PLANE >> 4);
+              b_lo += 2 * NG;
+            }
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           smem_u32(&acc_full[b]))
+                       : "memory");
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           smem_u32(&empty[slot[0]]))
+                       : "memory");
+        }
+        if (!ok) break;
+        // rows yhi - 1 and yhi have no later reader in this segment
+        for (int q = 0; q < 2; ++q)
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           smem_u32(&empty[(kb + nrows + q) % S]))
+                       : "memory");
+        kb += nrows + 2;
+        u += nrows;
+      }
+      // every MMA issued has finished before the tensor memory is released
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                       smem_u32(&mma_done))
+                   : "memory");
+      const unsigned long long t0 = clock64();
+      while (!mbar_try(smem_u32(&mma_done), 0u) && clock64() - t0 < tc::kSpinCycles) {
+      }
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 0-3)
+    const int qtr = warp;  // tensor-memory lanes 32 qtr .. 32 qtr + 31
+    int i = 0;
+    bool ok = true;
+    for (long long u = u0; u < uend && ok;) {
+      const long long col = u / d.H;
+      const int ylo = (int)(u - col * d.H);
+      const int yhi = (int)((long long)ylo + (uend - u) < d.H ? (long long)ylo + (uend - u) : d.H);
+      const int n = (int)(col / xt), x0 = (int)(col % xt) * tc::TILE;
+      for (int yy = ylo; yy < yhi; ++yy, ++i) {
+        const int b = i & 1;
+        if (!mbar_wait_warp(smem_u32(&acc_full[b]), (uint32_t)((i >> 1) & 1), &abort_flag)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const int xx = x0 + qtr * 32 + lane;
+        const long long m = ((long long)n * d.H + yy) * d.W + xx;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NG; c0 += 16) {
+          uint32_t r[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+              "[%16];\n"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+              : "r"(tmem + ((uint32_t)(qtr * 32) << 16) + (uint32_t)(b * NG + c0)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          if (xx < d.W) {
+            float v[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              v[k] = __uint_as_float(r[k]) + sbias[c0 + k];
+              if (relu) v[k] = fmaxf(v[k], 0.0f);
+            }
+            uint4 pk[2];
+            uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+              pw[k] = *reinterpret_cast<uint32_t*>(&h);
+            }
+            const long long o = m * d.y_cstride + d.y_coff + grp * NG + c0;
+            uint4* dst = reinterpret_cast<uint4*>(y + o);
+            dst[0] = pk[0];
+            dst[1] = pk[1];
+            if (y32) {
+              float4* d32 = reinterpret_cast<float4*>(y32 + o);
+#pragma unroll
+              for (int k = 0; k < 4; ++k) d32[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acc_empty[b])) : "memory");
+      }
+      u += yhi - ylo;
+    }
   }
-  if (!ok_all && tid == 0) atomicOr(err, ERR_BAD_NODE);
-  cp_async_wait<0>();
+
+  __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (tid == 0 && abort_flag) atomicOr(err, ERR_BAD_NODE);
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
@@ -897,70 +1028,82 @@ static int launch_tc(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16*
   return RX_OK;
 }
 
-// Row-strip kernel when the weights and a ring of at least 4 input rows fit
-// in shared memory (6 rows where they fit: copies 4 rows ahead); returns 1
-// if it launched.
-template <int COUT>
-static int launch_ring(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
-                       float* y32, int relu, cudaStream_t st, int* rc) {
-  const int limit = 232448 - 256;  // opt-in shared memory per block, less the static part
-  const int wbytes = tc::weights_bytes(d->Cin, COUT), rbytes = tc::row_bytes(d->Cin);
-  if (wbytes + 4 * rbytes > limit || (y32 && ((uintptr_t)y32 & 15))) return 0;
-  const int S = std::min(6, (limit - wbytes) / rbytes);
-  const int smem = wbytes + S * rbytes;
+template <int NG>
+static int launch_ws_ng(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                        float* y32, int relu, int S, int smem, cudaStream_t st, int* rc) {
+  const int limit = 232448 - 1024;  // opt-in shared memory per block, less the static part
   static int attr_dev = -1;
   if (attr_dev != ctx->device) {
-    if (cudaFuncSetAttribute(k_conv_fwd_ring<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit) !=
-        cudaSuccess) {
+    if (cudaFuncSetAttribute(k_conv_fwd_ws<NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit) != cudaSuccess) {
       cudaGetLastError();
       return 0;
     }
     attr_dev = ctx->device;
   }
-  // resident CTAs per SM from shared memory (the kernel's 128 B of static
-  // shared memory plus the per-block reservation), capped so that every
-  // resident CTA gets its tensor memory
+  // resident CTAs per SM from shared memory (dynamic + static + the
+  // per-block reservation), capped so that every resident CTA gets its
+  // tensor memory
+  cudaFuncAttributes fa{};
   int smem_sm = 0, reserved = 0;
+  cudaFuncGetAttributes(&fa, k_conv_fwd_ws<NG>);
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
   cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, ctx->device);
-  constexpr int tcols = 2 * COUT < 32 ? 32 : 2 * COUT;
-  int per_sm = smem_sm / (smem + 128 + reserved);
-  per_sm = std::max(1, std::min(std::min(per_sm, 512 / tcols), 16));
+  constexpr int tcols = 2 * NG < 32 ? 32 : 2 * NG;
+  int per_sm = smem_sm / (smem + (int)fa.sharedSizeBytes + reserved);
+  per_sm = std::max(1, std::min(std::min(per_sm, 512 / tcols), 9));  // 9 x 224 threads
+  const int G = d->Cout / NG;
   const long long total = (long long)d->N * d->H * ((d->W + tc::TILE - 1) / tc::TILE);
-  const long long want = std::min<long long>(total, (long long)ctx->num_sms * per_sm);
-  const long long per_cta = (total + want - 1) / want;
-  const int grid = (int)((total + per_cta - 1) / per_cta);
-  k_conv_fwd_ring<COUT><<<grid, 128, smem, st>>>(*d, x, w, bias, y, y32, relu, S, per_cta, ctx->d_err);
+  const long long strips_want = std::max<long long>(1, (long long)ctx->num_sms * per_sm / G);
+  const long long per_cta = (total + std::min(total, strips_want) - 1) / std::min(total, strips_want);
+  const long long strips = (total + per_cta - 1) / per_cta;
+  k_conv_fwd_ws<NG><<<(unsigned)(strips * G), 224, smem, st>>>(*d, x, w, bias, y, y32, relu, S, G, per_cta,
+                                                                 ctx->d_err);
   cudaError_t e = cudaGetLastError();
   *rc = e == cudaSuccess ? RX_OK : (set_error(ctx, "conv_bf16_fwd: %s", cudaGetErrorString(e)), RX_ERR_CUDA);
   return 1;
+}
+
+// Warp-specialised tcgen05 kernel: the widest output-channel group (128,
+// 64, 32 or 16, dividing Cout) whose weights fit in shared memory beside a
+// ring of at least 4 input rows (6 where they fit).  Returns 1 if it
+// launched, 0 if the shape or the pointers do not suit it.
+static int launch_ws(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                     float* y32, int relu, cudaStream_t st, int* rc) {
+  const int limit = 232448 - 1024;
+  if (((uintptr_t)x & 15) || ((uintptr_t)y & 15) || (y32 && ((uintptr_t)y32 & 15))) return 0;
+  const int SB = tc::slot_bytes(d->Cin);
+  int NG = 0;
+  // at most two groups: every group re-reads the input rows, and a UMMA's
+  // cost is mostly its A (pixel) operand read, so narrow groups do not pay
+  for (int ng = 128; ng >= 16; ng >>= 1)
+    if (d->Cout % ng == 0 && d->Cout / ng <= 2 && tc::weights_bytes(d->Cin, ng) + 4 * SB + 128 <= limit) {
+      NG = ng;
+      break;
+    }
+  if (!NG) return 0;
+  const int S = std::min(6, (limit - 128 - tc::weights_bytes(d->Cin, NG)) / SB);
+  const int smem = tc::weights_bytes(d->Cin, NG) + S * SB + 128;
+  switch (NG) {
+    case 128: return launch_ws_ng<128>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
+    case 64: return launch_ws_ng<64>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
+    case 32: return launch_ws_ng<32>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
+    default: return launch_ws_ng<16>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
+  }
 }
 
 int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
              int relu, cudaStream_t st) {
   if (!conv_ok(d) || !x || !w || !y)
     return set_error(ctx, "conv_bf16_fwd: bad descriptor (channels multiples of 16, strides of 8)"), RX_ERR_ARG;
-  if (ctx->conv_impl != 1 && d->H <= 65535 && d->N <= 65535) {
+  if (ctx->conv_impl == 0) {
+    int rc = RX_OK;
+    if (launch_ws(ctx, d, static_cast<const bf16*>(x), static_cast<const bf16*>(w), bias, static_cast<bf16*>(y), y32,
+                  relu, st, &rc))
+      return rc;
+  } else if (ctx->conv_impl == 2 && d->H <= 65535 && d->N <= 65535) {
     const bf16* xb = static_cast<const bf16*>(x);
     const bf16* wb = static_cast<const bf16*>(w);
     bf16* yb = static_cast<bf16*>(y);
-    int rc = RX_OK;
-    switch (ctx->conv_impl == 0 ? d->Cout : 0) {
-      case 16:
-        if (launch_ring<16>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
-        break;
-      case 32:
-        if (launch_ring<32>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
-        break;
-      case 64:
-        if (launch_ring<64>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
-        break;
-      case 128:
-        if (launch_ring<128>(ctx, d, xb, wb, bias, yb, y32, relu, st, &rc)) return rc;
-        break;
-      default:
-        break;
-    }
     switch (d->Cout) {
       case 16: return launch_tc<16>(ctx, d, xb, wb, bias, yb, y32, relu, st);
       case 32: return launch_tc<32>(ctx, d, xb, wb, bias, yb, y32, relu, st);

@@ -21,7 +21,7 @@ struct Ctx {
   std::string err;
   std::recursive_mutex mu;
   int* d_err = nullptr;  // device error bits
-  int conv_impl = 0;     // 0: tcgen05 (persistent where it fits), 1: mma.sync only, 2: tcgen05 streaming
+  int conv_impl = 0;     // 0: warp-specialised tcgen05 where it fits, 1: mma.sync only, 2: tcgen05 streaming
 };
 
 void set_error(Ctx* ctx, const char* fmt, ...);

@@ -357,6 +357,39 @@ int rx_dn_adam(rx_ctx* ctx, long long n, float* p, float* g, float* m, float* v,
 int rx_denoise(rx_ctx* ctx, int height, int width, const float* color, const float* normal, const float* albedo,
                const float* depth, const rx_denoise_params* params, float* out);
 
+/* ---- Wavefront OBJ text parsed on the device ----------------------------
+ * Replaces the line loop of OBJReader._parse_indexed / load_as_indexed_mesh
+ * (scene/io/obj_reader.py:345-441) with the same results: float64
+ * positions (V,3), normals (N,3), uvs (T,2); int32 tri_pos_idx,
+ * tri_normal_idx, tri_uv_idx (F,3) and tri_group_idx (F).  Sequence:
+ *   rx_obj_begin   upload the text, split lines, classify them;
+ *   rx_obj_listed  the lines the host must read itself: usemtl, mtllib, o,
+ *                  g, unrecognised tokens, lines with non-ASCII bytes, and
+ *                  lines whose numbers are outside the device's exact path
+ *                  (RX_OBJ_HOST in flags);
+ *   rx_obj_correct kind and triangle count of listed non-ASCII lines as
+ *                  the host splits them (positions into the listed list);
+ *   rx_obj_scan    totals {v, vn, vt, triangles, usemtl, faces, listed}
+ *                  and, per listed line, the counts before it {v, vn, vt,
+ *                  triangles, usemtl, faces};
+ *   rx_obj_emit    the arrays (caller host buffers sized from the totals;
+ *                  usemtl_gid = group id of each usemtl line in file order);
+ *                  entries of RX_OBJ_HOST lines are left for the caller;
+ *   rx_obj_end. */
+typedef struct rx_obj rx_obj;
+enum {
+  RX_OBJ_SKIP = 0, RX_OBJ_V = 1, RX_OBJ_VN = 2, RX_OBJ_VT = 3, RX_OBJ_F = 4, RX_OBJ_USEMTL = 5,
+  RX_OBJ_MTLLIB = 6, RX_OBJ_O = 7, RX_OBJ_G = 8, RX_OBJ_S = 9, RX_OBJ_OTHER = 10
+};
+enum { RX_OBJ_HOST = 1, RX_OBJ_NONASCII = 2 };
+int rx_obj_begin(rx_ctx* ctx, const void* text, long long n, rx_obj** out, int* lines, int* listed);
+int rx_obj_listed(rx_obj* o, long long* offset, int* length, int* kind, int* flags, int* line);
+int rx_obj_correct(rx_obj* o, int n, const int* listed_pos, const int* kind, const int* ntri);
+int rx_obj_scan(rx_obj* o, int* totals, int* listed_prefix);
+int rx_obj_emit(rx_obj* o, const int* usemtl_gid, double* positions, double* normals, double* uvs, int* tri_pos_idx,
+                int* tri_normal_idx, int* tri_uv_idx, int* tri_group_idx);
+int rx_obj_end(rx_obj* o);
+
 /* Allocation-free a-trous denoise on caller device buffers.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory at
  * call time (a host that owns the whole device budget through its own

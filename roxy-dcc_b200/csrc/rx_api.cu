@@ -27,6 +27,10 @@ struct rx_server {
   rx::Server* s;
   rx::Ctx* ctx;
 };
+struct rx_obj {
+  rx::ObjParse* o;
+  rx::Ctx* ctx;
+};
 
 namespace rx {
 
@@ -875,6 +879,66 @@ int rx_dn_adam(rx_ctx* ctx, long long n, float* p, float* g, float* m, float* v,
   if (!ctx) return RX_ERR_ARG;
   cudaSetDevice(ctx->c.device);
   return dn_adam(&ctx->c, n, p, g, m, v, p16, lr, b1, b2, eps, step, pick_stream(ctx, stream));
+}
+
+int rx_obj_begin(rx_ctx* ctx, const void* text, long long n, rx_obj** out, int* lines, int* listed) {
+  if (!ctx || !out || n < 0 || (n > 0 && !text)) return set_error(ctx ? &ctx->c : nullptr, "rx_obj_begin: bad arguments"), RX_ERR_ARG;
+  if (n >= (1LL << 40)) return set_error(&ctx->c, "rx_obj_begin: %lld bytes exceed the limit", n), RX_ERR_CAPACITY;
+  LOCK(&ctx->c);
+  cudaSetDevice(ctx->c.device);
+  *out = nullptr;
+  ObjParse* o = nullptr;
+  int rc = obj_begin(&ctx->c, text, n, &o);
+  if (rc) return rc;
+  rx_obj* h = new rx_obj();
+  h->o = o;
+  h->ctx = &ctx->c;
+  int l = 0, s = 0;
+  obj_info(o, &l, &s);
+  if (lines) *lines = l;
+  if (listed) *listed = s;
+  *out = h;
+  return RX_OK;
+}
+
+int rx_obj_listed(rx_obj* o, long long* offset, int* length, int* kind, int* flags, int* line) {
+  if (!o || !offset || !length || !kind || !flags) return RX_ERR_ARG;
+  LOCK(o->ctx);
+  cudaSetDevice(o->ctx->device);
+  return obj_listed(o->o, offset, length, kind, flags, line);
+}
+
+int rx_obj_correct(rx_obj* o, int n, const int* listed_pos, const int* kind, const int* ntri) {
+  if (!o || n < 0 || (n > 0 && (!listed_pos || !kind || !ntri))) return RX_ERR_ARG;
+  LOCK(o->ctx);
+  cudaSetDevice(o->ctx->device);
+  return obj_correct(o->o, n, listed_pos, kind, ntri);
+}
+
+int rx_obj_scan(rx_obj* o, int* totals, int* listed_prefix) {
+  if (!o || !totals) return RX_ERR_ARG;
+  LOCK(o->ctx);
+  cudaSetDevice(o->ctx->device);
+  return obj_scan(o->o, totals, listed_prefix);
+}
+
+int rx_obj_emit(rx_obj* o, const int* usemtl_gid, double* positions, double* normals, double* uvs, int* tri_pos_idx,
+                int* tri_normal_idx, int* tri_uv_idx, int* tri_group_idx) {
+  if (!o) return RX_ERR_ARG;
+  LOCK(o->ctx);
+  cudaSetDevice(o->ctx->device);
+  return obj_emit(o->o, usemtl_gid, positions, normals, uvs, tri_pos_idx, tri_normal_idx, tri_uv_idx, tri_group_idx);
+}
+
+int rx_obj_end(rx_obj* o) {
+  if (!o) return RX_OK;
+  {
+    LOCK(o->ctx);
+    cudaSetDevice(o->ctx->device);
+    obj_end(o->o);
+  }
+  delete o;
+  return RX_OK;
 }
 
 int rx_scene_device_bytes(rx_scene* scene, long long* bytes) {

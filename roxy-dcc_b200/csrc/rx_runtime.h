@@ -248,6 +248,17 @@ int dn_output(Ctx* ctx, long long P, const float* y32, int y_stride, const float
 int dn_adam(Ctx* ctx, long long n, float* p, float* g, float* m, float* v, void* p16, float lr, float b1, float b2,
             float eps, int step, cudaStream_t st);
 
+// OBJ text parsing on the device (rx_obj.cu)
+struct ObjParse;
+int obj_begin(Ctx* ctx, const void* text, long long n, ObjParse** out);
+int obj_info(ObjParse* o, int* lines, int* listed);
+int obj_listed(ObjParse* o, long long* off, int* len, int* kind, int* flags, int* line);
+int obj_correct(ObjParse* o, int n, const int* pos, const int* kind, const int* ntri);
+int obj_scan(ObjParse* o, int* totals, int* listed_prefix);
+int obj_emit(ObjParse* o, const int* usemtl_gid, double* pos, double* nrm, double* uv, int* tri_pos, int* tri_nrm,
+             int* tri_uv, int* tri_grp);
+void obj_end(ObjParse* o);
+
 // device bytes held by each object (serving admission)
 size_t accum_bytes(const Accum* a);
 size_t batch_bytes(const Batch* b);

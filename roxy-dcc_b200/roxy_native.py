@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
 SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu",
-           "rx_serve.cu", "rx_conv.cu"]
+           "rx_serve.cu", "rx_conv.cu", "rx_obj.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
 
 RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE, RX_ERR_TIMEOUT = range(7)
@@ -81,6 +81,9 @@ class DnOp(ctypes.Structure):
 
 
 RX_DN_COPY, RX_DN_RELU_MASK, RX_DN_POOL, RX_DN_POOL_BWD, RX_DN_UP, RX_DN_UP_BWD = range(6)
+(RX_OBJ_SKIP, RX_OBJ_V, RX_OBJ_VN, RX_OBJ_VT, RX_OBJ_F, RX_OBJ_USEMTL, RX_OBJ_MTLLIB, RX_OBJ_O, RX_OBJ_G, RX_OBJ_S,
+ RX_OBJ_OTHER) = range(11)
+RX_OBJ_HOST, RX_OBJ_NONASCII = 1, 2
 
 
 class DenoiseParams(ctypes.Structure):
@@ -196,6 +199,15 @@ _SIGS = {
                     ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_denoise_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.POINTER(DenoiseParams), ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rx_obj_begin": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_void_p), _i32p,
+                      _i32p], ctypes.c_int),
+    "rx_obj_listed": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_void_p], ctypes.c_int),
+    "rx_obj_correct": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                       ctypes.c_int),
+    "rx_obj_scan": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rx_obj_emit": ([ctypes.c_void_p] + [ctypes.c_void_p] * 8, ctypes.c_int),
+    "rx_obj_end": ([ctypes.c_void_p], ctypes.c_int),
 }
 
 

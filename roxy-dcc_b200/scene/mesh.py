@@ -68,6 +68,15 @@ class IndexedMesh:
     triangle_count = property(lambda s: len(s._tri_pos_idx))
     groups = property(lambda s: list(s._groups))
 
+    def triangle_vertices(self, tri_i):
+        """Vec3 corners of triangle tri_i (scene/mesh.py:382-384)."""
+        row = self._positions[self._tri_pos_idx[tri_i]]
+        return tuple(Vec3(float(r[0]), float(r[1]), float(r[2])) for r in row)
+
+    def group_for_triangle(self, tri_i):
+        """Material group name of triangle tri_i (scene/mesh.py:394-395)."""
+        return self._groups[int(self._tri_group_idx[tri_i])]
+
     def taichi_type_id(self):
         return 6
 

@@ -457,6 +457,164 @@ def make_sampling(out_dir):
     print("sampling.npz written")
 
 
+def _obj_num(rng, x):
+    """One number in one of the spellings OBJ exporters and people write."""
+    k = int(rng.integers(0, 10))
+    if k == 0:
+        return f"{x:.6f}"
+    if k == 1:
+        return f"{x:.3e}"
+    if k == 2:
+        return repr(float(x))  # up to 17 significant digits
+    if k == 3:
+        return f"{x:+.4f}"
+    if k == 4:
+        return f"{x:.9g}"
+    if k == 5:
+        return f"{x:.2E}"
+    if k == 6:
+        return str(int(round(x)))
+    if k == 7:
+        return f"{x:.1f}".replace("0.", ".", 1) if abs(x) < 1 and x >= 0 else f"{x:.1f}"
+    if k == 8:
+        return f"{x:.22f}"  # too many digits for the device's exact path
+    return f"{x:.5f}"
+
+
+def _obj_text(seed, n_blocks):
+    """Seeded OBJ text covering the reader's cases: v with extra components,
+    vt with 2 and 3, vn; faces of 2..6 vertices in every index form
+    (v, v/t, v//n, v/t/n, v/t/n/extra), absolute and relative indices;
+    usemtl runs (repeated, unnamed, non-ASCII); o / g / s / mtllib;
+    comments, blank lines, tabs, CRLF and lone CR endings; unrecognised
+    keywords; numbers with exponents, signs, long digit strings, inf / nan
+    and underscores."""
+    rng = np.random.default_rng(seed)
+    out = ["# synthetic OBJ, seed %d" % seed, "mtllib not_there.mtl", "", "o Body", "g part0", "s off"]
+    nv = nvt = nvn = 0
+    mats = ["red", "green", "blue", "steel", "mat_été", "red"]
+    for b in range(n_blocks):
+        for _ in range(int(rng.integers(3, 9))):
+            xs = rng.normal(size=4) * 10.0 ** rng.integers(-3, 3)
+            extra = " " + _obj_num(rng, xs[3]) if rng.random() < 0.1 else ""
+            out.append("v " + " ".join(_obj_num(rng, x) for x in xs[:3]) + extra)
+            nv += 1
+        for _ in range(int(rng.integers(0, 5))):
+            us = rng.random(3)
+            third = " " + _obj_num(rng, us[2]) if rng.random() < 0.2 else ""
+            out.append("vt\t" + " ".join(_obj_num(rng, u) for u in us[:2]) + third)
+            nvt += 1
+        for _ in range(int(rng.integers(0, 5))):
+            ns = rng.normal(size=3)
+            out.append("vn  " + " ".join(_obj_num(rng, n) for n in ns) + "  ")
+            nvn += 1
+        r = rng.random()
+        if r < 0.15:
+            name = mats[int(rng.integers(0, len(mats)))]
+            out.append("usemtl " + name if rng.random() < 0.9 else "usemtl")
+        elif r < 0.2:
+            out.append("g part%d" % b)
+        elif r < 0.23:
+            out.append("o Obj%d" % b)
+        for _ in range(int(rng.integers(1, 6))):
+            nverts = int(rng.integers(2, 7)) if rng.random() < 0.1 else int(rng.choice([3, 3, 3, 4]))
+            form = int(rng.integers(0, 5))
+            toks = []
+            for _ in range(nverts):
+                def ref(count):
+                    i = int(rng.integers(0, count))
+                    return str(i + 1) if rng.random() < 0.7 else str(i - count)
+                v = ref(nv)
+                t = ref(nvt) if nvt else ""
+                n = ref(nvn) if nvn else ""
+                if form == 0 or (form in (1, 3, 4) and not nvt) or (form == 2 and not nvn):
+                    toks.append(v)
+                elif form == 1:
+                    toks.append(v + "/" + t)
+                elif form == 2:
+                    toks.append(v + "//" + n)
+                elif form == 3:
+                    toks.append(v + "/" + t + "/" + (n if nvn else ""))
+                else:
+                    toks.append(v + "/" + t + "/" + (n if nvn else "") + "/9")
+            out.append("f " + " ".join(toks))
+        if rng.random() < 0.05:
+            out.append(["vp 0.5 0.5", "l 1 2", "# café comment", "s 1", "", "   "][int(rng.integers(0, 6))])
+    # numbers only the host converts, read as Python's float() does
+    out.append("v 1_000.25 inf -nan")
+    out.append("v 0.1000000000000000055511151231257827 1e-400 1e400")
+    out.append("f -1 -2 -3")
+    enders = ["\n"] * 18 + ["\r\n", "\r"]
+    return "".join(line + enders[int(rng.integers(0, len(enders)))] for line in out) + "f 1 2 3"
+
+
+def _tree(node, indexed):
+    shapes = []
+    for s in node.shapes:
+        g = s.geometry
+        tris = g.triangle_count if indexed else len(g._triangles)
+        shapes.append({"name": s.name if hasattr(s, "name") else "", "groups": sorted(s.material_groups.keys()),
+                       "tris": int(tris)})
+    return {"name": node.name, "shapes": shapes, "children": [_tree(c, indexed) for c in node.children]}
+
+
+def make_obj(out_dir):
+    """obj_*.npz: OBJ text and what OBJReader (scene/io/obj_reader.py) reads
+    from it: load_as_indexed_mesh arrays, _parse_indexed material groups,
+    the load(indexed=True / False) hierarchies and the printed warnings."""
+    import contextlib
+    import io
+    import json
+    import tempfile
+    from scene.io.obj_reader import OBJReader
+
+    cases = {
+        "obj_small": ("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nvt 0 0\nvt 1 0\nvt 0 1\nvn 0 0 1\n"
+                      "usemtl matA\nf 1/1/1 2/2/1 3/3/1\nusemtl matB\nf 2//1 4//1 3//1\nf 1 2 3 4\n"
+                      "usemtl matA\nf -4 -3 -2\n"),
+        "obj_random": _obj_text(7, 160),
+    }
+    for name, text in cases.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, name + ".obj")
+            with open(path, "w", newline="") as f:
+                f.write(text)
+            warn = io.StringIO()
+            with contextlib.redirect_stdout(warn):
+                mesh, mat_groups = OBJReader._parse_indexed(path)
+            tree_ix = _tree(OBJReader.load(path, indexed=True), True)
+            with contextlib.redirect_stdout(io.StringIO()):
+                tree_py = _tree(OBJReader.load(path, indexed=False), False)
+        z = lambda a, w: np.zeros((0, w)) if a is None else np.asarray(a)
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"),
+            text=np.frombuffer(text.encode("utf-8"), np.uint8),
+            positions=z(mesh._positions, 3), normals=z(mesh._normals, 3), uvs=z(mesh._uvs, 2),
+            has_normals=mesh._normals is not None, has_uvs=mesh._uvs is not None,
+            tri_pos_idx=mesh._tri_pos_idx, tri_normal_idx=mesh._tri_normal_idx, tri_uv_idx=mesh._tri_uv_idx,
+            tri_group_idx=mesh._tri_group_idx,
+            meta=np.frombuffer(json.dumps({"groups": list(mesh._groups), "mat_groups": sorted(mat_groups),
+                                           "tree_indexed": tree_ix, "tree_python": tree_py,
+                                           "warnings": warn.getvalue().splitlines()}).encode(), np.uint8))
+        print(name + ".npz written", mesh.vertex_count, "verts", mesh.triangle_count, "tris")
+
+
+def make_rxb(out_dir):
+    """meshes.rxb: an archive written by save_rxb_meshes
+    (scene/io/roxy_binary.py:13-83), two meshes sharing one position buffer."""
+    from scene.io.roxy_binary import save_rxb_meshes
+    from scene.mesh import IndexedMesh
+    rng = np.random.default_rng(11)
+    pos = rng.normal(size=(40, 3))
+    a = IndexedMesh(pos, rng.integers(0, 40, size=(25, 3)), normals=rng.normal(size=(40, 3)),
+                    tri_normal_idx=rng.integers(0, 40, size=(25, 3)), uvs=rng.random((40, 2)),
+                    tri_uv_idx=rng.integers(0, 40, size=(25, 3)), groups=["paint", "rubber"],
+                    tri_group_idx=rng.integers(0, 2, size=25), name="frame", build_bvh=False)
+    b = IndexedMesh(pos, rng.integers(0, 40, size=(7, 3)), name="wheel", build_bvh=False)
+    save_rxb_meshes(os.path.join(out_dir, "meshes.rxb"), {"frame": a, "parts/wheel": b})
+    print("meshes.rxb written")
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ROXY_REFERENCE")
     if not ref_root or not os.path.isdir(ref_root):
@@ -464,7 +622,7 @@ def main():
     _setup(ref_root)
     np.seterr(all="ignore")
     makers = [make_bvh, make_denoise, make_sampling, make_prims, make_traversal, make_trace_scene,
-              make_texture_scene]
+              make_texture_scene, make_obj, make_rxb]
     only = sys.argv[2:]  # optional generator names, e.g. make_texture_scene
     for fn in makers:
         if not only or fn.__name__ in only:

@@ -195,3 +195,27 @@ def test_philox_known_answer():
         [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
     assert list(oracle.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], 0xA4093822, 0x299F31D0)) == \
         [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def _f64_bits_equal(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+@pytest.mark.parametrize("name", ["obj_small", "obj_random"])
+def test_obj_parse_restatement_matches_reference_reader(name):
+    """oracle.obj_parse against OBJReader._parse_indexed run on the same text:
+    float64 bits (inf / nan / -0.0 included), index tables, group names,
+    used groups and the unrecognised-token warnings."""
+    import json
+    from oracle.obj_parse import parse_indexed
+    g = _load(name + ".npz")
+    meta = json.loads(bytes(g["meta"]).decode())
+    r = parse_indexed(bytes(g["text"]))
+    for k in ("positions", "normals", "uvs"):
+        assert _f64_bits_equal(r[k], g[k]), k
+    for k in ("tri_pos_idx", "tri_normal_idx", "tri_uv_idx", "tri_group_idx"):
+        np.testing.assert_array_equal(r[k], g[k], err_msg=k)
+    assert r["groups"] == meta["groups"]
+    assert sorted(r["used_groups"]) == meta["mat_groups"]
+    assert [f"Warning: Unrecognized OBJ token: {t!r}" for t in r["unknown"]] == meta["warnings"]

@@ -388,6 +388,9 @@ int rx_obj_correct(rx_obj* o, int n, const int* listed_pos, const int* kind, con
 int rx_obj_scan(rx_obj* o, int* totals, int* listed_prefix);
 int rx_obj_emit(rx_obj* o, const int* usemtl_gid, double* positions, double* normals, double* uvs, int* tri_pos_idx,
                 int* tri_normal_idx, int* tri_uv_idx, int* tri_group_idx);
+/* Device time (ms, CUDA events) of the parse so far: the kernels only, without
+ * the text upload, the result copies and the host's reading of listed lines. */
+int rx_obj_device_ms(rx_obj* o, float* ms);
 int rx_obj_end(rx_obj* o);
 
 /* Allocation-free a-trous denoise on caller device buffers.  No counterpart in

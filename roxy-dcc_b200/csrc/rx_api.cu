@@ -930,6 +930,13 @@ int rx_obj_emit(rx_obj* o, const int* usemtl_gid, double* positions, double* nor
   return obj_emit(o->o, usemtl_gid, positions, normals, uvs, tri_pos_idx, tri_normal_idx, tri_uv_idx, tri_group_idx);
 }
 
+int rx_obj_device_ms(rx_obj* o, float* ms) {
+  if (!o || !ms) return RX_ERR_ARG;
+  LOCK(o->ctx);
+  cudaSetDevice(o->ctx->device);
+  return obj_device_ms(o->o, ms);
+}
+
 int rx_obj_end(rx_obj* o) {
   if (!o) return RX_OK;
   {

@@ -472,6 +472,28 @@ struct ObjParse {
   DevBuf<int> cnt;  // C_N x lines
   DevBuf<int> totals;
   DevBuf<int> listed;
+  // CUDA-event pairs around each stretch of device work (no host waits or
+  // copies of the text / results inside), summed by obj_device_ms
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> spans;
+  void span_begin() {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+      cudaEventDestroy(a);
+      return;
+    }
+    cudaEventRecord(a, ctx->stream);
+    spans.push_back({a, b});
+  }
+  void span_end() {
+    if (!spans.empty()) cudaEventRecord(spans.back().second, ctx->stream);
+  }
+  ~ObjParse() {
+    for (auto& s : spans) {
+      cudaEventDestroy(s.first);
+      cudaEventDestroy(s.second);
+    }
+  }
 };
 
 static int grid_for(Ctx* ctx, long long n, int per_block = 256) {
@@ -497,8 +519,10 @@ int obj_begin(Ctx* ctx, const void* text, long long n, ObjParse** out) {
   // line starts
   DevBuf<int> blk(ctx, (size_t)nb + 1);
   if (!blk.p) return fail((set_error(ctx, "obj: out of device memory"), RX_ERR_CAPACITY));
+  o->span_begin();
   k_line_count<<<(unsigned)nb, kLineThreads, 0, st>>>(o->text.p, n, blk.p);
   int rc = excl_scan(ctx, blk.p, nb, blk.p + nb);
+  o->span_end();
   if (rc) return fail(rc);
   int lines = 0;
   if (cudaMemcpyAsync(&lines, blk.p + nb, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -508,19 +532,26 @@ int obj_begin(Ctx* ctx, const void* text, long long n, ObjParse** out) {
   if (!o->starts.alloc(ctx, (size_t)lines + 1) || !o->kind.alloc(ctx, std::max(lines, 1)) ||
       !o->flags.alloc(ctx, std::max(lines, 1)) || !o->cnt.alloc(ctx, (size_t)C_N * std::max(lines, 1)))
     return fail((set_error(ctx, "obj: out of device memory for %d lines", lines), RX_ERR_CAPACITY));
-  k_line_write<<<(unsigned)nb, kLineThreads, 0, st>>>(o->text.p, n, blk.p, o->starts.p);
   if (cudaMemcpyAsync(o->starts.p + lines, &o->n, sizeof(long long), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return fail((set_error(ctx, "obj: upload failed"), RX_ERR_CUDA));
+  o->span_begin();
+  k_line_write<<<(unsigned)nb, kLineThreads, 0, st>>>(o->text.p, n, blk.p, o->starts.p);
   if (lines > 0) {
     k_classify<<<grid_for(ctx, lines), 256, 0, st>>>(o->text.p, o->starts.p, lines, o->kind.p, o->flags.p, o->cnt.p);
-    if ((rc = excl_scan(ctx, o->cnt.p + (long long)C_LIST * lines, lines, o->totals.p + C_LIST))) return fail(rc);
+    rc = excl_scan(ctx, o->cnt.p + (long long)C_LIST * lines, lines, o->totals.p + C_LIST);
+    o->span_end();
+    if (rc) return fail(rc);
     int nl = 0;
     if (cudaMemcpyAsync(&nl, o->totals.p + C_LIST, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       return fail((set_error(ctx, "obj: %s", cudaGetErrorString(cudaGetLastError())), RX_ERR_CUDA));
     o->n_listed = nl;
     if (!o->listed.alloc(ctx, std::max(nl, 1))) return fail((set_error(ctx, "obj: out of device memory"), RX_ERR_CAPACITY));
+    o->span_begin();
     k_list<<<grid_for(ctx, lines), 256, 0, st>>>(o->kind.p, o->flags.p, o->cnt.p, lines, o->listed.p);
+    o->span_end();
+  } else {
+    o->span_end();
   }
   if (cudaGetLastError() != cudaSuccess) return fail((set_error(ctx, "obj: kernel launch failed"), RX_ERR_CUDA));
   *out = o;
@@ -577,10 +608,12 @@ int obj_scan(ObjParse* o, int* totals, int* listed_prefix) {
   Ctx* ctx = o->ctx;
   cudaStream_t st = ctx->stream;
   if (!o->scanned) {
+    o->span_begin();
     for (int c = 0; c < C_LIST; ++c) {
       int rc = excl_scan(ctx, o->cnt.p + (long long)c * o->lines, o->lines, o->totals.p + c);
       if (rc) return rc;
     }
+    o->span_end();
     CUDA_TRY(ctx, cudaMemcpyAsync(o->tot, o->totals.p, sizeof(int) * C_N, cudaMemcpyDeviceToHost, st));
     o->scanned = true;
   }
@@ -608,9 +641,11 @@ int obj_emit(ObjParse* o, const int* usemtl_gid, double* pos, double* nrm, doubl
       !d_gid.p)
     return set_error(ctx, "obj: out of device memory for the mesh arrays"), RX_ERR_CAPACITY;
   if (nm) CUDA_TRY(ctx, cudaMemcpyAsync(d_gid.p, usemtl_gid, sizeof(int) * nm, cudaMemcpyHostToDevice, st));
+  o->span_begin();
   if (o->lines > 0)
     k_emit<<<grid_for(ctx, o->lines), 256, 0, st>>>(o->text.p, o->starts.p, o->lines, o->kind.p, o->flags.p, o->cnt.p,
                                                    d_gid.p, d_pos.p, d_nrm.p, d_uv.p, d_tp.p, d_tn.p, d_tu.p, d_tg.p);
+  o->span_end();
   CUDA_TRY(ctx, cudaGetLastError());
   auto d2h = [&](void* dst, const void* src, size_t bytes) {
     return bytes && dst ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st) : cudaSuccess;
@@ -631,6 +666,18 @@ void obj_end(ObjParse* o) {
   Ctx* ctx = o->ctx;
   delete o;
   cudaStreamSynchronize(ctx->stream);
+}
+
+int obj_device_ms(ObjParse* o, float* ms) {
+  float total = 0.0f;
+  for (auto& s : o->spans) {
+    float t = 0.0f;
+    CUDA_TRY(o->ctx, cudaEventSynchronize(s.second));
+    CUDA_TRY(o->ctx, cudaEventElapsedTime(&t, s.first, s.second));
+    total += t;
+  }
+  *ms = total;
+  return RX_OK;
 }
 
 int obj_info(ObjParse* o, int* lines, int* listed) {

@@ -258,6 +258,7 @@ int obj_scan(ObjParse* o, int* totals, int* listed_prefix);
 int obj_emit(ObjParse* o, const int* usemtl_gid, double* pos, double* nrm, double* uv, int* tri_pos, int* tri_nrm,
              int* tri_uv, int* tri_grp);
 void obj_end(ObjParse* o);
+int obj_device_ms(ObjParse* o, float* ms);
 
 // device bytes held by each object (serving admission)
 size_t accum_bytes(const Accum* a);

@@ -207,6 +207,7 @@ _SIGS = {
                        ctypes.c_int),
     "rx_obj_scan": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "rx_obj_emit": ([ctypes.c_void_p] + [ctypes.c_void_p] * 8, ctypes.c_int),
+    "rx_obj_device_ms": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "rx_obj_end": ([ctypes.c_void_p], ctypes.c_int),
 }
 

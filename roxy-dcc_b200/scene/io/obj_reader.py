@@ -65,6 +65,7 @@ class ObjData:
         self.events = []  # (keyword, parts, counts before the line: v, vn, vt, tri, usemtl, faces)
         self.lines = 0
         self.totals = np.zeros(7, np.int32)  # v, vn, vt, tri, usemtl, faces, listed
+        self.device_ms = 0.0  # kernel time of the parse (CUDA events)
 
     triangle_count = property(lambda s: len(s.tri_pos_idx))
 
@@ -170,6 +171,9 @@ def _finish(ctx, L, h, data, n_lines, n_listed):
             out.tri_uv_idx[t] = (uvi[0], uvi[j], uvi[j + 1])
             out.tri_normal_idx[t] = (ni[0], ni[j], ni[j + 1])
             out.tri_group_idx[t] = g
+    ms = ctypes.c_float()
+    ctx.check(L.rx_obj_device_ms(h, ctypes.byref(ms)))
+    out.device_ms = ms.value
     return out
 
 

@@ -237,3 +237,26 @@ def camera_params(world, width, height):
     cam = world.active_camera
     return dict(fov_tan=math.tan(math.radians(cam.fov) / 2), aspect=cam.aspect_ratio, cam_pos=list(cam.position),
                 cam_fwd=list(cam.forward), cam_right=list(cam.right), cam_up=list(cam.up))
+
+
+def obj_text(copies=8, subdiv=7, seed=2024):
+    """The OBJ-ingestion workload: `copies` translated instances of the
+    displaced icosphere (327,680 triangles each at subdiv 7) as Wavefront
+    text, written the way exporters write it: one `o` and `usemtl` per copy,
+    `v` / `vn` rows with six decimals, faces as v//vn triples.  Seeded; with
+    8 copies about 2.6 M triangles in 190 MB of text."""
+    pos, faces = icosphere(subdiv)
+    pos = pos * (1.0 + 0.05 * value_noise3(pos, seed + 1))[:, None]
+    nrm = vertex_normals(pos, faces)
+    nv = len(pos)
+    vn_lines = "\n".join(f"vn {a:.6f} {b:.6f} {c:.6f}" for a, b, c in nrm.tolist())
+    out = ["# displaced icosphere x %d, seed %d" % (copies, seed)]
+    for k in range(copies):
+        p = pos + np.array([2.5 * (k % 4), 0.0, 2.5 * (k // 4)])
+        out.append(f"o sphere{k}")
+        out.append("\n".join(f"v {a:.6f} {b:.6f} {c:.6f}" for a, b, c in p.tolist()))
+        out.append(vn_lines)
+        out.append(f"usemtl mat{k % 3}")
+        f = faces + 1 + k * nv
+        out.append("\n".join(f"f {a}//{a} {b}//{b} {c}//{c}" for a, b, c in f.tolist()))
+    return ("\n".join(out) + "\n").encode("ascii")

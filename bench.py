@@ -552,7 +552,10 @@ def run_denoiser(args):
             "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": "learned denoiser, 3-level U-Net 32/64/128, 1920x1080 4-spp render of the "
                                    "displaced-icosphere scene", "flops_per_frame": r["flops_per_frame"]},
-            "roofline": {"bound": "tensor", "kernel": "k_conv_fwd (all layers of one inference)",
+            "roofline": {"bound": "tensor",
+                         "kernel": "whole inference: k_conv_fwd_ws (tcgen05, 9 layers) + k_conv_fwd (mma.sync, the "
+                                   "2 layers whose weights do not fit beside the row ring) + pool / upsample / "
+                                   "feature / output kernels; network FLOPs over the inference time",
                          "achieved": r["infer_tflops"], "peak": peak, "unit": "TFLOP/s",
                          "frac": r["infer_tflops"] / peak,
                          "peak_source": "measured" if "bf16_tflops" in peaks else "fallback", "traffic": None},

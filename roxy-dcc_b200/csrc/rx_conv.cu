@@ -883,6 +883,61 @@ __global__ void k_pool2(int N, int H, int W, int C, const bf16* __restrict__ x, 
   }
 }
 
+// The same two layers on 8-channel (16-byte) chunks, for views whose
+// channel count, stride and offset are multiples of 8: one item per chunk
+// of an input pixel (upsample: one load, four stores) or of an output pixel
+// (pool: four loads, one store); same float32 sum order as above.
+__device__ __forceinline__ void chunk_index(long long i, int CK, int W, int H, int& ck, int& x, int& y, long long& n) {
+  ck = (int)(i % CK);
+  long long q = i / CK;
+  x = (int)(q % W);
+  q /= W;
+  y = (int)(q % H);
+  n = q / H;
+}
+
+__global__ void k_up2_v8(int N, int H, int W, int C, const bf16* __restrict__ x, int x_stride, int x_off,
+                         bf16* __restrict__ y, int y_stride, int y_off) {
+  const int CK = C >> 3;
+  RX_EW_LOOP((long long)N * H * W * CK) {
+    int ck, xx, yy;
+    long long n;
+    chunk_index(i, CK, W, H, ck, xx, yy, n);
+    const uint4 v = *reinterpret_cast<const uint4*>(x + ((n * H + yy) * W + xx) * x_stride + x_off + ck * 8);
+    const long long o = (n * 2 * H + 2 * yy) * 2LL * W + 2 * xx;
+    bf16* d = y + y_off + ck * 8;
+    *reinterpret_cast<uint4*>(d + o * y_stride) = v;
+    *reinterpret_cast<uint4*>(d + (o + 1) * y_stride) = v;
+    *reinterpret_cast<uint4*>(d + (o + 2LL * W) * y_stride) = v;
+    *reinterpret_cast<uint4*>(d + (o + 2LL * W + 1) * y_stride) = v;
+  }
+}
+
+__global__ void k_pool2_v8(int N, int H, int W, int C, const bf16* __restrict__ x, int x_stride, int x_off,
+                           bf16* __restrict__ y, int y_stride, int y_off) {
+  const int CK = C >> 3, h2 = H / 2, w2 = W / 2;
+  RX_EW_LOOP((long long)N * h2 * w2 * CK) {
+    int ck, xo, yo;
+    long long n;
+    chunk_index(i, CK, w2, h2, ck, xo, yo, n);
+    const long long b = (n * H + 2 * yo) * W + 2 * xo;
+    const bf16* s = x + x_off + ck * 8;
+    uint4 q[4] = {*reinterpret_cast<const uint4*>(s + b * x_stride),
+                  *reinterpret_cast<const uint4*>(s + (b + 1) * x_stride),
+                  *reinterpret_cast<const uint4*>(s + (b + W) * x_stride),
+                  *reinterpret_cast<const uint4*>(s + (b + W + 1) * x_stride)};
+    const bf16* e[4] = {reinterpret_cast<const bf16*>(&q[0]), reinterpret_cast<const bf16*>(&q[1]),
+                        reinterpret_cast<const bf16*>(&q[2]), reinterpret_cast<const bf16*>(&q[3])};
+    uint4 out;
+    bf16* o = reinterpret_cast<bf16*>(&out);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      o[k] = __float2bfloat16_rn(0.25f * (__bfloat162float(e[0][k]) + __bfloat162float(e[1][k]) +
+                                          __bfloat162float(e[2][k]) + __bfloat162float(e[3][k])));
+    *reinterpret_cast<uint4*>(y + ((n * h2 + yo) * w2 + xo) * y_stride + y_off + ck * 8) = out;
+  }
+}
+
 // gradient of the pool: each input pixel gets a quarter of its output's
 // gradient; accumulate adds to dx
 __global__ void k_pool2_bwd(int N, int H, int W, int C, const bf16* __restrict__ dy, int dy_stride, int dy_off,
@@ -1177,6 +1232,9 @@ int dn_op(Ctx* ctx, const rx_dn_op* o, cudaStream_t st) {
   const bf16* a = static_cast<const bf16*>(o->a);
   bf16* b = static_cast<bf16*>(o->b);
   long long P = (long long)o->N * o->H * o->W;
+  // 16-byte chunks when channel count, strides, offsets and bases allow
+  const bool v8 = o->C % 8 == 0 && o->a_stride % 8 == 0 && o->a_off % 8 == 0 && o->b_stride % 8 == 0 &&
+                  o->b_off % 8 == 0 && ((uintptr_t)a & 15) == 0 && ((uintptr_t)b & 15) == 0;
   switch (o->kind) {
     case RX_DN_COPY:
       k_copy_ch<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(P, o->C, a, o->a_stride, o->a_off, b, o->b_stride, o->b_off,
@@ -1188,8 +1246,12 @@ int dn_op(Ctx* ctx, const rx_dn_op* o, cudaStream_t st) {
       break;
     case RX_DN_POOL:
       if (o->H % 2 || o->W % 2) return set_error(ctx, "dn_op: pool needs even H and W"), RX_ERR_ARG;
-      k_pool2<<<ew_blocks(ctx, P / 4 * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
-                                                           o->b_stride, o->b_off);
+      if (v8)
+        k_pool2_v8<<<ew_blocks(ctx, P / 4 * (o->C / 8)), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride,
+                                                                      o->a_off, b, o->b_stride, o->b_off);
+      else
+        k_pool2<<<ew_blocks(ctx, P / 4 * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                             o->b_stride, o->b_off);
       break;
     case RX_DN_POOL_BWD:
       if (o->H % 2 || o->W % 2) return set_error(ctx, "dn_op: pool needs even H and W"), RX_ERR_ARG;
@@ -1197,8 +1259,12 @@ int dn_op(Ctx* ctx, const rx_dn_op* o, cudaStream_t st) {
                                                            o->b_stride, o->b_off, o->flag);
       break;
     case RX_DN_UP:
-      k_up2<<<ew_blocks(ctx, 4 * P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
-                                                         o->b_stride, o->b_off);
+      if (v8)
+        k_up2_v8<<<ew_blocks(ctx, P * (o->C / 8)), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                                o->b_stride, o->b_off);
+      else
+        k_up2<<<ew_blocks(ctx, 4 * P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,
+                                                           o->b_stride, o->b_off);
       break;
     case RX_DN_UP_BWD:
       k_up2_bwd<<<ew_blocks(ctx, P * o->C), 256, 0, st>>>(o->N, o->H, o->W, o->C, a, o->a_stride, o->a_off, b,

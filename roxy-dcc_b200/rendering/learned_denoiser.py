@@ -431,7 +431,24 @@ def main():
     ap.add_argument("--views", type=int, default=48)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--eval", action="store_true")
+    ap.add_argument("--infer", default=None, metavar="WxH",
+                    help="only run `--repeat` inferences of the committed weights on seeded random WxH inputs "
+                         "(the kernel-profiling case) and exit")
+    ap.add_argument("--repeat", type=int, default=3)
     args = ap.parse_args()
+    if args.infer:
+        torch = _torch()
+        w, h = (int(v) for v in args.infer.lower().split("x"))
+        net = Denoiser(weights=load_weights())
+        g = torch.Generator(device=net.dev).manual_seed(1)
+        planes = [torch.rand((1, h, w, 3), generator=g, device=net.dev) for _ in range(3)]
+        dep = torch.rand((1, h, w, 1), generator=g, device=net.dev)
+        for _ in range(args.repeat):
+            net.denoise(*planes, dep)
+        torch.cuda.synchronize()
+        net.ctx.check(nat.lib().rx_ctx_sync(net.ctx.h))
+        print(json.dumps({"infer": [w, h], "repeat": args.repeat}))
+        return
     t0 = time.time()
     data = make_training_set(views_per_scene=args.views)
     t_data = time.time() - t0

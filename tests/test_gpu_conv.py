@@ -129,6 +129,20 @@ def test_pool_and_upsample_match_torch():
     xt = x.float().permute(0, 3, 1, 2)
     _close(p.float().permute(0, 3, 1, 2), F.avg_pool2d(xt, 2), 1e-2)
     _close(u.float().permute(0, 3, 1, 2), F.interpolate(xt, scale_factor=2, mode="nearest"), 1e-6)
+    # channel views (16-byte chunk kernels) and a stride that is not a
+    # multiple of 8 channels (element kernels): the same values
+    for stride, off in ((48, 16), (36, 4)):
+        wide = torch.zeros((N, H, W, stride), dtype=torch.bfloat16, device="cuda")
+        wide[..., off:off + C] = x
+        pv = torch.zeros((N, H // 2, W // 2, stride), dtype=torch.bfloat16, device="cuda")
+        uv = torch.zeros((N, 2 * H, 2 * W, stride), dtype=torch.bfloat16, device="cuda")
+        ctx.check(L.rx_dn_layer(ctx.h, ctypes.byref(nat.DnOp(nat.RX_DN_POOL, N, H, W, C, _p(wide), stride, off,
+                                                             _p(pv), stride, off, 0)), _stream()))
+        ctx.check(L.rx_dn_layer(ctx.h, ctypes.byref(nat.DnOp(nat.RX_DN_UP, N, H, W, C, _p(wide), stride, off,
+                                                             _p(uv), stride, off, 0)), _stream()))
+        torch.cuda.synchronize()
+        assert torch.equal(pv[..., off:off + C], p) and torch.equal(uv[..., off:off + C], u), (stride, off)
+        assert not pv[..., :off].any() and not uv[..., off + C:].any()
     # gradients
     gp = torch.randn((N, H // 2, W // 2, C), device="cuda").to(torch.bfloat16)
     gx = torch.zeros_like(x)

@@ -59,6 +59,9 @@ typedef struct {
                                   again on BSDF hits, as trace.py does          */
   uint32_t seed;               /* counter-based RNG key                         */
   int wave_paths;              /* paths per wavefront (0 = automatic)           */
+  int mis;                     /* default estimator only: weigh NEE and BSDF
+                                  hits of listed lights by the power heuristic
+                                  (needs rx_scene_set_light_sources)            */
 } rx_render_params;
 
 /* Edge-aware filter (rendering/denoise.py:23-104) and its a-trous extension:
@@ -152,6 +155,12 @@ int rx_scene_set_objects(rx_scene* scene, int n, const int* type, const float* c
 int rx_scene_set_lights(rx_scene* scene, int n, const int* kind, const float* p0, const float* p1,
                         const float* p2, const float* albedo, const float* emission, const float* area,
                         const float* pick_pdf, const float* alias_prob, const int* alias_idx);
+/* What each light of the last rx_scene_set_lights is: the caller's triangle
+ * index (triangle lights) or the object slot (sphere lights).  Needed only
+ * for multiple importance sampling (rx_render_params.mis): a BSDF ray that
+ * hits a light then weighs its emission against the light-sampling pdf
+ * (power heuristic, rendering/sampling.py:36-45 mis_power_weight). */
+int rx_scene_set_light_sources(rx_scene* scene, int n, const int* source);
 
 /* BVH build on the device.  RX_BVH_REFERENCE reproduces GPUBVHBuilder.build's
  * Morton method (bvh_builder.py:315-478) node for node; RX_BVH_LBVH_SAH builds

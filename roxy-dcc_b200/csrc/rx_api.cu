@@ -68,11 +68,14 @@ int Scene::upload_palette(Ctx* c) {
   return RX_OK;
 }
 
-int Scene::upload_linear_objects(Ctx* c, bool exclude_spheres) {
+// The linear slots scanned before the BVH: all objects, or, when the BVH
+// holds the bounded analytic objects (spheres and cubes), planes and slot
+// triangles only.
+int Scene::upload_linear_objects(Ctx* c, bool exclude_bvh_objects) {
   std::vector<ObjSlot> lin;
   lin_slot.clear();
   for (int i = 0; i < (int)objs.size(); ++i) {
-    if (exclude_spheres && objs[i].type == 0) continue;
+    if (exclude_bvh_objects && (objs[i].type == 0 || objs[i].type == 2)) continue;
     lin.push_back(objs[i]);
     lin_slot.push_back(i);
   }
@@ -81,6 +84,28 @@ int Scene::upload_linear_objects(Ctx* c, bool exclude_spheres) {
   if (!lin.empty())
     CUDA_TRY(c, cudaMemcpyAsync(d_objs.p, lin.data(), sizeof(ObjSlot) * lin.size(), cudaMemcpyHostToDevice,
                                 c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  ++version;
+  return upload_light_maps(c);
+}
+
+// light index of every emitting triangle / object slot / linear object
+int Scene::upload_light_maps(Ctx* c) {
+  if (light_src.empty() || (int)light_src.size() != n_lights || (int)light_kind.size() != n_lights) return RX_OK;
+  std::vector<int> lt(std::max(n_tris, 1), -1), lo(std::max<size_t>(objs.size(), 1), -1), ll(std::max(n_lin, 1), -1);
+  for (int i = 0; i < n_lights; ++i) {
+    const int s = light_src[i];
+    if (light_kind[i] == 1 && s >= 0 && s < n_tris) lt[s] = i;
+    if (light_kind[i] == 0 && s >= 0 && s < (int)objs.size()) lo[s] = i;
+  }
+  for (int j = 0; j < n_lin && j < (int)lin_slot.size(); ++j) ll[j] = lo[lin_slot[j]];
+  auto up = [&](DevBuf<int>& d, const std::vector<int>& h) -> int {
+    if (!d.alloc(c, h.size())) return set_error(c, "out of device memory"), RX_ERR_CAPACITY;
+    CUDA_TRY(c, cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    return RX_OK;
+  };
+  int rc;
+  if ((rc = up(d_light_of_tri, lt)) || (rc = up(d_light_of_obj, lo)) || (rc = up(d_light_of_lin, ll))) return rc;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   ++version;
   return RX_OK;
@@ -429,9 +454,23 @@ int rx_scene_set_lights(rx_scene* scene, int n, const int* kind, const float* p0
       (rc = upload(c, s.d_alias_prob, alias_prob, (size_t)n)) || (rc = upload(c, s.d_alias_idx, alias_idx, (size_t)n)))
     return rc;
   s.n_lights = n;
+  s.light_kind.assign(kind, kind + n);
+  s.light_src.clear();  // sources refer to the previous list
   ++s.version;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return RX_OK;
+}
+
+int rx_scene_set_light_sources(rx_scene* scene, int n, const int* source) {
+  if (!scene) return RX_ERR_ARG;
+  Scene& s = scene->s;
+  Ctx* c = s.ctx;
+  LOCK(c);
+  if (n != s.n_lights || (n > 0 && !source))
+    return set_error(c, "set_light_sources: %d sources for %d lights", n, s.n_lights), RX_ERR_ARG;
+  s.light_src.assign(source, source + n);
+  cudaSetDevice(c->device);
+  return s.upload_light_maps(c);
 }
 
 int rx_bvh_build(rx_scene* scene, int method, int max_leaf, int spheres_in_bvh) {

@@ -35,13 +35,16 @@ __device__ __forceinline__ float3 ldcg3(const float3* p) {
 // ----------------------------------------------------------------------------
 // front end
 // ----------------------------------------------------------------------------
-// Primitive i < n_tris is a triangle, else sphere (i - n_tris).  Triangle
-// bounds are padded by 1e-4 and centroids are (v0 + v1 + v2) / 3 with the
-// reference's float32 order (bvh_builder.py:363-368).
+// Primitive i < n_tris is a triangle, else analytic object i - n_tris
+// (sphere or cube: obj_a = (centre, kind), obj_b = (radius, 0, 0, 0) or
+// (half extents, 0)).  Triangle bounds are padded by 1e-4 and centroids are
+// (v0 + v1 + v2) / 3 with the reference's float32 order
+// (bvh_builder.py:363-368); an object's centroid is its centre.
 __global__ void k_prim_bounds(int n_tris, const float* __restrict__ v0, const float* __restrict__ v1,
-                              const float* __restrict__ v2, int n_sph, const float4* __restrict__ sph,
-                              float3* __restrict__ bmin, float3* __restrict__ bmax, float3* __restrict__ cen) {
-  int n = n_tris + n_sph;
+                              const float* __restrict__ v2, int n_obj, const float4* __restrict__ obj_a,
+                              const float4* __restrict__ obj_b, float3* __restrict__ bmin, float3* __restrict__ bmax,
+                              float3* __restrict__ cen) {
+  int n = n_tris + n_obj;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (i < n_tris) {
       float3 a = f3(v0[3 * i], v0[3 * i + 1], v0[3 * i + 2]);
@@ -51,11 +54,11 @@ __global__ void k_prim_bounds(int n_tris, const float* __restrict__ v0, const fl
       bmax[i] = vmax(a, vmax(b, c)) + f3(1e-4f, 1e-4f, 1e-4f);
       cen[i] = f3(((a.x + b.x) + c.x) / 3.0f, ((a.y + b.y) + c.y) / 3.0f, ((a.z + b.z) + c.z) / 3.0f);
     } else {
-      float4 s = sph[i - n_tris];
-      float r = s.w;
-      bmin[i] = f3(s.x - r, s.y - r, s.z - r) - f3(1e-4f, 1e-4f, 1e-4f);
-      bmax[i] = f3(s.x + r, s.y + r, s.z + r) + f3(1e-4f, 1e-4f, 1e-4f);
-      cen[i] = f3(s.x, s.y, s.z);
+      float4 a = obj_a[i - n_tris], b = obj_b[i - n_tris];
+      float3 e = __float_as_int(a.w) == PRIM_SPHERE ? f3(b.x, b.x, b.x) : f3(b.x, b.y, b.z);
+      bmin[i] = f3(a.x - e.x, a.y - e.y, a.z - e.z) - f3(1e-4f, 1e-4f, 1e-4f);
+      bmax[i] = f3(a.x + e.x, a.y + e.y, a.z + e.z) + f3(1e-4f, 1e-4f, 1e-4f);
+      cen[i] = f3(a.x, a.y, a.z);
     }
   }
 }
@@ -391,9 +394,9 @@ __global__ void k_gather_prims(int n, const int* __restrict__ order, int n_tris,
                                const float* __restrict__ v1, const float* __restrict__ v2,
                                const float* __restrict__ n0, const float* __restrict__ n1,
                                const float* __restrict__ n2, const int* __restrict__ tri_mat,
-                               const float4* __restrict__ sph, const int* __restrict__ sph_mat,
-                               const int* __restrict__ sph_slot, float4* __restrict__ prims,
-                               float4* __restrict__ shade) {
+                               const float4* __restrict__ obj_a, const float4* __restrict__ obj_b,
+                               const int* __restrict__ obj_mat, const int* __restrict__ obj_slot,
+                               float4* __restrict__ prims, float4* __restrict__ shade) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     int i = order[k];
     float4* P = prims + 3 * (size_t)k;
@@ -411,12 +414,11 @@ __global__ void k_gather_prims(int n, const int* __restrict__ order, int n_tris,
       S[2] = make_float4(n2[3 * i], n2[3 * i + 1], n2[3 * i + 2], 0.0f);
     } else {
       int s = i - n_tris;
-      float4 c = sph[s];
-      P[0] = make_float4(c.x, c.y, c.z, __int_as_float(PRIM_SPHERE));
-      P[1] = make_float4(c.w, 0.0f, 0.0f, 0.0f);
+      P[0] = obj_a[s];
+      P[1] = obj_b[s];
       P[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      S[0] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(sph_mat[s]));
-      S[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(sph_slot[s]));
+      S[0] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(obj_mat[s]));
+      S[1] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(obj_slot[s]));
       S[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
   }
@@ -597,13 +599,13 @@ static int grid_for(Ctx* ctx, long long n, int block = 256) {
 }
 
 // Shared front end: bounds, centroids, Morton codes, stable sort.
-static void front_end(Ctx* ctx, Scene* sc, int n_sph, const float4* d_sph, DevBuf<float3>& pmin,
-                      DevBuf<float3>& pmax, DevBuf<int>& order) {
-  int n = sc->n_tris + n_sph;
+static void front_end(Ctx* ctx, Scene* sc, int n_obj, const float4* d_obj_a, const float4* d_obj_b,
+                      DevBuf<float3>& pmin, DevBuf<float3>& pmax, DevBuf<int>& order) {
+  int n = sc->n_tris + n_obj;
   cudaStream_t st = ctx->stream;
   DevBuf<float3> cen(ctx, n);
-  k_prim_bounds<<<grid_for(ctx, n), 256, 0, st>>>(sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, n_sph, d_sph, pmin.p,
-                                                   pmax.p, cen.p);
+  k_prim_bounds<<<grid_for(ctx, n), 256, 0, st>>>(sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, n_obj, d_obj_a, d_obj_b,
+                                                   pmin.p, pmax.p, cen.p);
   int parts = std::min(grid_for(ctx, n), 1024);
   DevBuf<float3> part_min(ctx, parts), part_max(ctx, parts);
   k_reduce_bounds<<<parts, 256, 0, st>>>(n, cen.p, part_min.p, part_max.p);
@@ -620,7 +622,7 @@ int build_reference(Ctx* ctx, Scene* sc, int leaf) {
   if (n <= 0) return RX_OK;
   DevBuf<float3> pmin(ctx, n), pmax(ctx, n);
   DevBuf<int> order(ctx, n);
-  front_end(ctx, sc, 0, nullptr, pmin, pmax, order);
+  front_end(ctx, sc, 0, nullptr, nullptr, pmin, pmax, order);
   long long n_nodes_ll = 2 * median_tree_leaves(n, leaf) - 1;
   int n_nodes = (int)n_nodes_ll;
   DevBuf<int> left(ctx, n_nodes), right(ctx, n_nodes), tstart(ctx, n_nodes), tcount(ctx, n_nodes);
@@ -655,7 +657,7 @@ int build_reference(Ctx* ctx, Scene* sc, int leaf) {
   sc->d_prims.alloc(ctx, (size_t)3 * n);
   sc->d_shade.alloc(ctx, (size_t)3 * n);
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, order.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
-                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr,
+                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr, nullptr,
                                                     sc->d_prims.p, sc->d_shade.p);
   float3 rb[2];
   cudaMemcpyAsync(&rb[0], nmin.p, sizeof(float3), cudaMemcpyDeviceToHost, st);
@@ -702,7 +704,7 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
   sc->d_prims.alloc(ctx, (size_t)3 * n);
   sc->d_shade.alloc(ctx, (size_t)3 * n);
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, ord.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
-                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr,
+                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr, nullptr,
                                                     sc->d_prims.p, sc->d_shade.p);
   sc->ref_left.swap(l);
   sc->ref_right.swap(r);
@@ -726,40 +728,48 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
 int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t, float c_i) {
   cudaStream_t st = ctx->stream;
   sc->clear_bvh();
-  // spheres taken from the object slots into the BVH
-  std::vector<float4> sph;
-  std::vector<int> sph_mat, sph_slot;
+  // bounded analytic objects (spheres, cubes) taken from the object slots
+  // into the BVH; planes (unbounded) and slot triangles stay linear
+  std::vector<float4> oa, ob;
+  std::vector<int> obj_mat, obj_slot;
   sc->bvh_sphere_slots.clear();
   if (spheres_in_bvh) {
     for (int i = 0; i < (int)sc->objs.size(); ++i) {
       const ObjSlot& o = sc->objs[i];
       if (o.type == 0) {
-        sph.push_back(make_float4(o.center.x, o.center.y, o.center.z, o.radius));
-        sph_mat.push_back(o.mat);
-        sph_slot.push_back(i);
+        oa.push_back(make_float4(o.center.x, o.center.y, o.center.z, int_bits_as_float(PRIM_SPHERE)));
+        ob.push_back(make_float4(o.radius, 0.0f, 0.0f, 0.0f));
+      } else if (o.type == 2) {
+        oa.push_back(make_float4(o.center.x, o.center.y, o.center.z, int_bits_as_float(PRIM_CUBE)));
+        ob.push_back(make_float4(o.extra.x, o.extra.y, o.extra.z, 0.0f));
+      } else {
+        continue;
       }
+      obj_mat.push_back(o.mat);
+      obj_slot.push_back(i);
     }
   }
-  sc->bvh_sphere_slots = sph_slot;
+  sc->bvh_sphere_slots = obj_slot;
   sc->upload_linear_objects(ctx, spheres_in_bvh != 0);
-  int n_sph = (int)sph.size();
-  int n = sc->n_tris + n_sph;
+  int n_obj = (int)oa.size();
+  int n = sc->n_tris + n_obj;
   if (n <= 0) return RX_OK;
-  DevBuf<float4> d_sph(ctx, std::max(n_sph, 1));
-  DevBuf<int> d_sph_mat(ctx, std::max(n_sph, 1)), d_sph_slot(ctx, std::max(n_sph, 1));
-  if (n_sph) {
-    cudaMemcpyAsync(d_sph.p, sph.data(), sizeof(float4) * n_sph, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_sph_mat.p, sph_mat.data(), sizeof(int) * n_sph, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_sph_slot.p, sph_slot.data(), sizeof(int) * n_sph, cudaMemcpyHostToDevice, st);
+  DevBuf<float4> d_oa(ctx, std::max(n_obj, 1)), d_ob(ctx, std::max(n_obj, 1));
+  DevBuf<int> d_obj_mat(ctx, std::max(n_obj, 1)), d_obj_slot(ctx, std::max(n_obj, 1));
+  if (n_obj) {
+    cudaMemcpyAsync(d_oa.p, oa.data(), sizeof(float4) * n_obj, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_ob.p, ob.data(), sizeof(float4) * n_obj, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_obj_mat.p, obj_mat.data(), sizeof(int) * n_obj, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_obj_slot.p, obj_slot.data(), sizeof(int) * n_obj, cudaMemcpyHostToDevice, st);
   }
   DevBuf<float3> pmin(ctx, n), pmax(ctx, n);
   DevBuf<int> order(ctx, n);
-  front_end(ctx, sc, n_sph, d_sph.p, pmin, pmax, order);
+  front_end(ctx, sc, n_obj, d_oa.p, d_ob.p, pmin, pmax, order);
   sc->d_prims.alloc(ctx, (size_t)3 * n);
   sc->d_shade.alloc(ctx, (size_t)3 * n);
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, order.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
-                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, d_sph.p, d_sph_mat.p,
-                                                    d_sph_slot.p, sc->d_prims.p, sc->d_shade.p);
+                                                    sc->d_n1, sc->d_n2, sc->d_tri_mat, d_oa.p, d_ob.p, d_obj_mat.p,
+                                                    d_obj_slot.p, sc->d_prims.p, sc->d_shade.p);
   DevBuf<float3> rb(ctx, 2);
   {
     // root box = union of all primitive boxes (two-stage parallel reduction)
@@ -826,7 +836,7 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   sc->root_min = hb[0];
   sc->root_max = hb[1];
   sc->n_prims = n;
-  sc->n_bvh_spheres = n_sph;
+  sc->n_bvh_spheres = n_obj;
   sc->method = RX_BVH_LBVH_SAH;
   sc->exact_slab = 0;
   sc->leaf_size = max_leaf;

@@ -62,7 +62,8 @@ struct Node4 {
 // Primitives in leaf order, three float4 each (48 B):
 //   triangle: a = (v0, kind = 0), b = (v1 - v0, 0), c = (v2 - v0, 0)
 //   sphere:   a = (centre, kind = 1), b = (radius, 0, 0, 0), c = 0
-enum PrimKind { PRIM_TRI = 0, PRIM_SPHERE = 1 };
+//   cube:     a = (centre, kind = 2), b = (half extents, 0), c = 0
+enum PrimKind { PRIM_TRI = 0, PRIM_SPHERE = 1, PRIM_CUBE = 2 };
 
 // Shading record per primitive in leaf order (three float4):
 //   s0 = (n0, material index bits), s1 = (n1, source id bits), s2 = (n2, 0)
@@ -117,6 +118,12 @@ struct DevScene {
   const TexInfo* tex;
   const unsigned char* texels;
   int n_tex;
+  // light index of each emitter (-1: not a light), for the MIS weight of a
+  // BSDF ray that hits a light: by caller triangle, by object slot (BVH
+  // spheres), by linear object index; null when the caller gave no sources
+  const int* light_of_tri;
+  const int* light_of_obj;
+  const int* light_of_lin;
 };
 
 // _sample_texture (rendering/taichi/trace.py:96-126): repeat wrap, optional
@@ -282,6 +289,18 @@ __device__ __forceinline__ float3 cube_normal(float3 p, float3 c, float3 he) {
   if (ax >= ay && ax >= az) return f3(dd.x > 0.0f ? 1.0f : -1.0f, 0.0f, 0.0f);
   if (ay >= az) return f3(0.0f, dd.y > 0.0f ? 1.0f : -1.0f, 0.0f);
   return f3(0.0f, 0.0f, dd.z > 0.0f ? 1.0f : -1.0f);
+}
+
+// t of a BVH-resident analytic primitive (sphere or cube record a, b): the
+// same tests as the object slots, so a sphere or cube moved into the BVH
+// returns the same t
+__device__ __forceinline__ float analytic_t(float3 o, float3 d, float4 a, float4 b) {
+  return __float_as_int(a.w) == PRIM_SPHERE ? sphere_t(o, d, xyz(a), b.x) : cube_t(o, d, xyz(a), xyz(b));
+}
+
+// un-flipped normal at point p of a BVH-resident analytic primitive
+__device__ __forceinline__ float3 analytic_normal(float3 p, float4 a, float4 b) {
+  return __float_as_int(a.w) == PRIM_SPHERE ? normalized(p - xyz(a)) : cube_normal(p, xyz(a), xyz(b));
 }
 
 // Linear scan of the object slots (intersect.py:259-287): closest t and slot.
@@ -452,7 +471,7 @@ __device__ __forceinline__ int bvh_closest_ww(const DevScene& S, float3 o, float
           }
         } else {
           float4 b = __ldg(pp + 1);
-          t = sphere_t(o, d, xyz(a), b.x);
+          t = analytic_t(o, d, a, b);
           if (t > 0.001f && t < tmax) {
             tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
           }
@@ -479,7 +498,7 @@ __device__ __forceinline__ void leaf_closest(const DevScene& S, float3 o, float3
       }
     } else {
       float4 b = __ldg(pp + 1);
-      t = sphere_t(o, d, xyz(a), b.x);
+      t = analytic_t(o, d, a, b);
       if (t > 0.001f && t < tmax) {
         tmax = t; hu = 0.0f; hv = 0.0f; hit = k;
       }
@@ -688,7 +707,7 @@ __device__ __forceinline__ bool bvh_any(const DevScene& S, float3 o, float3 d, f
           if (tri_hit(o, d, a, b, c, max_t, t, u, v)) return true;
         } else {
           float4 b = __ldg(pp + 1);
-          t = sphere_t(o, d, xyz(a), b.x);
+          t = analytic_t(o, d, a, b);
           if (0.001f < t && t < max_t) return true;
         }
       }

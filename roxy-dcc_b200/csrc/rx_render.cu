@@ -43,6 +43,7 @@ struct RenderK {
   int mode, dlmd;
   float clamp;
   int compat;
+  int mis;  // power-heuristic MIS between NEE and BSDF hits of listed lights
   uint32_t seed;
   long long shadow_cap;
   long long queue_cap;
@@ -155,9 +156,12 @@ __device__ __forceinline__ void sphere_light_sample(float3 hit_p, float3 center,
 }
 
 // One light sample without visibility: direction, shadow distance and the
-// contribution it adds if unoccluded (albedo * L * geometry * weight).
+// contribution it adds if unoccluded (albedo * L * geometry * weight);
+// pdf = the density of the sampled direction in solid angle (the light's
+// own sampling, without the pick probability).  The cone sample's `sop` is
+// its solid angle over pi.
 __device__ __forceinline__ bool light_sample(const Light& L, float ru1, float ru2, float3 hit_p, float3 n, float3 alb,
-                                             float weight, float3& dir, float& max_t, float3& val) {
+                                             float weight, float3& dir, float& max_t, float3& val, float& pdf) {
   float3 base = (alb * L.albedo) * L.emission;
   if (L.kind == 0) {
     float3 ldir;
@@ -169,6 +173,7 @@ __device__ __forceinline__ bool light_sample(const Light& L, float ru1, float ru
     if (!(max_t > 0.001f)) return false;
     dir = ldir;
     val = ((base * ndotl) * sop) * weight;
+    pdf = sop > 0.0f ? 1.0f / (kPi * sop) : 0.0f;
     return true;
   }
   float su = sqrtf(ru1);
@@ -189,7 +194,35 @@ __device__ __forceinline__ bool light_sample(const Light& L, float ru1, float ru
   float g = (((ndotl * cos_l) * L.area) / (kPi * d2)) * weight;
   dir = wi;
   val = base * g;
+  pdf = cos_l * L.area > 0.0f ? d2 / (cos_l * L.area) : 3.0e38f;
   return true;
+}
+
+// Solid-angle density with which light L's own sampling picks direction d
+// from point o, given that d reaches L at distance t (the BSDF-hit side of
+// the MIS weight; same formulas as light_sample).
+__device__ __forceinline__ float light_dir_pdf(const Light& L, float3 o, float3 d, float t) {
+  if (L.kind == 0) {
+    float3 to_c = L.p0 - o;
+    float dist2 = fmaxf(dot(to_c, to_c), 1e-6f);
+    float sin2 = fminf(L.p1.x * L.p1.x / dist2, 1.0f);
+    float sop = 2.0f * (1.0f - sqrtf(fmaxf(0.0f, 1.0f - sin2)));
+    return sop > 0.0f ? 1.0f / (kPi * sop) : 0.0f;
+  }
+  float3 ln = normalized(cross(L.p1 - L.p0, L.p2 - L.p0));
+  float cos_l = fabsf(dot(ln, d));
+  return cos_l * L.area > 0.0f ? (t * t) / (cos_l * L.area) : 3.0e38f;
+}
+
+// power heuristic (beta = 2) weight of the strategy with density a against
+// one with density b (rendering/sampling.py:36-45)
+__device__ __forceinline__ float mis_power(float a, float b) {
+  a = fmaxf(a, 0.0f);
+  b = fmaxf(b, 0.0f);
+  if (a >= 1.0e18f) return 1.0f;
+  if (b >= 1.0e18f) return 0.0f;
+  const float aa = a * a, bb = b * b;
+  return aa + bb > 0.0f ? aa / (aa + bb) : 0.0f;
 }
 
 // ------------------------------------------------------------- path sources
@@ -431,7 +464,7 @@ __device__ __forceinline__ int warp_append_n(int cnt, int* counter) {
 }
 
 template <class Src>
-__global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int b, const int* __restrict__ qin,
+__global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int b, const int* __restrict__ qin,
                                                int* __restrict__ qout, int* counters,
                                                const int* __restrict__ frame_base, float4* __restrict__ ray_o,
                                                float4* __restrict__ ray_d, float4* __restrict__ thr_b,
@@ -452,6 +485,8 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int
     const int si = src.seg(qin[valid ? i : base]);
     const DevScene S = src.scene(si);
     const RenderK K = src.params(si);
+    // MIS needs the emitter -> light maps (rx_scene_set_light_sources)
+    const bool mis = K.mis && S.light_of_lin != nullptr;
     const bool last_bounce = (b + 1) >= K.max_depth;
     bool alive = false;
     bool do_nee = false;
@@ -500,9 +535,10 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int
             src_tri = __float_as_int(s1.w);
             nn = normalized((xyz(s0) * w + xyz(s1) * h.z) + xyz(__ldg(sp + 2)) * h.w);
           } else {
-            nn = normalized((o + d * t) - xyz(pa));
+            nn = analytic_normal(o + d * t, pa, __ldg(S.prims + 3 * (size_t)code + 1));
           }
-          listed = true;
+          // triangles and spheres can be lights; cubes are not in the light list
+          listed = __float_as_int(pa.w) != PRIM_CUBE;
         } else {
           const ObjSlot& ob = S.objs[-code - 2];
           m = ob.mat;
@@ -530,10 +566,25 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int
         }
         if (mt == 3) {
           // trace.py:194-196; with NEE on the previous diffuse vertex the
-          // default estimator already counted this emitter
+          // default estimator already counted this emitter, unless MIS
+          // shares it between the two samples
           if (!( !K.compat && prev_nee && listed)) {
             add = (thr * albedo) * em;
             has_add = true;
+          } else if (mis) {
+            int li = -1;
+            if (code >= 0)
+              li = src_tri >= 0 ? __ldg(S.light_of_tri + src_tri)
+                                : __ldg(S.light_of_obj + __float_as_int(__ldg(S.shade + 3 * (size_t)code + 1).w));
+            else
+              li = __ldg(S.light_of_lin + (-code - 2));
+            if (li >= 0) {
+              // d4.w: density of this direction under the previous vertex's BSDF
+              const Light& L = S.lights[li];
+              float pl = light_dir_pdf(L, o, d, t) * (K.mode == 0 ? L.pick_pdf : 1.0f);
+              add = ((thr * albedo) * em) * mis_power(d4.w, pl);
+              has_add = true;
+            }
           }
         } else {
           bool nee_here = false;
@@ -589,7 +640,11 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int
           if (alive) {
             float3 no = hit_p + nn * 1e-4f;
             ray_o[p] = make_float4(no.x, no.y, no.z, cur_ior);
-            ray_d[p] = make_float4(nd.x, nd.y, nd.z, nee_here ? 1.0f : 0.0f);
+            // w: 0 = no NEE here; with MIS the BSDF density of nd through
+            // the lobe NEE stands in for (nee_scale * cos / pi), else 1
+            float nee_w = 0.0f;
+            if (nee_here) nee_w = mis ? fmaxf(nee_scale * dot(nn, nd) / kPi, 1e-30f) : 1.0f;
+            ray_d[p] = make_float4(nd.x, nd.y, nd.z, nee_w);
             thr_b[p] = make_float4(thr.x, thr.y, thr.z, 0.0f);
           }
         }
@@ -631,13 +686,21 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 6 : 1) k_shade(Src src, int
         li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
         w = 1.0f / S.lights[li].pick_pdf;
       }
-      return light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
-                          max_t, val);
+      float pdf;
+      bool ok = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
+                             max_t, val, pdf);
+      // MIS: this light sample against the BSDF lobe that NEE stands in for
+      // (density nee_scale * cos / pi)
+      if (ok && mis) val = val * mis_power(pdf * S.lights[li].pick_pdf, nee_scale * dot(nrm, dir) / kPi);
+      return ok;
     };
     // direct_light_mode "all": light li with its own random slots
     auto sample_li = [&](int li, float3& dir, float& max_t, float3& val) {
       int s1 = SLOT_ALL_LIGHTS + 4 * li;
-      return light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val);
+      float pdf;
+      bool ok = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val, pdf);
+      if (ok && mis) val = val * mis_power(pdf, nee_scale * dot(nrm, dir) / kPi);
+      return ok;
     };
     bool one_light = false;  // warp-uniform: one scene, mode "one"
     if constexpr (!Src::kBatch) one_light = K.mode == 0;
@@ -893,6 +956,7 @@ static RenderK make_k(const rx_render_params* p, const Accum* a, int spf, long l
   K.dlmd = p->direct_light_max_depth;
   K.clamp = p->sample_clamp;
   K.compat = p->reference_compat;
+  K.mis = p->reference_compat ? 0 : p->mis;
   K.seed = p->seed;
   K.shadow_cap = shadow_cap;
   K.queue_cap = a->cap;

@@ -106,7 +106,7 @@ struct Scene {
   DevBuf<ObjSlot> d_objs;
   int n_lin = 0;
   std::vector<int> lin_slot;         // linear index -> object slot
-  std::vector<int> bvh_sphere_slots;
+  std::vector<int> bvh_sphere_slots;  // object slots of the BVH's spheres and cubes, in build order
   // lights
   DevBuf<Light> d_lights;
   DevBuf<float> d_alias_prob;
@@ -114,7 +114,7 @@ struct Scene {
   int n_lights = 0;
   // traversal structure
   DevBuf<float4> d_nodes, d_prims, d_shade;
-  int n_nodes = 0, n_prims = 0, n_bvh_spheres = 0;
+  int n_nodes = 0, n_prims = 0, n_bvh_spheres = 0;  // n_bvh_spheres: spheres and cubes in the BVH
   float3 root_min = {0, 0, 0}, root_max = {0, 0, 0};
   int method = -1, exact_slab = 0, leaf_size = 0, depth = 0;
   // reference-format copy (reference builder / uploaded trees)
@@ -140,7 +140,7 @@ struct Scene {
     ++version;
   }
   int upload_palette(Ctx* c);
-  int upload_linear_objects(Ctx* c, bool exclude_spheres);
+  int upload_linear_objects(Ctx* c, bool exclude_bvh_objects);
   DevScene view() const {
     DevScene s;
     s.nodes = d_nodes.p;
@@ -164,8 +164,18 @@ struct Scene {
     s.tex = d_tex.p;
     s.texels = d_texels.p;
     s.n_tex = n_tex;
+    const bool maps = !light_src.empty() && (int)light_src.size() == n_lights;
+    s.light_of_tri = maps ? d_light_of_tri.p : nullptr;
+    s.light_of_obj = maps ? d_light_of_obj.p : nullptr;
+    s.light_of_lin = maps ? d_light_of_lin.p : nullptr;
     return s;
   }
+  // per light: caller triangle index (triangle lights) or object slot
+  // (sphere lights), as given to rx_scene_set_light_sources; the inverse
+  // maps below are rebuilt whenever lights, triangles or linear objects change
+  std::vector<int> light_src, light_kind;
+  DevBuf<int> d_light_of_tri, d_light_of_obj, d_light_of_lin;
+  int upload_light_maps(Ctx* c);
 };
 
 // BVH builders (rx_bvh.cu)

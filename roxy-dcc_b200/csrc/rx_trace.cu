@@ -49,7 +49,7 @@ __device__ __forceinline__ float3 hit_normal(const DevScene& S, float3 o, float3
       float3 n0 = xyz(__ldg(sp)), n1 = xyz(__ldg(sp + 1)), n2 = xyz(__ldg(sp + 2));
       return normalized((n0 * w + n1 * h.u) + n2 * h.v);
     }
-    return normalized((o + d * h.t) - xyz(a));
+    return analytic_normal(o + d * h.t, a, __ldg(S.prims + 3 * (size_t)h.prim + 1));
   }
   if (h.slot >= 0) {
     const ObjSlot& ob = S.objs[h.slot];

@@ -211,16 +211,20 @@ class DeviceScene:
 
     light_args: (v0, v1, v2, palette index) of at least every emissive
     triangle, in scene order, followed by the palette's type, albedo and
-    emission arrays; pal_texture: texture index per palette entry.
+    emission arrays; light_index: scene triangle index of each of those rows
+    (None: the rows are all triangles in scene order); pal_texture: texture
+    index per palette entry.
     h2d_bytes: bytes copied host -> device for the geometry."""
 
-    def __init__(self, native, slots, stats, light_args, builder=None, h2d_bytes=0, pal_texture=None):
+    def __init__(self, native, slots, stats, light_args, builder=None, h2d_bytes=0, pal_texture=None,
+                 light_index=None):
         self.native = native
         self.slots = slots
         self.stats = stats
         self.builder = builder
         self.h2d_bytes = int(h2d_bytes)
         self._light_args = light_args
+        self._light_index = light_index
         self.pal_texture = pal_texture
         self._lights_mode = None
 
@@ -236,7 +240,8 @@ class DeviceScene:
         compat = bool(compat)
         if self._lights_mode is compat:
             return
-        lights = build_lights(self.slots, *self._light_args, compat=compat, pal_texture=self.pal_texture)
+        lights = build_lights(self.slots, *self._light_args, compat=compat, pal_texture=self.pal_texture,
+                              tri_index=self._light_index)
         self.native.set_lights(lights)
         self._lights_mode = compat
 
@@ -292,7 +297,8 @@ def _extract_on_device(world, native, builder, textures):
     """Fill `native`'s triangle arrays with the world's triangles in the order
     and palette of collect() + GPUBVHBuilder.build, transforming IndexedMesh
     geometry on the device (rx_scene_put_indexed).  Returns (slots, triangle
-    count, emissive triangle rows, host->device bytes)."""
+    count, emissive triangle rows, host->device bytes, scene triangle index of
+    each emissive row)."""
     items, slots = _walk(world)
     # material records in visit order (this numbers the textures as the
     # reference does), then triangles: IndexedMesh first, Mesh after
@@ -306,7 +312,7 @@ def _extract_on_device(world, native, builder, textures):
                 mesh_batches.append(b)
     total = sum(g.triangle_count for _, g, _ in indexed) + sum(b.triangle_count for b in mesh_batches)
     native.alloc_triangles(total)
-    lv0, lv1, lv2, lmat = [], [], [], []
+    lv0, lv1, lv2, lmat, lidx = [], [], [], [], []
     off, h2d = 0, 0
     for obj, geo, recs in indexed:
         n = geo.triangle_count
@@ -339,6 +345,7 @@ def _extract_on_device(world, native, builder, textures):
             lv1.append(w[:, 1])
             lv2.append(w[:, 2])
             lmat.append(group_mat[gidx[sel]])
+            lidx.append(off + sel)
         off += n
     for b in mesh_batches:
         remap = np.array([builder._add_material(m) for m in b.mat_palette], np.int32)
@@ -355,10 +362,12 @@ def _extract_on_device(world, native, builder, textures):
             lv1.append(b.v1[rows])
             lv2.append(b.v2[rows])
             lmat.append(mat[rows])
+            lidx.append(off + rows)
         off += b.triangle_count
     cat3 = lambda xs: np.concatenate(xs) if xs else np.zeros((0, 3), np.float32)  # noqa: E731
     lights = (cat3(lv0), cat3(lv1), cat3(lv2), np.concatenate(lmat) if lmat else np.zeros(0, np.int32))
-    return slots, total, lights, h2d
+    light_index = np.concatenate(lidx).astype(np.int32) if lidx else np.zeros(0, np.int32)
+    return slots, total, lights, h2d, light_index
 
 
 def _upload_textures(native, builder, textures):
@@ -397,7 +406,7 @@ def build_device_scene(world, method="lbvh", leaf_size=None):
     leaf = 4 if leaf_size is None else int(leaf_size)
     native = nat.NativeScene()
     builder = GPUBVHBuilder()  # palette bookkeeping only
-    slots, total, light_tris, h2d = _extract_on_device(world, native, builder, textures)
+    slots, total, light_tris, h2d, light_index = _extract_on_device(world, native, builder, textures)
     native.set_objects(slot_arrays(slots) if slots else None)
     pal = builder.palette_arrays()
     native.set_materials(*pal)
@@ -409,7 +418,7 @@ def build_device_scene(world, method="lbvh", leaf_size=None):
     stats = {"primitive_count": len(slots), "bvh_nodes": n_nodes, "bvh_triangles": total,
              "bvh_materials": len(builder.mat_palette), "bvh_leaf_size": leaf if total else 0}
     return DeviceScene(native, slots, stats, light_tris + (pal[0], pal[1], pal[4]), h2d_bytes=h2d,
-                       pal_texture=builder.palette_textures())
+                       pal_texture=builder.palette_textures(), light_index=light_index)
 
 
 def extract_scene(world, method="lbvh"):

@@ -44,18 +44,21 @@ def _lum(rgb):
 
 
 def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, pal_emission, compat,
-                 pal_texture=None):
+                 pal_texture=None, tri_index=None):
     """Light arrays for rx_scene_set_lights.
 
     slots: reference object-slot dicts; tri_*: triangles in caller order with
     palette index tri_mat; compat: sphere lights only, uniform pick;
     pal_texture: texture index per palette entry — textured emitters are
-    left out (their radiance varies over the surface; BSDF rays find them).
+    left out (their radiance varies over the surface; BSDF rays find them);
+    tri_index: scene triangle index of each tri_* row (None: row i is
+    triangle i), reported as the triangle lights' sources.
     """
-    kinds, p0, p1, p2, alb, em, area = [], [], [], [], [], [], []
-    for s in slots:
+    kinds, p0, p1, p2, alb, em, area, src = [], [], [], [], [], [], [], []
+    for si, s in enumerate(slots):
         if s["type"] == 0 and s["mat_type"] == 3 and s["emission"] > 0.0:
             kinds.append(0)
+            src.append(si)
             p0.append(s["center"])
             p1.append([s["radius"], 0.0, 0.0])
             p2.append([0.0, 0.0, 0.0])
@@ -70,6 +73,7 @@ def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, p
     ALB = np.array(alb, np.float32).reshape((-1, 3))
     EM = np.array(em, np.float32)
     AREA = np.array(area, np.float32)
+    SRC = np.array(src, np.int32)
     if not compat and tri_mat is not None and len(tri_mat):
         pt = np.asarray(pal_type)[tri_mat]
         pe = np.asarray(pal_emission)[tri_mat]
@@ -88,6 +92,7 @@ def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, p
             ALB = np.concatenate([ALB, np.asarray(pal_albedo, np.float32)[tri_mat[sel]]])
             EM = np.concatenate([EM, pe[sel].astype(np.float32)])
             AREA = np.concatenate([AREA, tarea.astype(np.float32)])
+            SRC = np.concatenate([SRC, (sel if tri_index is None else np.asarray(tri_index)[sel]).astype(np.int32)])
     n = len(kind)
     if n == 0:
         return None
@@ -96,4 +101,5 @@ def build_lights(slots, tri_v0, tri_v1, tri_v2, tri_mat, pal_type, pal_albedo, p
     else:
         prob, alias, pdf = alias_table(_lum(ALB) * EM * AREA)
     return {"kind": kind, "p0": P0, "p1": P1, "p2": P2, "albedo": ALB, "emission": EM, "area": AREA,
-            "pick_pdf": pdf, "alias_prob": prob, "alias_idx": alias, "n_spheres": n_sph}
+            "pick_pdf": pdf, "alias_prob": prob, "alias_idx": alias, "n_spheres": n_sph,
+            "source": SRC}  # object slot (sphere lights) or caller triangle index (triangle lights)

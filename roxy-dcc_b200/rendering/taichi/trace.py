@@ -6,7 +6,8 @@ from rendering.taichi import fields
 
 
 def make_params(W, H, fov_tan, aspect, max_depth, use_sky, direct_light_mode, direct_light_max_depth, sample_clamp,
-                bg_color, cam_pos, cam_fwd, cam_right, cam_up, reference_compat=False, seed=0, wave_paths=0):
+                bg_color, cam_pos, cam_fwd, cam_right, cam_up, reference_compat=False, seed=0, wave_paths=0,
+                mis=False):
     p = nat.RenderParams()
     p.width, p.height = int(W), int(H)
     p.fov_tan, p.aspect = float(fov_tan), float(aspect)
@@ -20,6 +21,7 @@ def make_params(W, H, fov_tan, aspect, max_depth, use_sky, direct_light_mode, di
     p.direct_light_mode, p.direct_light_max_depth = int(direct_light_mode), int(direct_light_max_depth)
     p.sample_clamp = float(sample_clamp) if sample_clamp is not None else 0.0
     p.reference_compat, p.seed, p.wave_paths = int(bool(reference_compat)), int(seed) & 0xFFFFFFFF, int(wave_paths)
+    p.mis = int(bool(mis))
     return p
 
 

@@ -46,7 +46,7 @@ class RenderParams(ctypes.Structure):
         ("cam_up", ctypes.c_float * 3), ("max_depth", ctypes.c_int), ("use_sky", ctypes.c_int),
         ("bg", ctypes.c_float * 3), ("direct_light_mode", ctypes.c_int), ("direct_light_max_depth", ctypes.c_int),
         ("sample_clamp", ctypes.c_float), ("reference_compat", ctypes.c_int), ("seed", ctypes.c_uint32),
-        ("wave_paths", ctypes.c_int),
+        ("wave_paths", ctypes.c_int), ("mis", ctypes.c_int),
     ]
 
 
@@ -140,6 +140,7 @@ _SIGS = {
     "rx_scene_set_objects": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p] + [_f32p] * 4,
                              ctypes.c_int),
     "rx_scene_set_lights": ([ctypes.c_void_p, ctypes.c_int, _i32p] + [_f32p] * 8 + [_i32p], ctypes.c_int),
+    "rx_scene_set_light_sources": ([ctypes.c_void_p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_bvh_build": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "rx_bvh_set_reference": ([ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, _i32p, _i32p, _i32p, _i32p, _i32p],
                              ctypes.c_int),
@@ -437,6 +438,8 @@ class NativeScene:
             fptr(f32(lights["p2"], (-1, 3))), fptr(f32(lights["albedo"], (-1, 3))), fptr(f32(lights["emission"])),
             fptr(f32(lights["area"])), fptr(f32(lights["pick_pdf"])), fptr(f32(lights["alias_prob"])),
             iptr(i32(lights["alias_idx"]))))
+        if lights.get("source") is not None:
+            self.ctx.check(lib().rx_scene_set_light_sources(self.h, n, iptr(i32(lights["source"]))))
         self.n_lights = n
 
     def build_bvh(self, method=RX_BVH_LBVH_SAH, max_leaf=4, spheres_in_bvh=True):

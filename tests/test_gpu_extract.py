@@ -117,7 +117,8 @@ def test_device_extraction_equals_host_flattening(name):
     assert ds.stats["bvh_triangles"] == b.triangle_count
     assert ds.stats["bvh_materials"] == len(h.builder.mat_palette)
     for compat in (False, True):
-        a = build_lights(ds.slots, *ds._light_args, compat=compat, pal_texture=ds.pal_texture)
+        a = build_lights(ds.slots, *ds._light_args, compat=compat, pal_texture=ds.pal_texture,
+                         tri_index=ds._light_index)
         r = h.lights(compat)
         assert (a is None) == (r is None)
         if a is not None:

@@ -124,3 +124,41 @@ def test_denoise_edge_sizes():
         px = np.random.default_rng(H * 31 + W).random((H, W, 3), dtype=np.float32)
         out = edge_aware_denoise(px, radius=2, sigma_color=0.3, amount=1.0, passes=3)
         assert out.shape == px.shape and np.isfinite(out).all()
+
+
+def test_spheres_and_cubes_in_the_bvh_hit_as_the_linear_scan():
+    """Spheres and cubes as BVH leaves return the same t (bit for bit),
+    object slot and normal as the reference's linear object scan; planes
+    stay linear."""
+    ns = _ns()
+    rng = np.random.default_rng(4)
+    world = ns.World(use_sky=False, background_color=ns.Color(0.2, 0.2, 0.2))
+    world.add_camera(ns.Camera(position=ns.Vec3(0, 2, 9), forward=ns.Vec3(0, -0.2, -1), up=ns.Vec3(0, 1, 0),
+                               fov=50, width=64, height=64))
+    for i in range(300):
+        p = rng.uniform(-4, 4, 3)
+        shape = ns.Cube(float(rng.uniform(0.1, 0.6))) if i % 2 else ns.Sphere(float(rng.uniform(0.05, 0.4)))
+        world.add_object(ns.SceneObject(shape=shape, material=ns.Diffuse(ns.Color(0.5, 0.5, 0.5)),
+                                        translation=ns.Vec3(*map(float, p)), name=f"o{i}"))
+    world.add_object(ns.SceneObject(shape=ns.Plane(ns.Vec3(0, 1, 0), 4.5), material=ns.Diffuse(ns.Color(1, 1, 1)),
+                                    name="floor"))
+    ds = build_device_scene(world, method="lbvh")
+    n = 40000
+    ro = np.tile(np.array([[0.0, 2.0, 9.0]], np.float32), (n, 1)) + rng.normal(0, 0.3, (n, 3)).astype(np.float32)
+    rd = rng.normal(size=(n, 3)).astype(np.float32)
+    rd[:, 2] = -np.abs(rd[:, 2]) - 0.5
+    rd /= np.linalg.norm(rd, axis=1, keepdims=True)
+    ds.native.build_bvh(nat.RX_BVH_LBVH_SAH, 4, spheres_in_bvh=True)  # no triangles: built on request only
+    in_bvh = ds.native.intersect(ro, rd)
+    ds.native.build_bvh(nat.RX_BVH_LBVH_SAH, 4, spheres_in_bvh=False)
+    linear = ds.native.intersect(ro, rd)
+    hit = linear["kind"] != 0
+    assert hit.mean() > 0.5
+    assert np.array_equal(in_bvh["t"].view(np.uint32), linear["t"].view(np.uint32))
+    assert np.array_equal(in_bvh["id"][hit], linear["id"][hit])
+    assert np.array_equal(in_bvh["normal"][hit], linear["normal"][hit])
+    objs = linear["kind"] == 3
+    # 2: object in the BVH, 3: linear slot; only the plane (slot 300) stays linear
+    plane = objs & (linear["id"] == 300)
+    assert plane.any() and (objs & ~plane).any()
+    assert (in_bvh["kind"][objs & ~plane] == 2).all() and (in_bvh["kind"][plane] == 3).all()

@@ -307,6 +307,13 @@ def run_ours(args):
         quality = {"relmse": rel_mse(acc.read(nat.RX_ACC_RADIANCE), ref), "spp": w["spp"],
                    "ref_spp": args.ref_spp, "ref": "float64-accumulated render, independent seed, same clamp",
                    "ref_render_s": time.perf_counter() - t_ref}
+        # the same frame with power-heuristic MIS (not the timed estimator)
+        pm = nat.RenderParams.from_buffer_copy(params)
+        pm.mis = 1
+        acc_m = nat.Accumulator(W, H)
+        acc_m.render(ds.native, pm, w["spp"])
+        quality["relmse_mis"] = rel_mse(acc_m.read(nat.RX_ACC_RADIANCE), ref)
+        del acc_m
 
     # -- end to end through TaichiRenderer ------------------------------------
     img = Image(W, H)

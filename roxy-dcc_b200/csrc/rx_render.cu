@@ -28,7 +28,9 @@
 namespace rx {
 
 constexpr int kMaxBounce = 64;
-enum { C_Q = 0, C_FE = 64, C_FS = 128, C_S = 192, C_FC = 256, C_N = 320 };
+// counters, 64 per kind (one per bounce): queue lengths, extend fetch,
+// shade fetch, shadow record counts
+enum { C_Q = 0, C_FE = 64, C_FS = 128, C_S = 192, C_N = 256 };
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kTwoPi = 6.283185307179586f;
 
@@ -362,6 +364,38 @@ __global__ void k_generate_batch(BatchSrc src, int n_segs, long long total, floa
   if (blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)total;
 }
 
+// One extend item of shadow records: a path's shadow rays of one bounce sit
+// in consecutive records; the first carries their count (the others 0) and
+// this item traces them all, adding the visible contributions in light
+// order.  Only this item writes the path's radiance in this launch: no
+// atomics, and the sum does not depend on scheduling.  Returns the rays
+// traced; job = the path's job (batches).
+template <bool EXACT, class Src>
+__device__ __forceinline__ int shadow_item(const Src& src, const float4* __restrict__ shadow, long long j,
+                                           long long ns, float4* __restrict__ rad, int* err, int& job) {
+  const float4* sp = shadow + 3 * (size_t)j;
+  const int cnt = min(__float_as_int(sp[2].w), (int)(ns - j));
+  if (cnt <= 0) return 0;
+  const int p = __float_as_int(sp[1].w);
+  const int si = src.seg(p);
+  const DevScene S = src.scene(si);
+  if constexpr (Src::kBatch) job = src.segs[si].job;
+  float3 sum = f3(0.0f, 0.0f, 0.0f);
+  bool any = false;
+  for (int k = 0; k < cnt; ++k) {
+    float4 s0 = sp[3 * k], s1 = sp[3 * k + 1];
+    if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
+      sum = any ? sum + xyz(sp[3 * k + 2]) : xyz(sp[3 * k + 2]);
+      any = true;
+    }
+  }
+  if (any) {
+    float4 r = rad[p];
+    rad[p] = make_float4(r.x + sum.x, r.y + sum.y, r.z + sum.z, r.w);
+  }
+  return cnt;
+}
+
 template <bool EXACT, class Src, int BS>
 __global__ void __launch_bounds__(BS, Src::kBatch ? 1024 / BS : 1)
     k_extend(Src src, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
@@ -396,35 +430,7 @@ __global__ void __launch_bounds__(BS, Src::kBatch ? 1024 / BS : 1)
       int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
       hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
     } else if (i < total) {
-      // A path's shadow rays of one bounce sit in consecutive records; the
-      // first carries their count (the others 0) and this item traces them
-      // all, adding the visible contributions in light order.  Only this
-      // item writes the path's radiance in this launch: no atomics, and the
-      // sum does not depend on scheduling.
-      const float4* sp = shadow + 3 * (size_t)(i - n);
-      const int cnt = min(__float_as_int(sp[2].w), (int)(ns - (i - n)));
-      if (cnt > 0) {
-        const int p = __float_as_int(sp[1].w);
-        const int si = src.seg(p);
-        const DevScene S = src.scene(si);
-        if constexpr (Src::kBatch) {
-          job = src.segs[si].job;
-          rays_here = cnt;
-        }
-        float3 sum = f3(0.0f, 0.0f, 0.0f);
-        bool any = false;
-        for (int k = 0; k < cnt; ++k) {
-          float4 s0 = sp[3 * k], s1 = sp[3 * k + 1];
-          if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
-            sum = any ? sum + xyz(sp[3 * k + 2]) : xyz(sp[3 * k + 2]);
-            any = true;
-          }
-        }
-        if (any) {
-          float4 r = rad[p];
-          rad[p] = make_float4(r.x + sum.x, r.y + sum.y, r.z + sum.z, r.w);
-        }
-      }
+      rays_here = shadow_item<EXACT>(src, shadow, i - n, ns, rad, err, job);
     }
     if constexpr (Src::kBatch) {
       // rays traced, counted per job (lanes of a warp mostly share one)

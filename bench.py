@@ -32,8 +32,10 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-# paths per wavefront when rx_render_params.wave_paths is 0 (rx_render.cu)
-WAVE_PATHS = 1 << 25
+# paths per wavefront when rx_render_params.wave_paths is 0 (rx_render.cu
+# picks 2^27 on a B200: the largest size whose state fits in a quarter of
+# the free memory); used to count extend launches per step
+WAVE_PATHS = 1 << 27
 sys.path[:0] = [os.path.join(ROOT, "roxy-dcc_b200"), ROOT]
 
 import numpy as np  # noqa: E402

@@ -1100,9 +1100,23 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
   if (rc) return rc;
   // Paths per wavefront.  Each extend launch ends in a tail where the last,
   // longest rays run on an emptying GPU; larger waves amortise it (measured on
-  // the 1080p 64-spp icosphere scene: 16 M paths -> 43.7 ms of extend per
-  // frame, 32 M -> 35.8 ms).  32 M paths hold ~5.4 GB of path state.
-  long long target = p->wave_paths > 0 ? p->wave_paths : (1LL << 25);
+  // the 1080p 64-spp icosphere scene, extend / frame time: 16 M paths 43.7 /
+  // 58.2 ms, 32 M 35.1 / 47.6 ms, 64 M 30.7 / 42.7 ms, 128 M (the whole
+  // frame in one wave) 28.0 / 39.9 ms).  By default the wave is the largest
+  // power of two from 32 M to 128 M paths whose state (path SoA, queues,
+  // hit and shadow records: ~120 B + 48 B per shadow record slot) fits in a
+  // quarter of the free device memory; 128 M paths hold ~22 GB.
+  long long target = p->wave_paths;
+  if (target <= 0) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = 0;
+    }
+    const long long per_path = 120 + 48LL * (p->direct_light_mode == 1 ? std::max(sc->n_lights, 1) : 1);
+    target = 1LL << 27;
+    while (target > (1LL << 25) && (long long)(free_b / 4) < target * per_path) target >>= 1;
+  }
   int spf = (int)std::max<long long>(1, std::min<long long>(frames, target / std::max<long long>(a->P, 1)));
   long long cap = (long long)spf * a->P;
   if (cap >= (1LL << 31)) return set_error(ctx, "render: wavefront of %lld paths is too large", cap), RX_ERR_CAPACITY;

@@ -19,14 +19,19 @@ import roxy_native as nat
 from rendering.taichi.extractor import build_device_scene
 from rendering.taichi.trace import make_params
 
-WAVE_CANDIDATES = (1 << 22, 1 << 23, 1 << 24, 1 << 25)
+# Wave sizes: the one-frame probe holds fewer paths than these waves, so it
+# cannot rank them; larger waves amortise the tail of every extend launch
+# (the 1080p 64-spp single-scene frame: 32 M paths 47.6 ms, 128 M 39.9 ms),
+# so the default is one size, 128 M paths (~22 GB of wave state), and the
+# probe tunes the leaf size and the extend block.
+WAVE_CANDIDATES = (1 << 27,)
 BLOCK_CANDIDATES = (64, 128, 256)
 LEAF_CANDIDATES = (2, 4, 8)
 
 
 @dataclass
 class BatchConfig:
-    wave_paths: int = 1 << 25
+    wave_paths: int = 1 << 27
     extend_block: int = 128
     leaf_size: int = 4
 

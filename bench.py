@@ -233,16 +233,17 @@ def run_ours(args):
     params = _params(world, w, make_params)
     acc = nat.Accumulator(W, H, ctx)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", dev))
+    # Frames are queued back to back (asynchronous accumulator): the timed
+    # region holds no host round trip; the device error bits of all timed
+    # frames are checked by the ctx.sync() after it.
+    acc.set_async(True)
     for _ in range(args.warmup):
         acc.reset()
         acc.render(ds.native, params, w["spp"])
-    acc.set_timing(True)
-    rays0 = 0
-    kern = {"extend_ms": 0.0, "shade_ms": 0.0, "connect_ms": 0.0, "other_ms": 0.0}
+    ctx.sync()
     launches = 0
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    step_rays = []
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -252,17 +253,30 @@ def run_ours(args):
         for _ in range(args.steps):
             acc.reset()
             acc.render(ds.native, params, w["spp"])
-            tm = acc.last_timing()
-            for k in kern:
-                kern[k] += tm[k]
-            launches += tm["launches"]
-            step_rays.append(acc.info()["rays"])
+            launches += acc.last_timing()["launches"]
         ev1.record(stream)
         ev1.synchronize()
     ctx.sync()
     torch.cuda.synchronize(dev)
     ms = ev0.elapsed_time(ev1)
+    acc.set_async(False)
+    rays_timed = acc.info()["rays"]  # the last timed frame's
+    # Per-kernel split: the same frames again with CUDA events around every
+    # launch (untimed for the headline); each frame must trace exactly the
+    # rays the timed frames traced (same seeds, same frame base).
+    acc.set_timing(True)
+    kern = {"extend_ms": 0.0, "shade_ms": 0.0, "connect_ms": 0.0, "other_ms": 0.0}
+    step_rays = []
+    for _ in range(args.steps):
+        acc.reset()
+        acc.render(ds.native, params, w["spp"])
+        tm = acc.last_timing()
+        for k in kern:
+            kern[k] += tm[k]
+        step_rays.append(acc.info()["rays"])
     acc.set_timing(False)
+    if any(r != rays_timed for r in step_rays):
+        raise RuntimeError(f"frames traced different ray counts: {rays_timed} timed, {step_rays} split")
     total_rays = sum(step_rays)
     extend_rays = 0
     if dist:
@@ -357,7 +371,13 @@ def run_ours(args):
                              "note": "traversal is latency/L2 bound; frac is of measured HBM copy bandwidth",
                              "extend_ms_per_step": ext_ms, "extend_rays_per_step": ext_rays,
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
-                                       "algorithmic_bytes_per_ray": 272, "ms_per_step": shade_ms}},
+                                       "algorithmic_bytes_per_ray": 272, "ms_per_step": shade_ms},
+                             # the rest of a step: generate + accumulate (+ a
+                             # separate shadow launch); and the timed step
+                             # minus all kernel spans of the split pass (the
+                             # reset memsets and launch gaps)
+                             "other_ms_per_step": (kern["other_ms"] + kern["connect_ms"]) / max(args.steps, 1),
+                             "gap_ms_per_step": (ms - sum(kern.values())) / max(args.steps, 1)},
                 "clocks": clocks.summary(),
                 "quality": quality,
                 "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -736,7 +756,7 @@ def run_serve(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="icosphere",

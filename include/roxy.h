@@ -217,6 +217,14 @@ int rx_accum_info(rx_accum* acc, int* width, int* height, int* frames, long long
 int rx_accum_denoise(rx_accum* acc, const rx_denoise_params* params, float* host_out);
 /* Per-kernel CUDA-event timing of the next render calls (for profiling). */
 int rx_accum_set_timing(rx_accum* acc, int on);
+/* Asynchronous frames: with on != 0, rx_accum_reset and rx_render return once
+ * their work is queued on the context's stream instead of waiting for it,
+ * so back-to-back frames leave the GPU no idle gap.  Error bits the kernels
+ * raise (an overflow, a bounded wait that ran out) then surface at the next
+ * rx_ctx_sync; every call that copies to the host still waits.  Off by
+ * default (each render returns with its frames done and checked, as the
+ * reference's ti.sync() after render_kernel does, trace.py:282). */
+int rx_accum_set_async(rx_accum* acc, int on);
 /* ms of the last render, ms per kernel class (extend, shade, connect, other)
  * and the number of kernel launches it made. */
 int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches);

@@ -747,6 +747,12 @@ int rx_accum_set_timing(rx_accum* acc, int on) {
   return accum_set_timing(acc->a, on);
 }
 
+int rx_accum_set_async(rx_accum* acc, int on) {
+  if (!acc) return RX_ERR_ARG;
+  LOCK(acc->ctx);
+  return accum_set_async(acc->a, on);
+}
+
 int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches) {
   if (!acc) return RX_ERR_ARG;
   LOCK(acc->ctx);

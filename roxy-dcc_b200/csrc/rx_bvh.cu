@@ -567,6 +567,77 @@ __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int ncur, int o
   }
 }
 
+// 4-wide nodes from the laid-out binary tree, one level per launch: the
+// 4-wide node of binary node b holds b's children, an internal child
+// replaced by its own two children (so a leaf child stays a leaf and an
+// internal grandchild becomes a 4-wide node of the next level).  Empty
+// binary slots (count 0 leaves) are dropped; unused slots get a box at
+// 1e30 and count 0.
+__global__ void k_bvh4_level(const int* __restrict__ cur, int ncur, int* __restrict__ next,
+                             int* __restrict__ next_count, int next_base, int next_cap,
+                             const float4* __restrict__ bin, int n_bin, float4* __restrict__ out4, int out_base,
+                             int* err) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ncur; q += gridDim.x * blockDim.x) {
+    float mn[4][3], mx[4][3];
+    int wd[4], ct[4];
+    int k = 0;
+    auto add = [&](const float4* nb, int side) {
+      const float4 n0 = nb[0], n1 = nb[1], n2 = nb[2], n3 = nb[3];
+      const int w = __float_as_int(side ? n3.y : n3.x), c = __float_as_int(side ? n3.w : n3.z);
+      if (w < 0 && c == 0) return;  // empty slot
+      if (k >= 4) return;           // cannot happen: at most 2 x 2 children
+      if (side == 0) {
+        mn[k][0] = n0.x, mx[k][0] = n0.y, mn[k][1] = n0.z, mx[k][1] = n0.w, mn[k][2] = n1.x, mx[k][2] = n1.y;
+      } else {
+        mn[k][0] = n1.z, mx[k][0] = n1.w, mn[k][1] = n2.x, mx[k][1] = n2.y, mn[k][2] = n2.z, mx[k][2] = n2.w;
+      }
+      int word = w;
+      if (w >= 0) {  // an internal binary node becomes a 4-wide node of the next level
+        const int o = atomicAdd(next_count, 1);
+        if (o < next_cap) {
+          next[o] = w;
+          word = next_base + o;
+        } else {
+          atomicOr(err, ERR_BAD_NODE);
+          word = pack_leaf(0, 0);
+        }
+      }
+      wd[k] = word;
+      ct[k] = w >= 0 ? 0 : c;
+      ++k;
+    };
+    const int b = cur[q];
+    const float4* nb = bin + 4 * (size_t)b;
+    for (int side = 0; side < 2; ++side) {
+      const int w = __float_as_int(side ? nb[3].y : nb[3].x);
+      if (w >= 0 && w < n_bin) {
+        const float4* cb = bin + 4 * (size_t)w;
+        add(cb, 0);
+        add(cb, 1);
+      } else if (w < 0) {
+        add(nb, side);
+      } else {
+        atomicOr(err, ERR_BAD_NODE);
+      }
+    }
+    for (; k < 4; ++k) {
+      mn[k][0] = mn[k][1] = mn[k][2] = 1e30f;
+      mx[k][0] = mx[k][1] = mx[k][2] = 1e30f;
+      wd[k] = pack_leaf(0, 0);
+      ct[k] = 0;
+    }
+    float4* o = out4 + 8 * (size_t)(out_base + q);
+    o[0] = make_float4(mn[0][0], mn[1][0], mn[2][0], mn[3][0]);
+    o[1] = make_float4(mx[0][0], mx[1][0], mx[2][0], mx[3][0]);
+    o[2] = make_float4(mn[0][1], mn[1][1], mn[2][1], mn[3][1]);
+    o[3] = make_float4(mx[0][1], mx[1][1], mx[2][1], mx[3][1]);
+    o[4] = make_float4(mn[0][2], mn[1][2], mn[2][2], mn[3][2]);
+    o[5] = make_float4(mx[0][2], mx[1][2], mx[2][2], mx[3][2]);
+    o[6] = make_float4(__int_as_float(wd[0]), __int_as_float(wd[1]), __int_as_float(wd[2]), __int_as_float(wd[3]));
+    o[7] = make_float4(__int_as_float(ct[0]), __int_as_float(ct[1]), __int_as_float(ct[2]), __int_as_float(ct[3]));
+  }
+}
+
 // Root record for a tree that is a single leaf of `cnt` primitives.
 __global__ void k_single_leaf_root(const float3* __restrict__ bmin, const float3* __restrict__ bmax, int cnt,
                                    float4* __restrict__ out) {
@@ -725,6 +796,36 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
   return RX_OK;
 }
 
+// The 4-wide copy of the laid-out binary tree (k_bvh4_level, level by
+// level from the root, breadth first).
+static int build_wide(Ctx* ctx, Scene* sc) {
+  cudaStream_t st = ctx->stream;
+  const int nb = sc->n_nodes;
+  sc->n_nodes4 = 0;
+  if (nb <= 0) return RX_OK;
+  if (!sc->d_nodes4.alloc(ctx, (size_t)8 * nb)) return set_error(ctx, "out of device memory for the 4-wide BVH"), RX_ERR_CAPACITY;
+  DevBuf<int> la(ctx, nb), lb(ctx, nb), cnt(ctx, 1);
+  if (!la.p || !lb.p || !cnt.p) return set_error(ctx, "out of device memory"), RX_ERR_CAPACITY;
+  CUDA_TRY(ctx, cudaMemsetAsync(la.p, 0, sizeof(int), st));  // level 0: binary root 0
+  int ncur = 1, base = 0;
+  int* cur = la.p;
+  int* nxt = lb.p;
+  while (ncur > 0) {
+    if (base + ncur > nb) return set_error(ctx, "4-wide BVH: level walk did not terminate"), RX_ERR_DEVICE;
+    CUDA_TRY(ctx, cudaMemsetAsync(cnt.p, 0, sizeof(int), st));
+    k_bvh4_level<<<grid_for(ctx, ncur), 256, 0, st>>>(cur, ncur, nxt, cnt.p, base + ncur, nb - base - ncur,
+                                                       sc->d_nodes.p, nb, sc->d_nodes4.p, base, ctx->d_err);
+    int h = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    base += ncur;
+    ncur = h;
+    std::swap(cur, nxt);
+  }
+  sc->n_nodes4 = base;
+  return RX_OK;
+}
+
 int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t, float c_i) {
   cudaStream_t st = ctx->stream;
   sc->clear_bvh();
@@ -833,6 +934,7 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   }
   sc->order.swap(order);
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (int rc = build_wide(ctx, sc)) return rc;
   sc->root_min = hb[0];
   sc->root_max = hb[1];
   sc->n_prims = n;

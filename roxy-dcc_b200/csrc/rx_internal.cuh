@@ -100,6 +100,8 @@ struct TexInfo {
 struct DevScene {
   const float4* nodes;     // n_nodes * 4
   int n_nodes;
+  const float4* nodes4;    // n_nodes4 * 8: the same tree 4-wide (LBVH builds), or null
+  int n_nodes4;
   float3 root_min, root_max;
   const float4* prims;     // n_prims * 3
   const float4* shade;     // n_prims * 3
@@ -640,6 +642,114 @@ __device__ __forceinline__ int bvh_closest_wwt(const DevScene& S, float3 o, floa
   return hit;
 }
 
+// ------------------------------------------------------------ 4-wide BVH
+// Node of 8 float4 (128 B, two cache lines): the children's boxes as
+// (min x, max x, min y, max y, min z, max z) each over the four children,
+// then the child words (>= 0: 4-wide node, < 0: packed leaf) and the
+// children's primitive counts.  An empty slot has a box at 1e30 (never
+// entered) and count 0.  The 4-wide tree is the LBVH with every other level
+// pulled up (a node's children are its binary grandchildren, a leaf child
+// staying a leaf), so traversal needs about half the dependent node fetches.
+__device__ __forceinline__ void slab4(const float4 (&q)[8], float3 inv, float3 oinv, float tmax, float (&t)[4],
+                                      int (&w)[4]) {
+  const float mnx[4] = {q[0].x, q[0].y, q[0].z, q[0].w}, mxx[4] = {q[1].x, q[1].y, q[1].z, q[1].w};
+  const float mny[4] = {q[2].x, q[2].y, q[2].z, q[2].w}, mxy[4] = {q[3].x, q[3].y, q[3].z, q[3].w};
+  const float mnz[4] = {q[4].x, q[4].y, q[4].z, q[4].w}, mxz[4] = {q[5].x, q[5].y, q[5].z, q[5].w};
+  const int wd[4] = {__float_as_int(q[6].x), __float_as_int(q[6].y), __float_as_int(q[6].z), __float_as_int(q[6].w)};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float x0 = __fmaf_rn(mnx[i], inv.x, -oinv.x), x1 = __fmaf_rn(mxx[i], inv.x, -oinv.x);
+    const float y0 = __fmaf_rn(mny[i], inv.y, -oinv.y), y1 = __fmaf_rn(mxy[i], inv.y, -oinv.y);
+    const float z0 = __fmaf_rn(mnz[i], inv.z, -oinv.z), z1 = __fmaf_rn(mxz[i], inv.z, -oinv.z);
+    const float te = fmaxf(fminf(x0, x1), fmaxf(fminf(y0, y1), fminf(z0, z1)));
+    const float tx = fminf(fmaxf(x0, x1), fminf(fmaxf(y0, y1), fmaxf(z0, z1)));
+    const bool h = tx >= te && tx >= 0.001f && te <= tmax;
+    t[i] = h ? te : INFINITY;
+    w[i] = wd[i];
+  }
+}
+
+__device__ __forceinline__ void cswap(float (&t)[4], int (&w)[4], int a, int b) {
+  if (t[b] < t[a]) {
+    float tt = t[a];
+    t[a] = t[b];
+    t[b] = tt;
+    int ww = w[a];
+    w[a] = w[b];
+    w[b] = ww;
+  }
+}
+
+// Closest hit on the 4-wide tree: children entered nearest first (sorting
+// network on entry distance), farther ones stacked with their distance and
+// skipped on pop once the current hit is closer.  Returns the same closest
+// primitive as the binary traversal (up to the order among exactly equal
+// hit distances).
+__device__ __forceinline__ int bvh4_closest(const DevScene& S, float3 o, float3 d, float& tmax, float& hu, float& hv,
+                                            int* err) {
+  int stk_w[kStack];
+  float stk_t[kStack];
+  int sp = 0;
+  const float3 inv = make_inv_dir(d);
+  const float3 oinv = o * inv;
+  int hit = -1;
+  float te;
+  if (S.n_nodes4 <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
+  int word = 0;
+  float wt = te;
+  int guard = 4 * S.n_nodes4 + 64;
+  for (;;) {
+    if (wt <= tmax) {
+      if (--guard < 0 || word >= S.n_nodes4) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return hit;
+      }
+      if (word >= 0) {
+        const float4* np = S.nodes4 + 8 * (size_t)word;
+        float4 q[8];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) q[k] = __ldg(np + k);
+        float t[4];
+        int w[4];
+        slab4(q, inv, oinv, tmax, t, w);
+        cswap(t, w, 0, 1);
+        cswap(t, w, 2, 3);
+        cswap(t, w, 0, 2);
+        cswap(t, w, 1, 3);
+        cswap(t, w, 1, 2);
+        if (t[0] < INFINITY) {
+#pragma unroll
+          for (int k = 3; k >= 1; --k)
+            if (t[k] < INFINITY) {
+              if (sp < kStack) {
+                stk_w[sp] = w[k];
+                stk_t[sp] = t[k];
+                ++sp;
+              } else if (err) {
+                atomicOr(err, ERR_STACK_OVERFLOW);
+              }
+            }
+          word = w[0];
+          wt = t[0];
+          continue;
+        }
+      } else {
+        const int first = leaf_first(word), cnt = leaf_count(word);
+        if (first + cnt > S.n_prims) {
+          if (err) atomicOr(err, ERR_BAD_NODE);
+          return hit;
+        }
+        leaf_closest(S, o, d, first, cnt, tmax, hu, hv, hit);
+      }
+    }
+    if (sp == 0) break;
+    --sp;
+    word = stk_w[sp];
+    wt = stk_t[sp];
+  }
+  return hit;
+}
+
 #ifndef RX_TRAV
 #define RX_TRAV 0
 #endif
@@ -647,6 +757,9 @@ __device__ __forceinline__ int bvh_closest_wwt(const DevScene& S, float3 o, floa
 template <bool EXACT>
 __device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d, float& tmax, float& hu, float& hv,
                                            int* err) {
+  if constexpr (!EXACT) {
+    if (S.nodes4) return bvh4_closest(S, o, d, tmax, hu, hv, err);
+  }
 #if RX_TRAV == 1
   return bvh_closest_ww<EXACT>(S, o, d, tmax, hu, hv, err);
 #elif RX_TRAV == 2
@@ -656,9 +769,79 @@ __device__ __forceinline__ int bvh_closest(const DevScene& S, float3 o, float3 d
 #endif
 }
 
+// Any hit before max_t on the 4-wide tree: every entered child is visited
+// (nearest first, the rest stacked) until the first primitive hit.
+__device__ __forceinline__ bool bvh4_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
+  int stack[kStack];
+  int sp = 0;
+  const float3 inv = make_inv_dir(d);
+  const float3 oinv = o * inv;
+  float te;
+  if (S.n_nodes4 <= 0 || !slab1(S.root_min, S.root_max, o, inv, max_t, te)) return false;
+  int word = 0;
+  int guard = 4 * S.n_nodes4 + 64;
+  for (;;) {
+    if (--guard < 0 || word >= S.n_nodes4) {
+      if (err) atomicOr(err, ERR_BAD_NODE);
+      return false;
+    }
+    if (word >= 0) {
+      const float4* np = S.nodes4 + 8 * (size_t)word;
+      float4 q[8];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) q[k] = __ldg(np + k);
+      float t[4];
+      int w[4];
+      slab4(q, inv, oinv, max_t, t, w);
+      int next = 0;
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (t[k] < INFINITY) {
+          if (!any) {
+            next = w[k];
+            any = true;
+          } else if (sp < kStack) {
+            stack[sp++] = w[k];
+          } else if (err) {
+            atomicOr(err, ERR_STACK_OVERFLOW);
+          }
+        }
+      if (any) {
+        word = next;
+        continue;
+      }
+    } else {
+      const int first = leaf_first(word), cnt = leaf_count(word);
+      if (first + cnt > S.n_prims) {
+        if (err) atomicOr(err, ERR_BAD_NODE);
+        return false;
+      }
+      for (int k = first; k < first + cnt; ++k) {
+        const float4* pp = S.prims + 3 * (size_t)k;
+        float4 a = __ldg(pp);
+        float t, u, v;
+        if (__float_as_int(a.w) == PRIM_TRI) {
+          float4 b = __ldg(pp + 1), c = __ldg(pp + 2);
+          if (tri_hit(o, d, a, b, c, max_t, t, u, v)) return true;
+        } else {
+          float4 b = __ldg(pp + 1);
+          t = analytic_t(o, d, a, b);
+          if (0.001f < t && t < max_t) return true;
+        }
+      }
+    }
+    if (sp == 0) return false;
+    word = stack[--sp];
+  }
+}
+
 // Any hit before max_t (intersect.py:155-219): stops at the first hit.
 template <bool EXACT>
 __device__ __forceinline__ bool bvh_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
+  if constexpr (!EXACT) {
+    if (S.nodes4) return bvh4_any(S, o, d, max_t, err);
+  }
   int stack[kStack];
   int sp = 0;
   stack[0] = kSentinel;

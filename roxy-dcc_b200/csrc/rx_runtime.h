@@ -115,6 +115,8 @@ struct Scene {
   // traversal structure
   DevBuf<float4> d_nodes, d_prims, d_shade;
   int n_nodes = 0, n_prims = 0, n_bvh_spheres = 0;  // n_bvh_spheres: spheres and cubes in the BVH
+  DevBuf<float4> d_nodes4;  // the LBVH 4-wide (8 float4 per node); traversal uses it when present
+  int n_nodes4 = 0;
   float3 root_min = {0, 0, 0}, root_max = {0, 0, 0};
   int method = -1, exact_slab = 0, leaf_size = 0, depth = 0;
   // reference-format copy (reference builder / uploaded trees)
@@ -134,7 +136,8 @@ struct Scene {
     order.release();
     ref_min.release();
     ref_max.release();
-    n_nodes = n_prims = n_bvh_spheres = 0;
+    d_nodes4.release();
+    n_nodes = n_prims = n_bvh_spheres = n_nodes4 = 0;
     depth = 0;
     method = -1;
     ++version;
@@ -145,6 +148,8 @@ struct Scene {
     DevScene s;
     s.nodes = d_nodes.p;
     s.n_nodes = n_nodes;
+    s.nodes4 = n_nodes4 > 0 ? d_nodes4.p : nullptr;
+    s.n_nodes4 = n_nodes4;
     s.root_min = root_min;
     s.root_max = root_max;
     s.prims = d_prims.p;
@@ -214,6 +219,7 @@ int accum_read(Accum* a, int which, float* host_out);
 int accum_info(Accum* a, int* w, int* h, int* frames, long long* rays);
 int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out);
 int accum_set_timing(Accum* a, int on);
+int accum_set_async(Accum* a, int on);
 int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
 int accum_set_f64(Accum* a, int on);
 int accum_read_f64(Accum* a, double* host_out);

@@ -268,6 +268,31 @@ def test_progressive_accumulation_equals_one_shot():
     assert a.info()["rays"] == b.info()["rays"] and b.info()["frames"] == 12
 
 
+def test_async_frames_equal_synchronous_frames():
+    """An asynchronous accumulator queues reset + render without waiting;
+    after a context sync its running means and ray count are bit-identical
+    to the synchronous ones, resets included."""
+    world = workloads.cornell_box(48, 32)
+    ds = build_device_scene(world)
+    ds.use_lights(False)
+    cam = world.active_camera
+    p = make_params(48, 32, math.tan(math.radians(cam.fov) / 2), 1.5, 8, 0, 0, 8, 10.0, [0, 0, 0],
+                    list(cam.position), list(cam.forward), list(cam.right), list(cam.up), seed=3)
+    a = nat.Accumulator(48, 32)
+    a.render(ds.native, p, 8)
+    b = nat.Accumulator(48, 32)
+    b.set_async(True)
+    b.render(ds.native, p, 5)
+    b.reset()
+    for k in (3, 5):
+        b.render(ds.native, p, k)
+    b.ctx.sync()
+    b.set_async(False)
+    np.testing.assert_array_equal(a.read(nat.RX_ACC_RADIANCE), b.read(nat.RX_ACC_RADIANCE))
+    np.testing.assert_array_equal(a.read(nat.RX_ACC_DISPLAY), b.read(nat.RX_ACC_DISPLAY))
+    assert a.info()["rays"] == b.info()["rays"] and b.info()["frames"] == 8
+
+
 def test_float64_reference_accumulation_and_relmse():
     """float64 sums agree with the float32 running means, a float64 render
     keeps its f32 outputs unchanged, and relMSE falls roughly as 1/spp."""

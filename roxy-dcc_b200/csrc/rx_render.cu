@@ -46,6 +46,7 @@ struct RenderK {
   float clamp;
   int compat;
   int mis;  // power-heuristic MIS between NEE and BSDF hits of listed lights
+  int camera0;  // bounce 0 makes its camera rays in place (no k_generate)
   uint32_t seed;
   long long shadow_cap;
   long long queue_cap;
@@ -251,6 +252,24 @@ struct JobAcc {
   unsigned long long* rays;
 };
 
+// Queue position s of a frame -> pixel: 4-row strips walked column by
+// column, so a warp covers an 8 x 4 tile.
+__device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& px, int& py) {
+  long long strip = s / (4LL * K.W);
+  long long r = s - strip * 4LL * K.W;
+  int hs = min(4, K.H - (int)(4 * strip));
+  px = (int)(r / hs);
+  py = (int)(4 * strip + r % hs);
+}
+
+// Bounce-0 queue position t of a wave -> path index, pixel and frame of the
+// wave: frames outer, then strip order inside a frame.
+__device__ __forceinline__ long long camera_path(const RenderK& K, long long t, int& px, int& py, int& f) {
+  f = (int)(t / K.P);
+  strip_pixel(K, t - (long long)f * K.P, px, py);
+  return (long long)f * K.P + (long long)py * K.W + px;
+}
+
 struct SingleSrc {
   static constexpr bool kBatch = false;
   DevScene S;
@@ -262,6 +281,21 @@ struct SingleSrc {
   __device__ __forceinline__ void locate(int, long long p, int fb, uint32_t& pix, uint32_t& smp) const {
     pix = (uint32_t)(p % K.P);
     smp = (uint32_t)(fb + (int)(p / K.P));
+  }
+  // With K.camera0, bounce 0 has no queue: its items are the wave's camera
+  // paths in k_generate's order, and k_extend / k_shade make each camera ray
+  // where they need it instead of reading the state k_generate would write.
+  const int* fbase = nullptr;  // the accumulator's frame base
+  __device__ __forceinline__ long long camera_items(int b) const {
+    return b == 0 && K.camera0 ? (long long)K.spf * K.P : 0;
+  }
+  __device__ __forceinline__ int frame0() const { return *fbase; }
+  __device__ __forceinline__ int camera_ray(long long t, int fb, float3& o, float3& d) const {
+    int px, py, f;
+    const long long p = camera_path(K, t, px, py, f);
+    o = K.cam_pos;
+    d = camera_dir(K, px, py, fb + f);
+    return (int)p;
   }
 };
 
@@ -289,6 +323,10 @@ struct BatchSrc {
     pix = (uint32_t)(l % g.P);
     smp = (uint32_t)(fb + (int)(l / g.P));
   }
+  // batches keep k_generate_batch's queue and path state at bounce 0
+  __device__ __forceinline__ long long camera_items(int) const { return 0; }
+  __device__ __forceinline__ int frame0() const { return 0; }
+  __device__ __forceinline__ int camera_ray(long long, int, float3&, float3&) const { return 0; }
 };
 
 // -------------------------------------------------------------------- kernels
@@ -306,16 +344,6 @@ __device__ __forceinline__ void init_path(const RenderK& K, int px, int py, int 
   ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// Queue position s of a frame -> pixel: 4-row strips walked column by
-// column, so a warp covers an 8 x 4 tile.
-__device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& px, int& py) {
-  long long strip = s / (4LL * K.W);
-  long long r = s - strip * 4LL * K.W;
-  int hs = min(4, K.H - (int)(4 * strip));
-  px = (int)(r / hs);
-  py = (int)(4 * strip + r % hs);
-}
-
 __global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4* __restrict__ ray_o,
                            float4* __restrict__ ray_d, float4* __restrict__ thr, float4* __restrict__ rad,
                            float4* __restrict__ gn, float4* __restrict__ ga, int* __restrict__ q0,
@@ -324,11 +352,8 @@ __global__ void k_generate(RenderK K, const int* __restrict__ frame_base, float4
   int fb = *frame_base;
   long long stride = (long long)gridDim.x * blockDim.x;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
-    int f = (int)(t / K.P);
-    long long s = t - (long long)f * K.P;
-    int px, py;
-    strip_pixel(K, s, px, py);
-    long long p = (long long)f * K.P + (long long)py * K.W + px;
+    int px, py, f;
+    const long long p = camera_path(K, t, px, py, f);
     init_path(K, px, py, fb + f, p, ray_o, ray_d, thr, rad, gn, ga);
     q0[t] = (int)p;
   }
@@ -404,7 +429,9 @@ __device__ __forceinline__ int shadow_item(const Src& src, const float4* __restr
 
 // 1024 resident threads per SM (64 registers): traversal is latency bound,
 // and the extra warps hide more of it than the registers they cost.
-template <bool EXACT, class Src, int BS>
+// CAM: the bounce-0 launch of a single render (camera items, no shadow
+// rays); the other launches are compiled without that code.
+template <bool EXACT, class Src, int BS, bool CAM = false>
 __global__ void __launch_bounds__(BS, 1024 / BS)
     k_extend(Src src, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
              const float4* __restrict__ ray_d, float4* __restrict__ hits, int sb, const float4* __restrict__ shadow,
@@ -412,7 +439,12 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
   // Items [0, n): closest hit of bounce b's queue.  Items [n, n + ns): the
   // shadow rays bounce sb (the previous one) emitted, traced any-hit here so
   // they share this launch instead of paying for a small one of their own.
-  const int n = b >= 0 ? *(volatile int*)&counters[C_Q + b] : 0;
+  // Camera items (bounce 0 without k_generate): item i is camera path i of
+  // the wave, its ray made here; this launch also sets the bounce-0 count.
+  const long long cam_n = CAM ? src.camera_items(b) : 0;
+  const int fb = cam_n ? src.frame0() : 0;
+  if (cam_n && blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)cam_n;
+  const int n = cam_n ? (int)cam_n : (b >= 0 ? *(volatile int*)&counters[C_Q + b] : 0);
   long long ns = sb >= 0 ? *(volatile int*)&counters[C_S + sb] : 0;
   if (ns > shadow_cap) ns = shadow_cap;
   const int total = n + (int)ns;
@@ -426,19 +458,27 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
     int i = base + lane;
     int job = -1, rays_here = 0;
     if (i < n) {
-      int p = qin[i];
+      float3 o, d;
+      int p;
+      if (cam_n) {
+        p = src.camera_ray(i, fb, o, d);
+      } else {
+        p = qin[i];
+        o = xyz(ray_o[p]);
+        d = xyz(ray_d[p]);
+      }
       const int si = src.seg(p);
       const DevScene S = src.scene(si);
       if constexpr (Src::kBatch) {
         job = src.segs[si].job;
         rays_here = 1;
       }
-      float4 o = ray_o[p], d = ray_d[p];
-      SceneHit h = scene_closest<EXACT>(S, xyz(o), xyz(d), err);
+      SceneHit h = scene_closest<EXACT>(S, o, d, err);
       int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
       hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
     } else if (i < total) {
-      rays_here = shadow_item<EXACT>(src, shadow, i - n, ns, rad, err, job);
+      // (no shadow rays precede bounce 0)
+      if constexpr (!CAM) rays_here = shadow_item<EXACT>(src, shadow, i - n, ns, rad, err, job);
     }
     if constexpr (Src::kBatch) {
       // rays traced, counted per job (lanes of a warp mostly share one)
@@ -485,7 +525,10 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
                                                float4* __restrict__ rad_b, float4* __restrict__ gn,
                                                float4* __restrict__ ga, const float4* __restrict__ hits,
                                                float4* __restrict__ shadow, int* err) {
-  const int n = *(volatile int*)&counters[C_Q + b];
+  // camera items: bounce 0 without k_generate (see k_extend); the path's
+  // state is the camera ray, unit throughput and no radiance yet
+  const long long cam_n = src.camera_items(b);
+  const int n = cam_n ? (int)cam_n : *(volatile int*)&counters[C_Q + b];
   const int fb = frame_base ? *frame_base : 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
@@ -496,7 +539,7 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
     int i = base + lane;
     bool valid = i < n;
     // lanes past the end take the first item's job (they write nothing)
-    const int si = src.seg(qin[valid ? i : base]);
+    const int si = src.seg(cam_n ? 0 : qin[valid ? i : base]);
     const DevScene S = src.scene(si);
     const RenderK K = src.params(si);
     // MIS needs the emitter -> light maps (rx_scene_set_light_sources)
@@ -509,9 +552,20 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
     float3 hit_p = f3(0, 0, 0), nrm = f3(0, 0, 1), alb = f3(0, 0, 0), thr_nee = f3(0, 0, 0);
     PathRng rng;
     if (valid) {
-      p = qin[i];
+      float4 o4, d4, t4;
+      if (cam_n) {
+        float3 co, cd;
+        p = src.camera_ray(i, fb, co, cd);
+        o4 = make_float4(co.x, co.y, co.z, 1.0f);
+        d4 = make_float4(cd.x, cd.y, cd.z, 0.0f);
+        t4 = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+      } else {
+        p = qin[i];
+        o4 = ray_o[p];
+        d4 = ray_d[p];
+        t4 = thr_b[p];
+      }
       float4 h = hits[i];
-      float4 o4 = ray_o[p], d4 = ray_d[p], t4 = thr_b[p];
       float3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
       float cur_ior = o4.w;
       bool prev_nee = d4.w != 0.0f;
@@ -532,6 +586,10 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
         }
         add = thr * sky;
         has_add = true;
+        if (cam_n) {  // no first hit: empty guides
+          gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
       } else {
         float t = h.x;
         float3 nn;
@@ -663,7 +721,9 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
           }
         }
       }
-      if (has_add) {
+      if (cam_n) {
+        rad_b[p] = make_float4(add.x, add.y, add.z, 0.0f);  // the path's first radiance
+      } else if (has_add) {
         float4 r = rad_b[p];
         rad_b[p] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, 0.0f);
       }
@@ -974,6 +1034,9 @@ static RenderK make_k(const rx_render_params* p, const Accum* a, int spf, long l
   K.clamp = p->sample_clamp;
   K.compat = p->reference_compat;
   K.mis = p->reference_compat ? 0 : p->mis;
+  // single renders make bounce 0's camera rays in place (batches and
+  // zero-bounce renders run k_generate)
+  K.camera0 = p->max_depth > 0 ? 1 : 0;
   K.seed = p->seed;
   K.shadow_cap = shadow_cap;
   K.queue_cap = a->cap;
@@ -989,15 +1052,19 @@ static int blocks_for(Ctx* ctx, const void* fn, int block) {
 
 static void launch_extend(Accum* a, const DevScene& S, const RenderK& K, int b, const int* qin, int sb) {
   Ctx* ctx = a->ctx;
-  SingleSrc src{S, K};
-  if (S.exact_slab)
-    k_extend<true, SingleSrc, 128><<<a->occ_ext, 128, 0, ctx->stream>>>(
-        src, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
-        ctx->d_err);
-  else
-    k_extend<false, SingleSrc, 128><<<a->occ_ext, 128, 0, ctx->stream>>>(
-        src, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p, sb, a->shadow.p, a->rad.p, K.shadow_cap,
-        ctx->d_err);
+  SingleSrc src{S, K, a->frame_base.p};
+  auto go = [&](auto kernel) {
+    kernel<<<a->occ_ext, 128, 0, ctx->stream>>>(src, b, qin, a->counters.p, a->ray_o.p, a->ray_d.p, a->hits.p, sb,
+                                                 a->shadow.p, a->rad.p, K.shadow_cap, ctx->d_err);
+  };
+  const bool cam = b == 0 && K.camera0;
+  if (S.exact_slab) {
+    if (cam) go(k_extend<true, SingleSrc, 128, true>);
+    else go(k_extend<true, SingleSrc, 128>);
+  } else {
+    if (cam) go(k_extend<false, SingleSrc, 128, true>);
+    else go(k_extend<false, SingleSrc, 128>);
+  }
 }
 
 // Records the launch sequence of one wave on the context stream.  With
@@ -1018,11 +1085,13 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   };
   mark(K_OTHER);
   cudaMemsetAsync(a->counters.p, 0, sizeof(int) * C_N, st);
-  long long total = (long long)K.spf * K.P;
-  int gblocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
-  k_generate<<<std::max(gblocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p,
-                                                    a->gn.p, a->ga.p, a->q0.p, a->counters.p);
-  ++launches;
+  if (!K.camera0) {
+    long long total = (long long)K.spf * K.P;
+    int gblocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
+    k_generate<<<std::max(gblocks, 1), 256, 0, st>>>(K, a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p,
+                                                      a->rad.p, a->gn.p, a->ga.p, a->q0.p, a->counters.p);
+    ++launches;
+  }
   mark(K_OTHER);
   for (int b = 0; b < K.max_depth; ++b) {
     const int* qin = (b & 1) ? a->q1.p : a->q0.p;
@@ -1032,7 +1101,7 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
     launch_extend(a, S, K, b, qin, sb);
     ++launches;
     mark(K_EXTEND);
-    k_shade<SingleSrc><<<a->occ_shade, 128, 0, st>>>(SingleSrc{S, K}, b, qin, qout, a->counters.p,
+    k_shade<SingleSrc><<<a->occ_shade, 128, 0, st>>>(SingleSrc{S, K, a->frame_base.p}, b, qin, qout, a->counters.p,
                                                       a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p,
                                                       a->gn.p, a->ga.p, a->hits.p, a->shadow.p, ctx->d_err);
     ++launches;
@@ -1552,6 +1621,7 @@ int batch_render(Batch* B) {
     const BatchJob& J = B->jobs[j];
     scenes[j] = J.sc->view();
     ks[j] = make_k(&J.p, J.acc, 0, B->shadow_cap);
+    ks[j].camera0 = 0;
     ks[j].queue_cap = B->cap;
     Accum* a = J.acc;
     accs[j] = JobAcc{a->acc_r.p, a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p, a->frame_base.p, a->rays.p};

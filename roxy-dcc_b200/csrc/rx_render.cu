@@ -845,19 +845,18 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
                                                  const JobAcc& A) {
   float4 a = A.acc_r[pix], an = A.acc_n[pix], aa = A.acc_a[pix];
   double sx = 0.0, sy = 0.0, sz = 0.0;
-  for (int f = 0; f < spf; ++f) {
-    long long p = path0 + (long long)f * P + pix;
-    float4 s = rad[p];
+  const bool f64 = A.acc64 != nullptr;
+  auto fold = [&](float4 s, float4 g, float4 al, int frame) {
     if (clamp > 0.0f) {
       s.x = fminf(fmaxf(s.x, 0.0f), clamp);
       s.y = fminf(fmaxf(s.y, 0.0f), clamp);
       s.z = fminf(fmaxf(s.z, 0.0f), clamp);
     }
-    sx += (double)s.x;
-    sy += (double)s.y;
-    sz += (double)s.z;
-    float4 g = gn[p], al = ga[p];
-    int frame = fb + f;
+    if (f64) {
+      sx += (double)s.x;
+      sy += (double)s.y;
+      sz += (double)s.z;
+    }
     if (frame == 0) {
       a = make_float4(s.x, s.y, s.z, 0.0f);
       an = g;
@@ -868,6 +867,26 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
       an = make_float4((an.x * F + g.x) / F1, (an.y * F + g.y) / F1, (an.z * F + g.z) / F1, (an.w * F + g.w) / F1);
       aa = make_float4((aa.x * F + al.x) / F1, (aa.y * F + al.y) / F1, (aa.z * F + al.z) / F1, 0.0f);
     }
+  };
+  // the wave's samples are read once: streaming loads, kU frames in flight
+  // per thread ahead of the (sequential) running-mean updates
+  constexpr int kU = 4;
+  int f = 0;
+  for (; f + kU <= spf; f += kU) {
+    float4 s[kU], g[kU], al[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const long long p = path0 + (long long)(f + u) * P + pix;
+      s[u] = __ldcs(rad + p);
+      g[u] = __ldcs(gn + p);
+      al[u] = __ldcs(ga + p);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) fold(s[u], g[u], al[u], fb + f + u);
+  }
+  for (; f < spf; ++f) {
+    const long long p = path0 + (long long)f * P + pix;
+    fold(__ldcs(rad + p), __ldcs(gn + p), __ldcs(ga + p), fb + f);
   }
   A.acc_r[pix] = a;
   A.acc_n[pix] = an;

@@ -335,7 +335,8 @@ def run_ours(args):
     img = Image(W, H)
     r = TaichiRenderer(world, img, None, samples=w["spp"], max_depth=w["max_depth"],
                        direct_light_max_depth=w["dlmd"])
-    r.render()  # warm
+    r.render()  # warm: wave buffers, graph
+    r.render()
     e2e_times, e2e_rays = [], []
     for _ in range(max(1, min(args.steps, 3))):
         ctx.sync()

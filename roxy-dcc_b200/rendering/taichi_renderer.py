@@ -22,6 +22,8 @@ GPU), so `last_ray_count` does not depend on core.timing.LEVEL.
 import math
 import time
 
+import numpy as np
+
 import roxy_native as nat
 from rendering.render_stats import RenderStats
 from rendering.taichi import fields
@@ -85,7 +87,11 @@ class TaichiRenderer:
                                   1)
             self._image.pixels[:] = acc.denoise(p)
         else:
-            self._image.pixels[:] = acc.read(nat.RX_ACC_DISPLAY)
+            px = self._image.pixels
+            if px.dtype == np.float32 and px.flags["C_CONTIGUOUS"]:
+                acc.read(nat.RX_ACC_DISPLAY, out=px)  # straight into the image
+            else:
+                px[:] = acc.read(nat.RX_ACC_DISPLAY)
 
     def render(self):
         W, H = self._image.width, self._image.height

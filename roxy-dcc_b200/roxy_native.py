@@ -579,9 +579,15 @@ class Accumulator:
     def render(self, scene, params, frames):
         self.ctx.check(lib().rx_render(scene.h, self.h, ctypes.byref(params), int(frames)))
 
-    def read(self, which):
+    def read(self, which, out=None):
+        """One accumulator plane as float32 (H, W) or (H, W, 3); with `out`
+        (C-contiguous float32 of that shape, e.g. an Image's pixels) the
+        device copy lands in it directly, with no new host array."""
         shape = (self.height, self.width) if which == RX_ACC_DEPTH else (self.height, self.width, 3)
-        out = np.zeros(shape, np.float32)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"read: out must be a C-contiguous float32 array of shape {shape}")
         self.ctx.check(lib().rx_accum_read(self.h, int(which), fptr(out)))
         return out
 

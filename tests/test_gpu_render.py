@@ -291,6 +291,12 @@ def test_async_frames_equal_synchronous_frames():
     np.testing.assert_array_equal(a.read(nat.RX_ACC_RADIANCE), b.read(nat.RX_ACC_RADIANCE))
     np.testing.assert_array_equal(a.read(nat.RX_ACC_DISPLAY), b.read(nat.RX_ACC_DISPLAY))
     assert a.info()["rays"] == b.info()["rays"] and b.info()["frames"] == 8
+    # a read into a caller's buffer (the renderer reads into its Image)
+    out = np.full((32, 48, 3), -1.0, np.float32)
+    assert b.read(nat.RX_ACC_DISPLAY, out=out) is out
+    np.testing.assert_array_equal(out, a.read(nat.RX_ACC_DISPLAY))
+    with pytest.raises(ValueError, match="C-contiguous float32"):
+        b.read(nat.RX_ACC_DISPLAY, out=np.zeros((32, 48, 3), np.float64))
 
 
 def test_float64_reference_accumulation_and_relmse():

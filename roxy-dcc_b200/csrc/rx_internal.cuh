@@ -793,19 +793,23 @@ __device__ __forceinline__ bool bvh4_any(const DevScene& S, float3 o, float3 d, 
       float t[4];
       int w[4];
       slab4(q, inv, oinv, max_t, t, w);
+      cswap(t, w, 0, 1);
+      cswap(t, w, 2, 3);
+      cswap(t, w, 0, 2);
+      cswap(t, w, 1, 3);
+      cswap(t, w, 1, 2);
       int next = 0;
       bool any = false;
+      // nearest next, the others stacked farthest first
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 3; k >= 0; --k)
         if (t[k] < INFINITY) {
-          if (!any) {
-            next = w[k];
-            any = true;
-          } else if (sp < kStack) {
-            stack[sp++] = w[k];
-          } else if (err) {
-            atomicOr(err, ERR_STACK_OVERFLOW);
+          if (any) {
+            if (sp < kStack) stack[sp++] = next;
+            else if (err) atomicOr(err, ERR_STACK_OVERFLOW);
           }
+          next = w[k];
+          any = true;
         }
       if (any) {
         word = next;

@@ -298,11 +298,20 @@ def run_ours(args):
     # the device; shadow rays are at most one per diffuse bounce below dlmd
     stats = _ray_split(ds, acc, params, w)
     ext_rays = stats["extend_rays"]
-    ext_gbs = 40.0 * ext_rays / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
-    shade_gbs = 272.0 * ext_rays / (shade_ms / 1e3) / 1e9 if shade_ms > 0 else 0.0
-    # DRAM bytes per k_extend launch: ncu's bytes per ray (committed summary,
-    # measured on the profiling case of this scene) times the average rays
-    # per launch here (max_depth launches per wave)
+    # algorithmic bytes of the closest-hit items: 40 B per ray (origin and
+    # direction in, hit record out), 16 B for a camera ray, which bounce 0
+    # makes in the kernel (only its hit record is written)
+    cam_rays = W * H * w["spp"]
+    ext_bytes = 40.0 * max(ext_rays - cam_rays, 0) + 16.0 * min(cam_rays, ext_rays)
+    ext_gbs = ext_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
+    # k_shade: 272 B per ray, less the 48 B of ray state a camera ray does
+    # not read at bounce 0
+    shade_bytes = 272.0 * ext_rays - 48.0 * min(cam_rays, ext_rays)
+    shade_gbs = shade_bytes / (shade_ms / 1e3) / 1e9 if shade_ms > 0 else 0.0
+    # DRAM bytes per k_extend launch: ncu's DRAM bytes per closest-hit ray
+    # (committed summary: one-pass DRAM counters over the 12 extend launches
+    # of this frame) times the average rays per launch here (max_depth
+    # launches per wave)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic_extend.json")
     spf = max(1, min(w["spp"], WAVE_PATHS // (W * H)))
@@ -368,11 +377,12 @@ def run_ours(args):
                 "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
                              "achieved": ext_gbs, "peak": peak, "unit": "GB/s", "frac": ext_gbs / peak,
                              "traffic": traffic, "peak_source": peak_kind,
-                             "algorithmic_bytes_per_ray": 40,
+                             "algorithmic_bytes_per_ray": ext_bytes / max(ext_rays, 1),
                              "note": "traversal is latency/L2 bound; frac is of measured HBM copy bandwidth",
                              "extend_ms_per_step": ext_ms, "extend_rays_per_step": ext_rays,
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
-                                       "algorithmic_bytes_per_ray": 272, "ms_per_step": shade_ms},
+                                       "algorithmic_bytes_per_ray": shade_bytes / max(ext_rays, 1),
+                                       "ms_per_step": shade_ms},
                              # the rest of a step: generate + accumulate (+ a
                              # separate shadow launch); and the timed step
                              # minus all kernel spans of the split pass (the

@@ -378,7 +378,7 @@ def run_ours(args):
                              "achieved": ext_gbs, "peak": peak, "unit": "GB/s", "frac": ext_gbs / peak,
                              "traffic": traffic, "peak_source": peak_kind,
                              "algorithmic_bytes_per_ray": ext_bytes / max(ext_rays, 1),
-                             "note": "traversal is latency/L2 bound; frac is of measured HBM copy bandwidth",
+                             "note": f"traversal is latency/L2 bound; frac is of the {peak_kind} HBM copy bandwidth",
                              "extend_ms_per_step": ext_ms, "extend_rays_per_step": ext_rays,
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
                                        "algorithmic_bytes_per_ray": shade_bytes / max(ext_rays, 1),

@@ -309,7 +309,8 @@ struct BatchSrc {
   unsigned long long* job_rays;  // rays traced per job in this wave
   __device__ __forceinline__ int seg(long long p) const { return __ldg(pseg + p); }
   // Batches traverse the binary tree: with the 4-wide traversal inlined as
-  // well, the kernels spill at 64 registers and ran 7% slower (64 scenes).
+  // well, the kernels spill at 64 registers and ran 7% slower (64 scenes),
+  // and 7% slower as well at 80 registers with 768 threads per SM.
   __device__ __forceinline__ DevScene scene(int si) const {
     DevScene s = scenes[segs[si].job];
     s.nodes4 = nullptr;

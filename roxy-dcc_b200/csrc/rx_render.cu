@@ -1299,12 +1299,29 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
       bool cached = a->gexec && a->g_scene == sc && a->g_ver == sc->version && a->g_spf == spf &&
                     a->g_timed == timed && std::memcmp(&a->g_params, p, sizeof(*p)) == 0;
       if (!cached) {
-        a->drop_graph();
         cudaGraph_t g;
         CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         enqueue_wave(a, sc, K, timed, &nlaunch);
         CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
-        CUDA_TRY(ctx, cudaGraphInstantiate(&a->gexec, g, 0));
+        // same launch sequence with new arguments (another scene, other
+        // parameters): update the executable graph in place, else rebuild it
+        bool updated = false;
+        if (a->gexec) {
+          cudaGraphExecUpdateResultInfo info;
+          updated = cudaGraphExecUpdate(a->gexec, g, &info) == cudaSuccess;
+          if (!updated) {
+            cudaGetLastError();
+            a->drop_graph();
+          }
+        }
+        if (!updated) {
+          cudaError_t e = cudaGraphInstantiate(&a->gexec, g, 0);
+          if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            a->gexec = nullptr;
+            CUDA_TRY(ctx, e);
+          }
+        }
         cudaGraphDestroy(g);
         a->g_scene = sc;
         a->g_ver = sc->version;

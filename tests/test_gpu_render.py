@@ -299,6 +299,35 @@ def test_async_frames_equal_synchronous_frames():
         b.read(nat.RX_ACC_DISPLAY, out=np.zeros((32, 48, 3), np.float64))
 
 
+def test_reused_accumulator_across_scenes_and_parameters():
+    """One accumulator alternating between two scenes and two seeds (its
+    wave graph is updated in place with the new arguments) gives the same
+    images as fresh accumulators."""
+    W = H = 32
+    worlds = [workloads.cornell_box(W, H), gs.build_trace_scene(_ns())]
+    scenes = []
+    for world in worlds:
+        ds = build_device_scene(world)
+        ds.use_lights(False)
+        scenes.append((world, ds))
+
+    def params(world, seed):
+        cam = world.active_camera
+        return make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 6, world._use_sky, 0, 6,
+                           10.0, list(world._background_color), list(cam.position), list(cam.forward),
+                           list(cam.right), list(cam.up), seed=seed)
+
+    shared = nat.Accumulator(W, H)
+    for k, (world, ds) in enumerate(scenes * 2):
+        p = params(world, 11 + k)
+        shared.reset()
+        shared.render(ds.native, p, 4)
+        fresh = nat.Accumulator(W, H)
+        fresh.render(ds.native, p, 4)
+        np.testing.assert_array_equal(shared.read(nat.RX_ACC_RADIANCE), fresh.read(nat.RX_ACC_RADIANCE))
+        assert shared.info()["rays"] == fresh.info()["rays"]
+
+
 def test_float64_reference_accumulation_and_relmse():
     """float64 sums agree with the float32 running means, a float64 render
     keeps its f32 outputs unchanged, and relMSE falls roughly as 1/spp."""

@@ -43,8 +43,9 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "icosphere": dict(width=1920, height=1080, spp=64, max_depth=12, dlmd=1,
                       desc="displaced icosphere 327,680 tris + 64 spheres, 1920x1080, 64 spp, depth 12"),
-    "cornell": dict(width=256, height=256, spp=16, max_depth=8, dlmd=8,
-                    desc="Cornell box 36 tris, 256x256, 16 spp, depth 8, NEE every bounce"),
+    "cornell": dict(width=256, height=256, spp=16, max_depth=8, dlmd=8, denoise_passes=5,
+                    desc="Cornell box 36 tris, 256x256, 16 spp, depth 8, NEE every bounce, "
+                         "then the 5-pass a-trous denoise"),
     # same scene at 640x360 / 16 spp: the kernel-profiling case (same kernels,
     # one wave of 3.7M paths, < 1 GB on the device)
     "icosphere-small": dict(width=640, height=360, spp=16, max_depth=12, dlmd=1,
@@ -133,7 +134,8 @@ def _peaks():
 
 
 def cpu_baseline(wname, world, seconds_target=15.0, rows=None, spp=None):
-    """Oracle (C++/OpenMP) on a bounded row band of the workload."""
+    """Oracle (C++/OpenMP) on a row-stratified sample of the workload: bands of
+    rows spaced evenly over the frame, spp sized to a bounded CPU time."""
     from oracle import oracle
     from rendering.taichi.extractor import HostScene, slot_arrays
     w = WORKLOADS[wname]
@@ -154,23 +156,45 @@ def cpu_baseline(wname, world, seconds_target=15.0, rows=None, spp=None):
                            int(world._use_sky), list(world._background_color), direct_light_mode=0,
                            direct_light_max_depth=w["dlmd"], sample_clamp=10.0, reference_compat=0, seed=0)
     cores = os.cpu_count() or 1
-    # calibrate: one spp on a small band, then size the sample to ~seconds_target
-    y0 = w["height"] // 2 - 8
+    H = w["height"]
+    # calibrate on 8 rows at 1 spp spread over the frame, then size the
+    # sample to ~seconds_target: `bands` bands of rows spaced evenly from top
+    # to bottom (row-stratified, so sky, mesh and spheres enter in the
+    # frame's own proportions), each band's rows contiguous
+    bands = min(16, H)
     t0 = time.perf_counter()
-    rays = oracle.render(sc, p, 1, rows=(y0, y0 + 16), n_threads=cores)["rays"]
-    dt = max(time.perf_counter() - t0, 1e-3)
+    for k in range(8):
+        y = (2 * k + 1) * H // 16
+        oracle.render(sc, p, 1, rows=(y, y + 1), n_threads=cores)
+    per_row_spp = max(time.perf_counter() - t0, 1e-3) / 8.0
+    fixed = rows is not None
     if rows is None:
-        per_row_spp = dt / 16.0
         budget_rows_spp = seconds_target / per_row_spp
-        spp = spp or max(1, min(w["spp"], int(budget_rows_spp // 32) or 1))
-        rows = int(max(16, min(w["height"], budget_rows_spp / spp)))
-    y0 = max(0, w["height"] // 2 - rows // 2)
-    t0 = time.perf_counter()
-    rays = oracle.render(sc, p, spp, rows=(y0, y0 + rows), n_threads=cores)["rays"]
-    dt = time.perf_counter() - t0
+        spp = spp or max(1, min(w["spp"], int(budget_rows_spp // (4 * bands)) or 1))
+        rows = int(max(bands, min(H, budget_rows_spp / spp)))
+    for _ in range(4):
+        rows = max(bands, min(H, rows))
+        per_band = rows // bands
+        starts = [max(0, min(H - per_band, (2 * k + 1) * H // (2 * bands) - per_band // 2)) for k in range(bands)]
+        rays, dt = 0, 0.0
+        for y0 in starts:
+            t0 = time.perf_counter()
+            rays += oracle.render(sc, p, spp, rows=(y0, y0 + per_band), n_threads=cores)["rays"]
+            dt += time.perf_counter() - t0
+        # the calibration rows carry per-call overhead: grow the sample
+        # (rows first, then spp) until it takes about seconds_target
+        if fixed or dt >= 0.6 * seconds_target or (rows >= H and spp >= w["spp"]):
+            break
+        grow = min(8.0, seconds_target / max(dt, 1e-3))
+        if rows < H:
+            rows = int(min(H, rows * grow))
+        else:
+            spp = int(min(w["spp"], max(spp + 1, spp * grow)))
+    rows = per_band * bands
     return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": cores, "kind": "port",
-            "sample": f"{w['width']}x{rows} rows of the frame, {spp} spp, depth {w['max_depth']} "
-                      f"({rays} rays in {dt:.2f} s)", "seconds": dt, "rays": rays}
+            "sample": f"{bands} bands of {per_band} rows spaced evenly over the {w['width']}x{H} frame "
+                      f"({rows} rows), {spp} spp, depth {w['max_depth']} ({rays} rays in {dt:.2f} s)",
+            "seconds": dt, "rays": rays}
 
 
 def run_reference(args):
@@ -237,9 +261,17 @@ def run_ours(args):
     # region holds no host round trip; the device error bits of all timed
     # frames are checked by the ctx.sync() after it.
     acc.set_async(True)
-    for _ in range(args.warmup):
+    dn_passes = w.get("denoise_passes", 0)
+    dn_params = nat.DenoiseParams(1, max(dn_passes, 5), 0.08, 0.35, 0.20, 1.0, 0.8, 1, 1, 1, 1)
+
+    def step():
         acc.reset()
         acc.render(ds.native, params, w["spp"])
+        if dn_passes:
+            acc.denoise(dn_params, out=False)
+
+    for _ in range(args.warmup):
+        step()
     ctx.sync()
     launches = 0
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -251,9 +283,8 @@ def run_ours(args):
     with ClockSampler(dev) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            acc.reset()
-            acc.render(ds.native, params, w["spp"])
-            launches += acc.last_timing()["launches"]
+            step()
+            launches += acc.last_timing()["launches"] + dn_passes
         ev1.record(stream)
         ev1.synchronize()
     ctx.sync()
@@ -265,7 +296,7 @@ def run_ours(args):
     # launch (untimed for the headline); each frame must trace exactly the
     # rays the timed frames traced (same seeds, same frame base).
     acc.set_timing(True)
-    kern = {"extend_ms": 0.0, "shade_ms": 0.0, "connect_ms": 0.0, "other_ms": 0.0}
+    kern = {"extend_ms": 0.0, "shade_ms": 0.0, "connect_ms": 0.0, "other_ms": 0.0, "accumulate_ms": 0.0}
     step_rays = []
     for _ in range(args.steps):
         acc.reset()
@@ -323,6 +354,14 @@ def run_ours(args):
         except (OSError, ValueError, KeyError):
             traffic = None
 
+    # k_accumulate: one launch folds the wave's frames; per pixel it reads
+    # each frame's sample radiance and first-hit guides (3 x 16 B) and reads
+    # (3 x 16 B) and writes (4 x 16 B, display included) the running means
+    acc_ms = kern["accumulate_ms"] / max(args.steps, 1)
+    acc_bytes = W * H * (48.0 * w["spp"] + 112.0)
+    acc_gbs = acc_bytes / (acc_ms / 1e3) / 1e9 if acc_ms > 0 else 0.0
+    atrous = _atrous_roofline(nat, acc, stream, dn_params, W, H, peak, dev)
+
     # -- image error of the timed render against a float64 high-spp render ------
     quality = None
     if args.ref_spp > 0:
@@ -343,7 +382,8 @@ def run_ours(args):
     # -- end to end through TaichiRenderer ------------------------------------
     img = Image(W, H)
     r = TaichiRenderer(world, img, None, samples=w["spp"], max_depth=w["max_depth"],
-                       direct_light_max_depth=w["dlmd"])
+                       direct_light_max_depth=w["dlmd"], denoise=bool(dn_passes),
+                       denoise_passes=max(dn_passes, 1))
     r.render()  # warm: wave buffers, graph
     r.render()
     e2e_times, e2e_rays = [], []
@@ -383,6 +423,10 @@ def run_ours(args):
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
                                        "algorithmic_bytes_per_ray": shade_bytes / max(ext_rays, 1),
                                        "ms_per_step": shade_ms},
+                             "accumulate": {"achieved": acc_gbs, "frac": acc_gbs / peak, "ms_per_step": acc_ms,
+                                            "algorithmic_bytes_per_step": acc_bytes,
+                                            "bytes": "per pixel 48 B x spp sample reads + 112 B running means"},
+                             "atrous": atrous,
                              # the rest of a step: generate + accumulate (+ a
                              # separate shadow launch); and the timed step
                              # minus all kernel spans of the split pass (the
@@ -392,13 +436,42 @@ def run_ours(args):
                 "clocks": clocks.summary(),
                 "quality": quality,
                 "e2e": {"value": e2e_val, "unit": "Mrays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "path": "TaichiRenderer.render(): extract + H2D + GPU BVH build + render + D2H image"},
+                        "path": "TaichiRenderer.render(): extract + H2D + GPU BVH build + render"
+                                + (f" + {dn_passes}-pass a-trous" if dn_passes else "") + " + D2H image"},
                 "cpu_baseline": cb and {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}}
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _atrous_roofline(nat, acc, stream, dp, W, H, peak, dev, iters=10):
+    """The edge-aware a-trous filter (all guides, radius 1, dp.passes passes)
+    on the resident accumulators, each call timed alone with CUDA events on
+    the library stream after a 256 MB write that evicts L2.  Algorithmic
+    bytes: 52 B per pixel per pass (colour 12 + normal 12 + albedo 12 +
+    depth 4 read, 12 written)."""
+    import torch
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(iters + 3):
+            flush.fill_(float(i))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            acc.denoise(dp, out=False)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= 3:
+                times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    alg = 52.0 * W * H * dp.passes
+    gbs = alg / (ms / 1e3) / 1e9
+    return {"achieved": gbs, "frac": gbs / peak, "ms": ms, "passes": dp.passes, "pixels": W * H,
+            "ms_per_pass": ms / dp.passes, "algorithmic_bytes": alg,
+            "layout_bytes_per_pixel_pass": 64, "l2": "flushed (256 MB write) before each timed call"}
 
 
 def _ray_split(ds, acc, params, w):

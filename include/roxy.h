@@ -225,8 +225,9 @@ int rx_accum_set_timing(rx_accum* acc, int on);
  * default (each render returns with its frames done and checked, as the
  * reference's ti.sync() after render_kernel does, trace.py:282). */
 int rx_accum_set_async(rx_accum* acc, int on);
-/* ms of the last render, ms per kernel class (extend, shade, connect, other)
- * and the number of kernel launches it made. */
+/* ms of the last render, ms per kernel class (extend, shade, connect, other,
+ * accumulate; n_kernels <= 5 of them) and the number of kernel launches it
+ * made. */
 int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
 /* Float64 sums of the clamped sample radiance next to the float32 running
  * means, for high-spp reference renders (no reference counterpart: the
@@ -419,11 +420,14 @@ int rx_obj_end(rx_obj* o);
  * library, which limits height * width to 1,048,576 pixels (larger sizes
  * return RX_ERR_CAPACITY).  Buffers are float4 per pixel: colour (rgb, -),
  * normal guide (xyz, depth), albedo guide (rgb, -), output (rgb, 0); guides
- * are used as params->use_normal / use_albedo / use_depth say.  Runs on
- * `stream` (a cudaStream_t, NULL = legacy default stream) of the current
- * device; the first call on a device looks the array up and should come
- * before any stream capture.  Calls that can overlap on the GPU share the
- * array and race; the caller orders them.  Errors: rx_last_error(NULL). */
+ * are used as params->use_normal / use_albedo / use_depth say (a guide not in
+ * use may be NULL).  d_out must not overlap the colour or a guide in use
+ * (RX_ERR_ARG).  Runs on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) in the CUDA context current on the calling thread; the first call
+ * in a context (per device, and again after cudaDeviceReset or in a caller's
+ * own driver-API context) looks the array up and should come before any
+ * stream capture.  Calls that can overlap on the GPU share the array and
+ * race; the caller orders them.  Errors: rx_last_error(NULL). */
 int rx_denoise_noalloc(int height, int width, const float* d_color, const float* d_guide_normal,
                        const float* d_guide_albedo, const rx_denoise_params* params, float* d_out, void* stream);
 

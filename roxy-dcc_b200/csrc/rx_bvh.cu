@@ -239,12 +239,13 @@ __global__ void __launch_bounds__(kSortWarps * 32)
 }
 
 // Sorts (codes, idx) in place by the low `bits` bits of the key; stable.
-static void radix_sort(Ctx* ctx, int n, uint32_t* keys, int* vals, int bits) {
-  if (n <= 1) return;
+static int radix_sort(Ctx* ctx, int n, uint32_t* keys, int* vals, int bits) {
+  if (n <= 1) return RX_OK;
   cudaStream_t st = ctx->stream;
   int nblocks = (n + kSortTile - 1) / kSortTile;
   DevBuf<uint32_t> k2(ctx, n), hist(ctx, (size_t)256 * nblocks);
   DevBuf<int> v2(ctx, n);
+  if (!all_ok(k2, hist, v2)) return set_error(ctx, "BVH sort: out of device memory"), RX_ERR_CAPACITY;
   uint32_t* ka = keys;
   uint32_t* kb = k2.p;
   int* va = vals;
@@ -263,6 +264,7 @@ static void radix_sort(Ctx* ctx, int n, uint32_t* keys, int* vals, int bits) {
     cudaMemcpyAsync(vals, va, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
   }
   // k2, v2, hist are released after the stream drains (DevBuf defers frees)
+  return RX_OK;
 }
 
 // ----------------------------------------------------------------------------
@@ -670,20 +672,23 @@ static int grid_for(Ctx* ctx, long long n, int block = 256) {
 }
 
 // Shared front end: bounds, centroids, Morton codes, stable sort.
-static void front_end(Ctx* ctx, Scene* sc, int n_obj, const float4* d_obj_a, const float4* d_obj_b,
-                      DevBuf<float3>& pmin, DevBuf<float3>& pmax, DevBuf<int>& order) {
+static int front_end(Ctx* ctx, Scene* sc, int n_obj, const float4* d_obj_a, const float4* d_obj_b,
+                     DevBuf<float3>& pmin, DevBuf<float3>& pmax, DevBuf<int>& order) {
   int n = sc->n_tris + n_obj;
   cudaStream_t st = ctx->stream;
   DevBuf<float3> cen(ctx, n);
+  const int parts = std::min(grid_for(ctx, n), 1024);
+  DevBuf<float3> part_min(ctx, parts), part_max(ctx, parts);
+  DevBuf<uint32_t> codes(ctx, n);
+  if (!all_ok(pmin, pmax, order, cen, part_min, part_max, codes))
+    return set_error(ctx, "BVH build: out of device memory"), RX_ERR_CAPACITY;
   k_prim_bounds<<<grid_for(ctx, n), 256, 0, st>>>(sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, n_obj, d_obj_a, d_obj_b,
                                                    pmin.p, pmax.p, cen.p);
-  int parts = std::min(grid_for(ctx, n), 1024);
-  DevBuf<float3> part_min(ctx, parts), part_max(ctx, parts);
   k_reduce_bounds<<<parts, 256, 0, st>>>(n, cen.p, part_min.p, part_max.p);
-  DevBuf<uint32_t> codes(ctx, n);
   k_morton<<<grid_for(ctx, n), 256, 0, st>>>(n, cen.p, part_min.p, part_max.p, parts, codes.p, order.p);
-  radix_sort(ctx, n, codes.p, order.p, 30);
+  if (int rc = radix_sort(ctx, n, codes.p, order.p, 30)) return rc;
   sc->tmp_codes.swap(codes);
+  return RX_OK;
 }
 
 int build_reference(Ctx* ctx, Scene* sc, int leaf) {
@@ -693,7 +698,7 @@ int build_reference(Ctx* ctx, Scene* sc, int leaf) {
   if (n <= 0) return RX_OK;
   DevBuf<float3> pmin(ctx, n), pmax(ctx, n);
   DevBuf<int> order(ctx, n);
-  front_end(ctx, sc, 0, nullptr, nullptr, pmin, pmax, order);
+  if (int rc = front_end(ctx, sc, 0, nullptr, nullptr, pmin, pmax, order)) return rc;
   long long n_nodes_ll = 2 * median_tree_leaves(n, leaf) - 1;
   int n_nodes = (int)n_nodes_ll;
   DevBuf<int> left(ctx, n_nodes), right(ctx, n_nodes), tstart(ctx, n_nodes), tcount(ctx, n_nodes);
@@ -701,6 +706,8 @@ int build_reference(Ctx* ctx, Scene* sc, int leaf) {
   DevBuf<float3> nmin(ctx, n_nodes), nmax(ctx, n_nodes);
   DevBuf<RefNodeItem> la(ctx, n_nodes), lb(ctx, n_nodes);
   DevBuf<int> cnt(ctx, 1);
+  if (!all_ok(left, right, tstart, tcount, parent, flags, nmin, nmax, la, lb, cnt))
+    return set_error(ctx, "reference build: out of device memory"), RX_ERR_CAPACITY;
   RefNodeItem root{0, 0, n, -1};
   cudaMemcpyAsync(la.p, &root, sizeof(root), cudaMemcpyHostToDevice, st);
   int ncur = 1;
@@ -723,10 +730,14 @@ int build_reference(Ctx* ctx, Scene* sc, int leaf) {
   k_ref_bounds<<<grid_for(ctx, n_nodes), 256, 0, st>>>(n_nodes, left.p, right.p, tstart.p, tcount.p, parent.p,
                                                         order.p, pmin.p, pmax.p, nmin.p, nmax.p, flags.p);
   sc->d_nodes.alloc(ctx, (size_t)4 * n_nodes);
-  k_ref_to_layout<<<grid_for(ctx, n_nodes), 256, 0, st>>>(n_nodes, left.p, right.p, tstart.p, tcount.p, nmin.p,
-                                                           nmax.p, sc->d_nodes.p);
   sc->d_prims.alloc(ctx, (size_t)3 * n);
   sc->d_shade.alloc(ctx, (size_t)3 * n);
+  if (!all_ok(sc->d_nodes, sc->d_prims, sc->d_shade)) {
+    sc->clear_bvh();
+    return set_error(ctx, "reference build: out of device memory"), RX_ERR_CAPACITY;
+  }
+  k_ref_to_layout<<<grid_for(ctx, n_nodes), 256, 0, st>>>(n_nodes, left.p, right.p, tstart.p, tcount.p, nmin.p,
+                                                           nmax.p, sc->d_nodes.p);
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, order.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
                                                     sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr, nullptr,
                                                     sc->d_prims.p, sc->d_shade.p);
@@ -762,6 +773,13 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
   if (n <= 0 || n_nodes <= 0) return RX_OK;
   DevBuf<int> l(ctx, n_nodes), r(ctx, n_nodes), s(ctx, n_nodes), c(ctx, n_nodes), ord(ctx, n);
   DevBuf<float3> nmin(ctx, n_nodes), nmax(ctx, n_nodes);
+  sc->d_nodes.alloc(ctx, (size_t)4 * n_nodes);
+  sc->d_prims.alloc(ctx, (size_t)3 * n);
+  sc->d_shade.alloc(ctx, (size_t)3 * n);
+  if (!all_ok(l, r, s, c, ord, nmin, nmax, sc->d_nodes, sc->d_prims, sc->d_shade)) {
+    sc->clear_bvh();
+    return set_error(ctx, "BVH upload: out of device memory"), RX_ERR_CAPACITY;
+  }
   cudaMemcpyAsync(l.p, left, sizeof(int) * n_nodes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(r.p, right, sizeof(int) * n_nodes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s.p, start, sizeof(int) * n_nodes, cudaMemcpyHostToDevice, st);
@@ -769,11 +787,8 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
   cudaMemcpyAsync(nmin.p, node_min, sizeof(float3) * n_nodes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(nmax.p, node_max, sizeof(float3) * n_nodes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(ord.p, order, sizeof(int) * n, cudaMemcpyHostToDevice, st);
-  sc->d_nodes.alloc(ctx, (size_t)4 * n_nodes);
   k_ref_to_layout<<<grid_for(ctx, n_nodes), 256, 0, st>>>(n_nodes, l.p, r.p, s.p, c.p, nmin.p, nmax.p,
                                                            sc->d_nodes.p);
-  sc->d_prims.alloc(ctx, (size_t)3 * n);
-  sc->d_shade.alloc(ctx, (size_t)3 * n);
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, ord.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
                                                     sc->d_n1, sc->d_n2, sc->d_tri_mat, nullptr, nullptr, nullptr, nullptr,
                                                     sc->d_prims.p, sc->d_shade.p);
@@ -857,6 +872,7 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   if (n <= 0) return RX_OK;
   DevBuf<float4> d_oa(ctx, std::max(n_obj, 1)), d_ob(ctx, std::max(n_obj, 1));
   DevBuf<int> d_obj_mat(ctx, std::max(n_obj, 1)), d_obj_slot(ctx, std::max(n_obj, 1));
+  if (!all_ok(d_oa, d_ob, d_obj_mat, d_obj_slot)) return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
   if (n_obj) {
     cudaMemcpyAsync(d_oa.p, oa.data(), sizeof(float4) * n_obj, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_ob.p, ob.data(), sizeof(float4) * n_obj, cudaMemcpyHostToDevice, st);
@@ -865,17 +881,25 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   }
   DevBuf<float3> pmin(ctx, n), pmax(ctx, n);
   DevBuf<int> order(ctx, n);
-  front_end(ctx, sc, n_obj, d_oa.p, d_ob.p, pmin, pmax, order);
+  if (int rc = front_end(ctx, sc, n_obj, d_oa.p, d_ob.p, pmin, pmax, order)) return rc;
   sc->d_prims.alloc(ctx, (size_t)3 * n);
   sc->d_shade.alloc(ctx, (size_t)3 * n);
+  DevBuf<float3> rb(ctx, 2);
+  if (!all_ok(sc->d_prims, sc->d_shade, rb)) {
+    sc->clear_bvh();
+    return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+  }
   k_gather_prims<<<grid_for(ctx, n), 256, 0, st>>>(n, order.p, sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, sc->d_n0,
                                                     sc->d_n1, sc->d_n2, sc->d_tri_mat, d_oa.p, d_ob.p, d_obj_mat.p,
                                                     d_obj_slot.p, sc->d_prims.p, sc->d_shade.p);
-  DevBuf<float3> rb(ctx, 2);
   {
     // root box = union of all primitive boxes (two-stage parallel reduction)
     int parts = std::min(grid_for(ctx, n), 1024);
     DevBuf<float3> lo_min(ctx, parts), lo_max(ctx, parts), hi_min(ctx, parts), hi_max(ctx, parts);
+    if (!all_ok(lo_min, lo_max, hi_min, hi_max)) {
+      sc->clear_bvh();
+      return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+    }
     k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmin.p, lo_min.p, lo_max.p);
     k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmax.p, hi_min.p, hi_max.p);
     k_box_finish<<<1, 1, 0, st>>>(parts, lo_min.p, hi_max.p, rb.p);
@@ -884,7 +908,10 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   cudaMemcpyAsync(hb, rb.p, sizeof(hb), cudaMemcpyDeviceToHost, st);
   int n_int = n - 1;
   if (n == 1) {
-    sc->d_nodes.alloc(ctx, 4);
+    if (!sc->d_nodes.alloc(ctx, 4)) {
+      sc->clear_bvh();
+      return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+    }
     k_single_leaf_root<<<1, 1, 0, st>>>(rb.p, rb.p + 1, 1, sc->d_nodes.p);
     sc->n_nodes = 1;
   } else {
@@ -892,6 +919,10 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
     DevBuf<int> par_int(ctx, n_int), par_leaf(ctx, n), flags(ctx, n_int), icount(ctx, n_int), collapse(ctx, n_int);
     DevBuf<float3> imin(ctx, n_int), imax(ctx, n_int);
     DevBuf<float> icost(ctx, n_int);
+    if (!all_ok(kl, kr, first, last, par_int, par_leaf, flags, icount, collapse, imin, imax, icost)) {
+      sc->clear_bvh();
+      return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+    }
     cudaMemsetAsync(par_int.p, 0xff, sizeof(int) * n_int, st);
     k_karras<<<grid_for(ctx, n_int), 256, 0, st>>>(n, sc->tmp_codes.p, kl.p, kr.p, first.p, last.p, par_int.p,
                                                     par_leaf.p);
@@ -903,12 +934,19 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
     cudaMemcpyAsync(&root_col, collapse.p, sizeof(int), cudaMemcpyDeviceToHost, st);
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (root_col) {
-      sc->d_nodes.alloc(ctx, 4);
+      if (!sc->d_nodes.alloc(ctx, 4)) {
+        sc->clear_bvh();
+        return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+      }
       k_single_leaf_root<<<1, 1, 0, st>>>(rb.p, rb.p + 1, n, sc->d_nodes.p);
       sc->n_nodes = 1;
     } else {
       sc->d_nodes.alloc(ctx, (size_t)4 * n_int);
       DevBuf<int> la(ctx, n_int), lb(ctx, n_int), cnt(ctx, 1);
+      if (!all_ok(sc->d_nodes, la, lb, cnt)) {
+        sc->clear_bvh();
+        return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
+      }
       int zero = 0;
       cudaMemcpyAsync(la.p, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
       int ncur = 1, base = 0;
@@ -934,7 +972,10 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
   }
   sc->order.swap(order);
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  if (int rc = build_wide(ctx, sc)) return rc;
+  if (int rc = build_wide(ctx, sc)) {
+    sc->clear_bvh();
+    return rc;
+  }
   sc->root_min = hb[0];
   sc->root_max = hb[1];
   sc->n_prims = n;

@@ -40,53 +40,50 @@ struct AtrousArgs {
   int to_display;
 };
 
-__global__ void __launch_bounds__(256) k_atrous(AtrousArgs A, const float4* __restrict__ in,
-                                                const float4* __restrict__ src, const float4* __restrict__ gn,
-                                                const float4* __restrict__ ga, float4* __restrict__ out) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= A.W || y >= A.H) return;
-  long long c = (long long)y * A.W + x;
-  float4 cc = __ldg(in + c);
-  float4 cn = A.use_n || A.use_d ? __ldg(gn + c) : make_float4(0, 0, 0, 0);
-  float4 ca = A.use_a ? __ldg(ga + c) : make_float4(0, 0, 0, 0);
-  float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
-  for (int dy = -A.r; dy <= A.r; ++dy) {
-    int yy = reflect_idx(y + dy * A.step, A.H);
-    for (int dx = -A.r; dx <= A.r; ++dx) {
-      int xx = reflect_idx(x + dx * A.step, A.W);
-      long long q = (long long)yy * A.W + xx;
-      float4 nb = __ldg(in + q);
-      float ex = nb.x - cc.x, ey = nb.y - cc.y, ez = nb.z - cc.z;
-      float d2 = (ex * ex + ey * ey) + ez * ez;
-      float sw = (float)(1.0 / (1.0 + (double)(dx * dx + dy * dy)));
-      float w = sw * expf(-d2 / A.s2c);
-      if (A.use_n || A.use_d) {
-        float4 g = __ldg(gn + q);
-        if (A.use_n) {
-          float gx = g.x - cn.x, gy = g.y - cn.y, gz = g.z - cn.z;
-          w = w * expf(-((gx * gx + gy * gy) + gz * gz) / A.s2n);
-        }
-        if (A.use_a) {
-          float4 al = __ldg(ga + q);
-          float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
-          w = w * expf(-((hx * hx + hy * hy) + hz * hz) / A.s2a);
-        }
-        if (A.use_d) {
-          float gd = g.w - cn.w;
-          w = w * expf(-(gd * gd) / A.s2d);
-        }
-      } else if (A.use_a) {
-        float4 al = __ldg(ga + q);
-        float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
-        w = w * expf(-((hx * hx + hy * hy) + hz * hz) / A.s2a);
-      }
-      ax = ax + nb.x * w;
-      ay = ay + nb.y * w;
-      az = az + nb.z * w;
-      ws = ws + w;
+// One tap's weight.  EXACT (pass 0) is the reference's expression: each
+// range term its own exp of (-d^2 / 2 sigma^2) in float32, multiplied in the
+// reference's order.  The a-trous passes after it (no reference
+// counterpart) sum the exponents and take one exp.
+template <bool EXACT>
+__device__ __forceinline__ float tap_weight(const AtrousArgs& A, float sw, float4 nb, float4 cc, float4 g, float4 cn,
+                                            float4 al, float4 ca) {
+  float ex = nb.x - cc.x, ey = nb.y - cc.y, ez = nb.z - cc.z;
+  float d2 = (ex * ex + ey * ey) + ez * ez;
+  if (EXACT) {
+    float w = sw * expf(-d2 / A.s2c);
+    if (A.use_n) {
+      float gx = g.x - cn.x, gy = g.y - cn.y, gz = g.z - cn.z;
+      w = w * expf(-((gx * gx + gy * gy) + gz * gz) / A.s2n);
     }
+    if (A.use_a) {
+      float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
+      w = w * expf(-((hx * hx + hy * hy) + hz * hz) / A.s2a);
+    }
+    if (A.use_d) {
+      float gd = g.w - cn.w;
+      w = w * expf(-(gd * gd) / A.s2d);
+    }
+    return w;
   }
+  // s2* hold 1 / (2 sigma^2) here
+  float e = d2 * A.s2c;
+  if (A.use_n) {
+    float gx = g.x - cn.x, gy = g.y - cn.y, gz = g.z - cn.z;
+    e += ((gx * gx + gy * gy) + gz * gz) * A.s2n;
+  }
+  if (A.use_a) {
+    float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
+    e += ((hx * hx + hy * hy) + hz * hz) * A.s2a;
+  }
+  if (A.use_d) {
+    float gd = g.w - cn.w;
+    e += (gd * gd) * A.s2d;
+  }
+  return sw * __expf(-e);
+}
+
+__device__ __forceinline__ float4 finish_pixel(const AtrousArgs& A, float ax, float ay, float az, float ws,
+                                               const float4* __restrict__ src, long long c) {
   float den = fmaxf(ws, 1e-8f);
   float fx = ax / den, fy = ay / den, fz = az / den;
   if (A.last) {
@@ -100,7 +97,128 @@ __global__ void __launch_bounds__(256) k_atrous(AtrousArgs A, const float4* __re
       fz = sqrtf(fminf(fmaxf(fz, 0.0f), 1.0f));
     }
   }
-  out[c] = make_float4(fx, fy, fz, 0.0f);
+  return make_float4(fx, fy, fz, 0.0f);
+}
+
+// Shared-memory tiled pass.  Pixels whose coordinates agree modulo `step`
+// form a sub-lattice on which the pass's taps (2^i apart) are direct
+// neighbours, so a block filters a kAtTW x kAtTH tile of one sub-lattice
+// from a shared-memory copy of the tile plus an r-wide halo: colour, the
+// normal / depth guide and the albedo guide are read from HBM once per
+// block (halo overhead (32 + 2r)(16 + 2r) / 512, 1.2x at r = 1) instead of
+// (2r + 1)^2 times per pixel.  Halo pixels are loaded through the reflect
+// padding, so every tap equals the one the reference indexes.  The grid is
+// one-dimensional: block b = ((tile_y * tiles_x + tile_x) * step + ry) *
+// step + rx, with the sub-lattice residue fastest so neighbouring blocks
+// share cache lines.  256 threads: each filters two pixels of a column.
+constexpr int kAtTW = 32, kAtTH = 16, kAtThreads = 256, kAtMaxTiledR = 8;
+
+// Spatial weight 1 / (1 + dx^2 + dy^2), rounded to float32 from double as
+// the reference's float64 kernel weights are.
+__host__ __device__ constexpr float spatial_weight(int dx, int dy) {
+  return (float)(1.0 / (1.0 + (double)(dx * dx + dy * dy)));
+}
+
+// R > 0: the radius as a compile-time constant (taps unrolled, weights
+// folded); R == 0: A.r at run time, weights from a shared-memory table.
+template <bool EXACT, int R>
+__global__ void __launch_bounds__(kAtThreads) k_atrous_tiled(AtrousArgs A, int tiles_x, const float4* __restrict__ in,
+                                                             const float4* __restrict__ src,
+                                                             const float4* __restrict__ gn,
+                                                             const float4* __restrict__ ga, float4* __restrict__ out) {
+  extern __shared__ float4 sm[];
+  const int r = R > 0 ? R : A.r, step = A.step;
+  const int SW = kAtTW + 2 * r, SH = kAtTH + 2 * r, SN = SW * SH;
+  const bool need_g = A.use_n || A.use_d;
+  float4* s_c = sm;
+  float4* s_g = sm + SN;
+  float4* s_a = sm + (need_g ? 2 : 1) * SN;
+  __shared__ float s_sw[(2 * kAtMaxTiledR + 1) * (2 * kAtMaxTiledR + 1)];
+  if (R == 0) {
+    const int d = 2 * r + 1;
+    for (int i = threadIdx.x; i < d * d; i += kAtThreads) s_sw[i] = spatial_weight(i % d - r, i / d - r);
+  }
+  long long b = blockIdx.x;
+  const int rx = (int)(b % step);
+  b /= step;
+  const int ry = (int)(b % step);
+  b /= step;
+  const int tx0 = (int)(b % tiles_x) * kAtTW;
+  const int ty0 = (int)(b / tiles_x) * kAtTH;
+  for (int i = threadIdx.x; i < SN; i += kAtThreads) {
+    const int sy = i / SW, sx = i - sy * SW;
+    const int gy = reflect_idx(ry + step * (ty0 + sy - r), A.H);
+    const int gx = reflect_idx(rx + step * (tx0 + sx - r), A.W);
+    const long long q = (long long)gy * A.W + gx;
+    s_c[i] = __ldg(in + q);
+    if (need_g) s_g[i] = __ldg(gn + q);
+    if (A.use_a) s_a[i] = __ldg(ga + q);
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & (kAtTW - 1);
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll 1
+  for (int ty = threadIdx.x / kAtTW; ty < kAtTH; ty += kAtThreads / kAtTW) {
+    const int x = rx + step * (tx0 + tx), y = ry + step * (ty0 + ty);
+    if (x >= A.W || y >= A.H) continue;
+    const int ci = (ty + r) * SW + tx + r;
+    const float4 cc = s_c[ci];
+    const float4 cn = need_g ? s_g[ci] : zero;
+    const float4 ca = A.use_a ? s_a[ci] : zero;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+#pragma unroll
+    for (int dy = -r; dy <= r; ++dy) {
+      const int row = ci + dy * SW;
+#pragma unroll
+      for (int dx = -r; dx <= r; ++dx) {
+        const int q = row + dx;
+        const float4 nb = s_c[q];
+        const float4 g = need_g ? s_g[q] : zero;
+        const float4 al = A.use_a ? s_a[q] : zero;
+        const float sw = R > 0 ? spatial_weight(dx, dy) : s_sw[(dy + r) * (2 * r + 1) + dx + r];
+        const float w = tap_weight<EXACT>(A, sw, nb, cc, g, cn, al, ca);
+        ax = ax + nb.x * w;
+        ay = ay + nb.y * w;
+        az = az + nb.z * w;
+        ws = ws + w;
+      }
+    }
+    const long long c = (long long)y * A.W + x;
+    out[c] = finish_pixel(A, ax, ay, az, ws, src, c);
+  }
+}
+
+// Radii beyond kAtMaxTiledR: every tap gathered from global memory.
+template <bool EXACT>
+__global__ void __launch_bounds__(256) k_atrous_gather(AtrousArgs A, const float4* __restrict__ in,
+                                                       const float4* __restrict__ src, const float4* __restrict__ gn,
+                                                       const float4* __restrict__ ga, float4* __restrict__ out) {
+  const long long c = blockIdx.x * 256LL + threadIdx.x;
+  if (c >= (long long)A.H * A.W) return;
+  const int y = (int)(c / A.W), x = (int)(c - (long long)y * A.W);
+  const bool need_g = A.use_n || A.use_d;
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 cc = __ldg(in + c);
+  const float4 cn = need_g ? __ldg(gn + c) : zero;
+  const float4 ca = A.use_a ? __ldg(ga + c) : zero;
+  float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+  for (int dy = -A.r; dy <= A.r; ++dy) {
+    const int yy = reflect_idx(y + dy * A.step, A.H);
+    for (int dx = -A.r; dx <= A.r; ++dx) {
+      const int xx = reflect_idx(x + dx * A.step, A.W);
+      const long long q = (long long)yy * A.W + xx;
+      const float4 nb = __ldg(in + q);
+      const float4 g = need_g ? __ldg(gn + q) : zero;
+      const float4 al = A.use_a ? __ldg(ga + q) : zero;
+      const float sw = (float)(1.0 / (1.0 + (double)(dx * dx + dy * dy)));
+      const float w = tap_weight<EXACT>(A, sw, nb, cc, g, cn, al, ca);
+      ax = ax + nb.x * w;
+      ay = ay + nb.y * w;
+      az = az + nb.z * w;
+      ws = ws + w;
+    }
+  }
+  out[c] = finish_pixel(A, ax, ay, az, ws, src, c);
 }
 
 __global__ void k_copy_display(long long n, const float4* __restrict__ in, float4* __restrict__ out, int to_display) {
@@ -117,6 +235,58 @@ static float two_sigma2(float s) {
   double v = (double)s * (double)s;
   if (v < 1e-8) v = 1e-8;
   return (float)(2.0 * v);
+}
+
+// Dynamic shared memory of one tiled block: colour, plus each guide in use.
+static size_t atrous_smem(const AtrousArgs& A) {
+  const size_t px = (size_t)(kAtTW + 2 * A.r) * (kAtTH + 2 * A.r);
+  return px * sizeof(float4) * (1 + ((A.use_n || A.use_d) ? 1 : 0) + (A.use_a ? 1 : 0));
+}
+
+// Enqueues `passes` a-trous passes on `st`: pass i reads `in` (the colour for
+// i = 0) and writes scratch half (i & 1), the last pass writes `out` (and
+// reads `color` again for the blend).  A is filled except step / last.
+static cudaError_t atrous_passes(cudaStream_t st, AtrousArgs A, int passes, const float4* color, const float4* gn,
+                                 const float4* ga, float4* out, float4* s0, float4* s1) {
+  const long long P = (long long)A.H * A.W;
+  const float inv_c = 1.0f / A.s2c, inv_n = 1.0f / A.s2n, inv_a = 1.0f / A.s2a, inv_d = 1.0f / A.s2d;
+  const float s2[4] = {A.s2c, A.s2n, A.s2a, A.s2d};
+  const float4* in = color;
+  for (int i = 0; i < passes; ++i) {
+    A.step = 1 << i;
+    A.last = i == passes - 1;
+    const bool exact = i == 0;
+    if (exact) {
+      A.s2c = s2[0], A.s2n = s2[1], A.s2a = s2[2], A.s2d = s2[3];
+    } else {
+      A.s2c = inv_c, A.s2n = inv_n, A.s2a = inv_a, A.s2d = inv_d;
+    }
+    float4* o = A.last ? out : ((i & 1) ? s1 : s0);
+    if (A.r <= kAtMaxTiledR) {
+      const long long sub_w = (A.W + A.step - 1) / A.step, sub_h = (A.H + A.step - 1) / A.step;
+      const long long tiles_x = (sub_w + kAtTW - 1) / kAtTW, tiles_y = (sub_h + kAtTH - 1) / kAtTH;
+      const long long blocks = tiles_x * tiles_y * A.step * A.step;
+      const size_t smem = atrous_smem(A);
+      if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      auto kern = A.r == 1   ? (exact ? k_atrous_tiled<true, 1> : k_atrous_tiled<false, 1>)
+                  : A.r == 2 ? (exact ? k_atrous_tiled<true, 2> : k_atrous_tiled<false, 2>)
+                             : (exact ? k_atrous_tiled<true, 0> : k_atrous_tiled<false, 0>);
+      if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+      }
+      kern<<<(unsigned)blocks, kAtThreads, smem, st>>>(A, (int)tiles_x, in, color, gn, ga, o);
+    } else {
+      const long long blocks = (P + 255) / 256;
+      if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      if (exact)
+        k_atrous_gather<true><<<(unsigned)blocks, 256, 0, st>>>(A, in, color, gn, ga, o);
+      else
+        k_atrous_gather<false><<<(unsigned)blocks, 256, 0, st>>>(A, in, color, gn, ga, o);
+    }
+    in = o;
+  }
+  return cudaGetLastError();
 }
 
 int denoise_device(Ctx* ctx, int h, int w, const float4* d_color, const float4* d_gn, const float4* d_ga,
@@ -146,17 +316,7 @@ int denoise_device(Ctx* ctx, int h, int w, const float4* d_color, const float4* 
   A.keep = (float)(1.0 - amount);
   A.amount = (float)amount;
   A.to_display = to_display;
-  dim3 blk(32, 8);
-  dim3 grd((w + 31) / 32, (h + 7) / 8);
-  const float4* in = d_color;
-  for (int i = 0; i < passes; ++i) {
-    A.step = 1 << i;
-    A.last = i == passes - 1;
-    float4* o = A.last ? d_out : ((i & 1) ? d_s1 : d_s0);
-    k_atrous<<<grd, blk, 0, st>>>(A, in, d_color, d_gn, d_ga, o);
-    in = o;
-  }
-  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, atrous_passes(st, A, passes, d_color, d_gn, d_ga, d_out, d_s0, d_s1));
   return RX_OK;
 }
 
@@ -235,26 +395,75 @@ int denoise_host(Ctx* ctx, int h, int w, const float* color, const float* normal
 constexpr long long kNoAllocMaxPixels = 1LL << 20;
 static __device__ __align__(256) float4 g_noalloc_scratch[2 * kNoAllocMaxPixels];
 
+// The array's device address differs per CUDA context (the module is loaded
+// into each context), so the looked-up address is cached per context,
+// identified by cuCtxGetId: an id the driver never hands out twice in a
+// process, so a context created after cudaDeviceReset, or a caller's own
+// driver-API context, gets a fresh lookup instead of a stale address.  The
+// driver calls are reached through the runtime's entry-point table (the
+// library does not link libcuda).  Without them the address is looked up on
+// every call, which also allocates nothing.
+typedef int (*PfnCtxGetCurrent)(void**);
+typedef int (*PfnCtxGetId)(void*, unsigned long long*);
 static std::mutex g_noalloc_mu;
-static float4* g_noalloc_ptr[64] = {};
+static bool g_noalloc_fn_init = false;
+static PfnCtxGetCurrent g_ctx_get_current = nullptr;
+static PfnCtxGetId g_ctx_get_id = nullptr;
+constexpr int kNoAllocCache = 16;
+static unsigned long long g_noalloc_ctx[kNoAllocCache] = {};
+static float4* g_noalloc_ptr[kNoAllocCache] = {};
+static int g_noalloc_next = 0;
 
-// Device address of the scratch array on the current device.
+// Device address of the scratch array in the context current on this thread.
 static int noalloc_scratch(float4** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(nullptr, "rx_denoise_noalloc: cudaGetDevice: %s", cudaGetErrorString(e)),
-                               RX_ERR_CUDA;
-  if (dev < 0 || dev >= 64) return set_error(nullptr, "rx_denoise_noalloc: device %d out of range", dev), RX_ERR_ARG;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return set_error(nullptr, "rx_denoise_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
-    g_noalloc_ptr[dev] = static_cast<float4*>(p);
+  if (!g_noalloc_fn_init) {
+    g_noalloc_fn_init = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(f);
+    (void)cudaGetLastError();
   }
-  *out = g_noalloc_ptr[dev];
+  // make the runtime's context current (a no-op when one already is)
+  cudaError_t e = cudaFree(nullptr);
+  if (e != cudaSuccess)
+    return set_error(nullptr, "rx_denoise_noalloc: no usable CUDA context: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
+  unsigned long long id = 0;
+  void* cu = nullptr;
+  const bool have_id = g_ctx_get_current && g_ctx_get_id && g_ctx_get_current(&cu) == 0 && cu &&
+                       g_ctx_get_id(cu, &id) == 0;
+  if (have_id) {
+    for (int i = 0; i < kNoAllocCache; ++i)
+      if (g_noalloc_ptr[i] && g_noalloc_ctx[i] == id) {
+        *out = g_noalloc_ptr[i];
+        return RX_OK;
+      }
+  }
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return set_error(nullptr, "rx_denoise_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
+  if (have_id) {
+    g_noalloc_ctx[g_noalloc_next] = id;
+    g_noalloc_ptr[g_noalloc_next] = static_cast<float4*>(p);
+    g_noalloc_next = (g_noalloc_next + 1) % kNoAllocCache;
+  }
+  *out = static_cast<float4*>(p);
   return RX_OK;
+}
+
+// True when [a, a + an) and [b, b + bn) share a byte.
+static bool overlaps(const void* a, size_t an, const void* b, size_t bn) {
+  if (!a || !b) return false;
+  const char* pa = static_cast<const char*>(a);
+  const char* pb = static_cast<const char*>(b);
+  return pa < pb + bn && pb < pa + an;
 }
 
 }  // namespace rx
@@ -271,23 +480,33 @@ extern "C" int rx_denoise_noalloc(int height, int width, const float* d_color, c
            RX_ERR_CAPACITY;
   if (P == 0) return RX_OK;
   if (!d_color || !d_out) return set_error(nullptr, "rx_denoise_noalloc: NULL colour or output"), RX_ERR_ARG;
-  if ((params->use_normal || params->use_depth) && !d_guide_normal)
+  const bool need_n = params->use_normal || params->use_depth;
+  if (need_n && !d_guide_normal)
     return set_error(nullptr, "rx_denoise_noalloc: normal/depth guide requested but NULL"), RX_ERR_ARG;
   if (params->use_albedo && !d_guide_albedo)
     return set_error(nullptr, "rx_denoise_noalloc: albedo guide requested but NULL"), RX_ERR_ARG;
   if (params->radius < 0 || params->passes < 1 || params->passes > 12)
     return set_error(nullptr, "rx_denoise_noalloc: radius must be >= 0 and passes in [1, 12]"), RX_ERR_ARG;
+  const size_t bytes = (size_t)P * sizeof(float4);
+  if (overlaps(d_out, bytes, d_color, bytes) || (need_n && overlaps(d_out, bytes, d_guide_normal, bytes)) ||
+      (params->use_albedo && overlaps(d_out, bytes, d_guide_albedo, bytes)))
+    return set_error(nullptr, "rx_denoise_noalloc: the output must not overlap the colour or a guide in use"),
+           RX_ERR_ARG;
+  // an error left pending by earlier, unrelated work is not this call's
+  (void)cudaGetLastError();
   float4* scratch = nullptr;
   int rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const float4* color = reinterpret_cast<const float4*>(d_color);
-  const float4* gn = reinterpret_cast<const float4*>(d_guide_normal);
-  const float4* ga = reinterpret_cast<const float4*>(d_guide_albedo);
+  const float4* gn = need_n ? reinterpret_cast<const float4*>(d_guide_normal) : nullptr;
+  const float4* ga = params->use_albedo ? reinterpret_cast<const float4*>(d_guide_albedo) : nullptr;
   float4* out = reinterpret_cast<float4*>(d_out);
+  cudaError_t e = cudaSuccess;
   if (params->radius <= 0 || params->amount <= 0.0f) {
     int blocks = (int)std::min<long long>((P + 255) / 256, 4096);
     k_copy_display<<<blocks, 256, 0, st>>>(P, color, out, params->to_display);
+    e = cudaGetLastError();
   } else {
     double amount = std::min(std::max((double)params->amount, 0.0), 1.0);
     AtrousArgs A;
@@ -304,18 +523,8 @@ extern "C" int rx_denoise_noalloc(int height, int width, const float* d_color, c
     A.keep = (float)(1.0 - amount);
     A.amount = (float)amount;
     A.to_display = params->to_display;
-    dim3 blk(32, 8);
-    dim3 grd((width + 31) / 32, (height + 7) / 8);
-    const float4* in = color;
-    for (int i = 0; i < params->passes; ++i) {
-      A.step = 1 << i;
-      A.last = i == params->passes - 1;
-      float4* o = A.last ? out : scratch + (size_t)(i & 1) * kNoAllocMaxPixels;
-      k_atrous<<<grd, blk, 0, st>>>(A, in, color, gn, ga, o);
-      in = o;
-    }
+    e = atrous_passes(st, A, params->passes, color, gn, ga, out, scratch, scratch + kNoAllocMaxPixels);
   }
-  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_error(nullptr, "rx_denoise_noalloc: launch failed: %s", cudaGetErrorString(e)), RX_ERR_CUDA;
   return RX_OK;

@@ -955,7 +955,7 @@ __global__ void k_pack(long long P, const float4* __restrict__ src, int comp, fl
 }
 
 // -------------------------------------------------------------------- host
-enum { K_EXTEND = 0, K_SHADE = 1, K_CONNECT = 2, K_OTHER = 3, K_CLASSES = 4 };
+enum { K_EXTEND = 0, K_SHADE = 1, K_CONNECT = 2, K_OTHER = 3, K_ACCUM = 4, K_CLASSES = 5 };
 
 struct Accum {
   Ctx* ctx = nullptr;
@@ -985,7 +985,7 @@ struct Accum {
   std::vector<cudaEvent_t> ev;
   std::vector<int> ev_class;
   float last_ms = 0.0f;
-  float last_k[K_CLASSES] = {0, 0, 0, 0};
+  float last_k[K_CLASSES] = {0, 0, 0, 0, 0};
   int last_launches = 0;
   // denoise scratch
   DevBuf<float4> dn0, dn1, dn_out;
@@ -1184,6 +1184,7 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   int ablocks = (int)std::min<long long>((K.P + 255) / 256, (long long)ctx->num_sms * 16);
   JobAcc A{a->acc_r.p, a->acc_n.p, a->acc_a.p, a->pixels.p, a->acc64.p, a->frame_base.p, a->rays.p};
   k_accumulate<<<std::max(ablocks, 1), 256, 0, st>>>(K, A, a->rad.p, a->gn.p, a->ga.p);
+  mark(K_ACCUM);
   k_finish<<<1, 1, 0, st>>>(a->counters.p, K.max_depth, a->frame_base.p, a->rays.p, K.spf);
   launches += 2;
   mark(K_OTHER);
@@ -1287,7 +1288,7 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
     a->drop_graph();
   }
   cudaStream_t st = ctx->stream;
-  float k_ms[K_CLASSES] = {0, 0, 0, 0};
+  float k_ms[K_CLASSES] = {0, 0, 0, 0, 0};
   float total_ms = 0.0f;
   int launches_total = 0;
   int remaining = frames;
@@ -1378,6 +1379,7 @@ int accum_read(Accum* a, int which, float* host_out) {
     default: return set_error(ctx, "accum_read: unknown buffer %d", which), RX_ERR_ARG;
   }
   DevBuf<float> tmp(ctx, (size_t)a->P * comp);
+  if (!tmp.ok()) return set_error(ctx, "accum_read: out of device memory"), RX_ERR_CAPACITY;
   int blocks = (int)std::min<long long>((a->P + 255) / 256, (long long)ctx->num_sms * 16);
   k_pack<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(a->P, src, comp, tmp.p);
   return read_to_host(a, host_out, tmp.p, tmp.bytes());
@@ -1456,6 +1458,7 @@ int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out) {
   if (rc) return rc;
   if (host_out) {
     DevBuf<float> tmp(ctx, (size_t)a->P * 3);
+    if (!tmp.ok()) return set_error(ctx, "accum_denoise: out of device memory"), RX_ERR_CAPACITY;
     int blocks = (int)std::min<long long>((a->P + 255) / 256, (long long)ctx->num_sms * 16);
     k_pack<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(a->P, a->dn_out.p, 3, tmp.p);
     CUDA_TRY(ctx, cudaMemcpyAsync(host_out, tmp.p, tmp.bytes(), cudaMemcpyDeviceToHost, ctx->stream));

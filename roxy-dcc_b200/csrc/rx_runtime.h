@@ -44,6 +44,7 @@ struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
   Ctx* ctx = nullptr;
+  bool failed = false;  // the last alloc() could not get its memory
   DevBuf() {}
   DevBuf(Ctx* c, size_t count) { alloc(c, count); }
   DevBuf(const DevBuf&) = delete;
@@ -53,14 +54,18 @@ struct DevBuf {
     release();
     ctx = c;
     n = count;
+    failed = false;
     if (count == 0) return true;
     if (cudaMallocAsync((void**)&p, sizeof(T) * count, c->stream) != cudaSuccess) {
+      (void)cudaGetLastError();  // out of memory is not sticky: drop it here
       p = nullptr;
       n = 0;
+      failed = true;
       return false;
     }
     return true;
   }
+  bool ok() const { return !failed; }
   void release() {
     if (p && ctx) cudaFreeAsync(p, ctx->stream);
     p = nullptr;
@@ -70,9 +75,16 @@ struct DevBuf {
     std::swap(p, o.p);
     std::swap(n, o.n);
     std::swap(ctx, o.ctx);
+    std::swap(failed, o.failed);
   }
   size_t bytes() const { return sizeof(T) * n; }
 };
+
+// True when every buffer got the memory its last alloc() asked for.
+template <class... B>
+inline bool all_ok(const B&... b) {
+  return (b.ok() && ...);
+}
 
 struct HostMat {
   int type;

@@ -127,6 +127,7 @@ int scene_query(Ctx* ctx, Scene* sc, long n, const float* d_ro, const float* d_r
   DevScene S = sc->view();
   if (n <= 0) return RX_OK;
   DevBuf<int> lin(ctx, std::max<size_t>(sc->lin_slot.size(), 1));
+  if (!lin.ok()) return set_error(ctx, "scene query: out of device memory"), RX_ERR_CAPACITY;
   if (!sc->lin_slot.empty())
     cudaMemcpyAsync(lin.p, sc->lin_slot.data(), sizeof(int) * sc->lin_slot.size(), cudaMemcpyHostToDevice,
                     ctx->stream);

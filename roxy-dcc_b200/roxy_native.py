@@ -612,11 +612,11 @@ class Accumulator:
 
     def last_timing(self):
         tot = ctypes.c_float()
-        ks = (ctypes.c_float * 4)()
+        ks = (ctypes.c_float * 5)()
         nl = ctypes.c_int()
-        self.ctx.check(lib().rx_accum_last_timing(self.h, ctypes.byref(tot), ks, 4, ctypes.byref(nl)))
+        self.ctx.check(lib().rx_accum_last_timing(self.h, ctypes.byref(tot), ks, 5, ctypes.byref(nl)))
         return dict(total_ms=tot.value, extend_ms=ks[0], shade_ms=ks[1], connect_ms=ks[2], other_ms=ks[3],
-                    launches=nl.value)
+                    accumulate_ms=ks[4], launches=nl.value)
 
     def set_f64(self, on):
         """Keep float64 sums of the clamped sample radiance (reset first)."""

@@ -68,3 +68,46 @@ def test_noalloc_denoise_rejects_sizes_beyond_its_scratch():
     rc = L.rx_denoise_noalloc(1025, 1024, None, None, None, ctypes.byref(p), None, None)
     assert rc == nat.RX_ERR_CAPACITY
     assert b"scratch limit" in L.rx_last_error(None)
+
+
+def _noalloc(torch, L, H, W, c4, n4, a4, p, out):
+    rc = L.rx_denoise_noalloc(H, W, c4.data_ptr(), n4.data_ptr() if n4 is not None else None,
+                              a4.data_ptr() if a4 is not None else None, ctypes.byref(p), out.data_ptr(),
+                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == nat.RX_OK, L.rx_last_error(None)
+    torch.cuda.synchronize()
+    return out[..., :3].cpu().numpy()
+
+
+def test_noalloc_copy_path_and_guides_off():
+    """radius 0 (the display copy) and a filter with every guide off and NULL
+    guide pointers, each against the allocating entry point."""
+    torch = pytest.importorskip("torch")
+    L = nat.lib()
+    nat.context()
+    H, W = 40, 57
+    color, normal, albedo, depth = _inputs(5, H, W)
+    c4 = _pack4(torch, color)
+    out = torch.full((H, W, 4), float("nan"), device="cuda")
+    p = nat.DenoiseParams(0, 1, 0.1, 0.35, 0.20, 1.0, 0.8, 0, 0, 0, 1)
+    got = _noalloc(torch, L, H, W, c4, None, None, p, out)
+    np.testing.assert_array_equal(got, np.sqrt(np.clip(color, 0.0, 1.0)))
+    for passes in (1, 4):
+        ref = nat.denoise(color, radius=1, sigma_color=0.2, amount=0.9, passes=passes)
+        p = nat.DenoiseParams(1, passes, 0.2, 0.35, 0.20, 1.0, 0.9, 0, 0, 0, 0)
+        out.fill_(float("nan"))
+        got = _noalloc(torch, L, H, W, c4, None, None, p, out)
+        np.testing.assert_allclose(got, ref, rtol=2e-6, atol=2e-6, err_msg=f"{passes} passes, no guides")
+
+
+def test_noalloc_rejects_an_output_that_overlaps_an_input():
+    torch = pytest.importorskip("torch")
+    L = nat.lib()
+    H, W = 8, 8
+    c4 = torch.zeros((H, W, 4), device="cuda")
+    n4 = torch.zeros((H, W, 4), device="cuda")
+    p = nat.DenoiseParams(1, 2, 0.1, 0.35, 0.20, 1.0, 0.8, 1, 0, 0, 0)
+    for out in (c4, n4):
+        rc = L.rx_denoise_noalloc(H, W, c4.data_ptr(), n4.data_ptr(), None, ctypes.byref(p), out.data_ptr(), None)
+        assert rc == nat.RX_ERR_ARG
+        assert b"overlap" in L.rx_last_error(None)

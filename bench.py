@@ -773,11 +773,15 @@ def run_obj(args):
 
 
 def run_serve(args):
-    """Serving configuration: Poisson arrivals at swept rates; each request
-    renders one of four displaced-icosphere scenes (the large-mesh
-    generator, seeds 2024-2027, resident on the device) at a resolution
-    from {256^2, 512^2, 1024^2} and spp from {1, 4, 16, 64}, max depth 12.
-    The batched server (continuous batching, 150 GB admission budget, 1-spp
+    """Serving configuration: Poisson arrivals at swept rates.  By default
+    (--serve-scenes fresh) every request arrives as a world from the
+    large-mesh generator (eight seeds, 2024-2031, generated on the host
+    before the sweep) and its scene is extracted and its BVH built on the
+    device when it arrives, inside the request's latency; requests are
+    1920x1080, 64 spp, depth 12 as in that configuration
+    (--serve-sizes c2).  --serve-scenes resident reuses four resident
+    scenes, --serve-sizes mixed draws 256^2-1024^2 and 1-64 spp.  The
+    batched server (continuous batching, 150 GB admission budget, 1-spp
     preview first) is compared with the plain path: the same server with
     one active request at a time.  Every rate uses the same seeded request
     list (the first N of one draw)."""
@@ -785,51 +789,85 @@ def run_serve(args):
     import workloads
     from rendering.batch import Job
     from rendering.serving import RenderServer, poisson_run
+    from rendering.taichi.extractor import build_device_scene
+    from rendering.taichi.trace import make_params
 
     ws, rank, local = _dist()
     if rank != 0:
         return 0
     ctx = nat.context(0)
+    fresh = args.serve_scenes == "fresh"
+    c2 = args.serve_sizes == "c2"
     t0 = time.perf_counter()
-    pool = [Job(workloads.displaced_icosphere_scene(64, 64, seed=2024 + k), 64, 64, 1, 12).prepare(ctx=ctx)
-            for k in range(4)]
-    build_s = time.perf_counter() - t0
+    n_worlds = 8 if fresh else 4
+    aspect = (1920, 1080) if c2 else (64, 64)
+    worlds = [workloads.displaced_icosphere_scene(*aspect, seed=2024 + k) for k in range(n_worlds)]
+    pool = [] if fresh else [Job(w, 64, 64, 1, 12).prepare(ctx=ctx) for w in worlds]
+    gen_s = time.perf_counter() - t0
+    max_req = args.max_requests or (120 if c2 else 600)
     rng = np.random.default_rng(99)
+    build_ms = []
+
+    def fresh_request(world, W, H, spp, seed):
+        def prepare():
+            tb = time.perf_counter()
+            ds = build_device_scene(world, method="lbvh")
+            ds.use_lights(False)
+            cam = world.active_camera
+            p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
+                            1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
+                            list(cam.right), list(cam.up), seed=seed)
+            build_ms.append((time.perf_counter() - tb) * 1e3)
+            return ds.native, p, spp, ds
+        return prepare
+
     all_reqs = []
-    for _ in range(args.max_requests):
-        base = pool[int(rng.integers(0, len(pool)))]
-        res = int(rng.choice([256, 512, 1024]))
-        spp = int(rng.choice([1, 4, 16, 64]))
-        j = Job(base.world, res, res, spp, 12, scene=base.scene, seed=int(rng.integers(0, 1 << 30))).prepare(ctx=ctx)
-        all_reqs.append((j.scene.native, j.params, j.spp))
+    for _ in range(max_req):
+        k = int(rng.integers(0, n_worlds))
+        if c2:
+            W, H, spp = 1920, 1080, 64
+        else:
+            W = H = int(rng.choice([256, 512, 1024]))
+            spp = int(rng.choice([1, 4, 16, 64]))
+        seed = int(rng.integers(0, 1 << 30))
+        if fresh:
+            all_reqs.append(fresh_request(worlds[k], W, H, spp, seed))
+        else:
+            j = Job(worlds[k], W, H, spp, 12, scene=pool[k].scene, seed=seed).prepare(ctx=ctx)
+            all_reqs.append((j.scene.native, j.params, j.spp))
     rates = [float(r) for r in args.rates.split(",")]
     rows = []
     for rate in rates:
-        n = int(min(max(rate * args.duration, 20), args.max_requests))
+        n = int(min(max(rate * args.duration, 20), max_req))
         reqs = all_reqs[:n]
         row = {"rate_rps": rate, "requests": n}
         for name, kw in (("batched", dict(max_active=1024, step_paths=1 << 23)),
                          ("plain", dict(max_active=1, step_paths=1 << 40))):
             srv = RenderServer(hbm_budget=150e9, wave_paths=1 << 25, preview_frames=1, ctx=ctx, **kw)
-            poisson_run(srv, all_reqs[-8:], rate=rate, seed=1)  # warm
+            poisson_run(srv, all_reqs[-4:], rate=rate, seed=1)  # warm
             st0 = srv.stats()
+            build_ms.clear()
             with ClockSampler(0) as clocks:
                 r = poisson_run(srv, reqs, rate=rate, seed=2)
             st = srv.stats()
             srv.close()
             row[name] = {k: r[k] for k in ("preview_p50_ms", "preview_p99_ms", "final_p50_ms", "final_p99_ms",
-                                           "throughput_rps")}
+                                           "throughput_rps", "prepare_p50_ms", "prepare_p99_ms")}
             row[name].update(max_active=st["max_active_seen"], max_gb=st["max_bytes_in_use"] / 1e9,
                              steps=st["steps"] - st0["steps"], busy_s=st["busy_s"] - st0["busy_s"],
                              clocks=clocks.summary())
+            if build_ms:
+                row[name]["scene_build_ms_p50"] = float(np.percentile(build_ms, 50))
         rows.append(row)
     top = rows[-1]
+    desc = ("Poisson arrivals; each request a displaced-icosphere world (327,680 tris + 64 spheres, "
+            + ("8 seeds, extracted + BVH-built on arrival" if fresh else "4 resident scenes") + "), "
+            + ("1920x1080, 64 spp" if c2 else "256^2-1024^2, 1-64 spp") + ", depth 12, 150 GB budget, 1-spp preview")
     line = {"metric": "requests/s", "value": top["batched"]["throughput_rps"], "unit": "requests/s", "n_gpus": 1,
             "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": "Poisson arrivals, 4 resident displaced-icosphere scenes (327,680 tris + 64 "
-                                   "spheres), 256^2-1024^2, 1-64 spp, depth 12, 150 GB budget, 1-spp preview",
-                       "scene_build_s": build_s, "rates_rps": rates},
+            "config": {"workload": desc, "world_generation_s": gen_s, "rates_rps": rates,
+                       "latency_from": "arrival (scene build included)" if fresh else "submission"},
             "sweep": rows,
             "speedup_vs_plain_at_top_rate": top["batched"]["throughput_rps"] / top["plain"]["throughput_rps"],
             "preview_p99_ms_at_top_rate": top["batched"]["preview_p99_ms"]}
@@ -848,7 +886,12 @@ def main():
     ap.add_argument("--scenes", type=int, default=64, help="scenes in the batch workload")
     ap.add_argument("--rates", default="10,50,100,200,500", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=3.0, help="serve workload: seconds of arrivals per rate")
-    ap.add_argument("--max-requests", type=int, default=600, help="serve workload: requests per rate at most")
+    ap.add_argument("--max-requests", type=int, default=0,
+                    help="serve workload: requests per rate at most (0: 120 for c2 sizes, 600 for mixed)")
+    ap.add_argument("--serve-scenes", default="fresh", choices=["fresh", "resident"],
+                    help="serve workload: build each request's scene on arrival, or reuse resident scenes")
+    ap.add_argument("--serve-sizes", default="c2", choices=["c2", "mixed"],
+                    help="serve workload: 1920x1080 64 spp per request, or 256^2-1024^2 x 1-64 spp")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-spp", type=int, default=4096,
                     help="spp of the float64 reference render for relMSE (0: skip)")

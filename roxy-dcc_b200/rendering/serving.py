@@ -86,17 +86,22 @@ def percentile(xs, q):
 
 
 def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0):
-    """Submit `requests` (list of (NativeScene, RenderParams, frames)) with
-    exponential inter-arrival times of mean 1/rate.  A second thread plays
-    the client that waits for each final image, reads it if asked and
-    releases the request as soon as it is done, while arrivals continue.
-    Returns latency and throughput figures."""
+    """Submit `requests` with exponential inter-arrival times of mean
+    1/rate.  A request is (NativeScene, RenderParams, frames), or a callable
+    that returns one: it runs when the request arrives (building the
+    request's scene, say), and the time it takes counts toward the
+    request's latencies.  A second thread plays the client that waits for
+    each final image, reads it if asked and releases the request as soon as
+    it is done, while arrivals continue.  Returns latency and throughput
+    figures (latencies from arrival)."""
     import queue
     import threading
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, size=len(requests))
     ids = queue.Queue()
     infos, errors = [], []
+    prep_s = {}
+    keep = {}
 
     def collect():
         for _ in range(len(requests)):
@@ -105,10 +110,13 @@ def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0)
                 return
             try:
                 server.wait(rid, final=True, timeout=timeout)
-                infos.append(server.info(rid))
+                info = server.info(rid)
+                info["prep_s"] = prep_s.get(rid, 0.0)
+                infos.append(info)
                 if read_final:
                     server.read(rid)
                 server.release(rid)
+                keep.pop(rid, None)
             except Exception as e:  # re-raised after the run
                 errors.append(e)
 
@@ -117,12 +125,20 @@ def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0)
     t_start = time.perf_counter()
     t_next = t_start
     try:
-        for (scene, params, frames), gap in zip(requests, gaps):
+        for req, gap in zip(requests, gaps):
             t_next += gap
             delay = t_next - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            ids.put(server.submit(scene, params, frames))
+            made = req() if callable(req) else req
+            scene, params, frames = made[:3]
+            # a request's latency runs from its arrival: the time spent
+            # behind earlier arrivals' preparation counts too
+            prep = time.perf_counter() - t_next
+            rid = server.submit(scene, params, frames)
+            prep_s[rid] = prep
+            keep[rid] = made
+            ids.put(rid)
     except Exception:
         ids.put(None)
         th.join()
@@ -131,11 +147,13 @@ def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0)
     if errors:
         raise errors[0]
     t_end = time.perf_counter()
-    prev = [i["t_preview"] - i["t_submit"] for i in infos]
-    fin = [i["t_final"] - i["t_submit"] for i in infos]
+    prev = [i["t_preview"] - i["t_submit"] + i["prep_s"] for i in infos]
+    fin = [i["t_final"] - i["t_submit"] + i["prep_s"] for i in infos]
+    prep = [i["prep_s"] for i in infos]
     first = min(i["t_submit"] for i in infos)
     last = max(i["t_final"] for i in infos)
     return {"requests": len(infos), "rate": rate, "preview_p50_ms": 1e3 * percentile(prev, 50),
             "preview_p99_ms": 1e3 * percentile(prev, 99), "final_p50_ms": 1e3 * percentile(fin, 50),
             "final_p99_ms": 1e3 * percentile(fin, 99), "throughput_rps": len(infos) / max(last - first, 1e-9),
+            "prepare_p50_ms": 1e3 * percentile(prep, 50), "prepare_p99_ms": 1e3 * percentile(prep, 99),
             "wall_s": t_end - t_start}

@@ -132,3 +132,50 @@ def test_poisson_run_reports_latencies():
     assert r["throughput_rps"] > 0
     assert srv.stats()["completed"] == len(jobs)
     srv.close()
+
+
+def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
+    """Each request arrives as a world: its scene is extracted and its BVH
+    built when it arrives, while earlier requests are rendering; the served
+    image equals a solo render of the same world bit for bit, and the
+    scenes' device memory is charged and given back with the requests."""
+    import math
+
+    from rendering.taichi.extractor import build_device_scene
+    from rendering.taichi.trace import make_params
+    worlds = [workloads.displaced_icosphere_scene(48, 27, subdiv=5, n_spheres=8, seed=3000 + k) for k in range(3)]
+    specs = [(worlds[k % 3], 48 + 16 * (k % 2), 27 + 9 * (k % 2), 1 + k % 4, 100 + k) for k in range(8)]
+
+    def request(world, W, H, spp, seed):
+        def prepare():
+            ds = build_device_scene(world, method="lbvh")
+            ds.use_lights(False)
+            cam = world.active_camera
+            p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
+                            1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
+                            list(cam.right), list(cam.up), seed=seed)
+            return ds.native, p, spp, ds
+        return prepare
+
+    srv = RenderServer(hbm_budget=8e9, max_active=4, step_paths=3000, wave_paths=1 << 16)
+    base = srv.stats()["bytes_in_use"]
+    r = poisson_run(srv, [request(*s) for s in specs], rate=400.0, seed=3)
+    assert r["requests"] == len(specs) and r["prepare_p50_ms"] > 0
+    st = srv.stats()
+    assert st["completed"] == len(specs) and st["failed"] == 0
+    assert st["bytes_in_use"] == base
+    srv.close()
+    # served images of scenes built while earlier requests render, against
+    # solo renders of the same scenes
+    srv = RenderServer(hbm_budget=8e9, max_active=4, step_paths=3000, wave_paths=1 << 16)
+    ids = []
+    for s in specs:
+        scene, p, spp, ds = request(*s)()
+        ids.append((srv.submit(scene, p, spp), scene, p, spp, ds))
+    for rid, scene, p, spp, _ in ids:
+        srv.wait(rid, final=True, timeout=60)
+        acc = nat.Accumulator(p.width, p.height)
+        acc.render(scene, p, spp)
+        _check_same(srv, rid, [acc.read(w) for w in BUFS])
+        srv.release(rid)
+    srv.close()

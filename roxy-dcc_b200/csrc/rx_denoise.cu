@@ -35,6 +35,8 @@ struct AtrousArgs {
   int H, W, r, step;
   int use_n, use_a, use_d;
   float s2c, s2n, s2a, s2d;  // 2 sigma^2 of each range term (float32 of the double value)
+  float r2c, r2n, r2a, r2d;  // RN(1 / (2 sigma^2)) of the same float32 values
+  int quot;                  // pass 0 forms its quotients with div_by (all 2 sigma^2 <= 2^30)
   int last;                  // fuse blend + display
   float keep, amount;        // f32(1 - amount), f32(amount)
   int to_display;
@@ -50,42 +52,54 @@ __device__ __forceinline__ float tap_weight(const AtrousArgs& A, float sw, float
   float ex = nb.x - cc.x, ey = nb.y - cc.y, ez = nb.z - cc.z;
   float d2 = (ex * ex + ey * ey) + ez * ez;
   if (EXACT) {
-    float w = sw * expf(-d2 / A.s2c);
+    // each quotient is the float the division gives (div_by)
+    auto q = [&](float x, float s2, float r2) { return A.quot ? div_by(x, s2, r2) : x / s2; };
+    float w = sw * expf(q(-d2, A.s2c, A.r2c));
     if (A.use_n) {
       float gx = g.x - cn.x, gy = g.y - cn.y, gz = g.z - cn.z;
-      w = w * expf(-((gx * gx + gy * gy) + gz * gz) / A.s2n);
+      w = w * expf(q(-((gx * gx + gy * gy) + gz * gz), A.s2n, A.r2n));
     }
     if (A.use_a) {
       float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
-      w = w * expf(-((hx * hx + hy * hy) + hz * hz) / A.s2a);
+      w = w * expf(q(-((hx * hx + hy * hy) + hz * hz), A.s2a, A.r2a));
     }
     if (A.use_d) {
       float gd = g.w - cn.w;
-      w = w * expf(-(gd * gd) / A.s2d);
+      w = w * expf(q(-(gd * gd), A.s2d, A.r2d));
     }
     return w;
   }
-  // s2* hold 1 / (2 sigma^2) here
-  float e = d2 * A.s2c;
+  // fused multiply-adds throughout
+  float e = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, ex * ex)) * A.r2c;
   if (A.use_n) {
     float gx = g.x - cn.x, gy = g.y - cn.y, gz = g.z - cn.z;
-    e += ((gx * gx + gy * gy) + gz * gz) * A.s2n;
+    e = __fmaf_rn(__fmaf_rn(gz, gz, __fmaf_rn(gy, gy, gx * gx)), A.r2n, e);
   }
   if (A.use_a) {
     float hx = al.x - ca.x, hy = al.y - ca.y, hz = al.z - ca.z;
-    e += ((hx * hx + hy * hy) + hz * hz) * A.s2a;
+    e = __fmaf_rn(__fmaf_rn(hz, hz, __fmaf_rn(hy, hy, hx * hx)), A.r2a, e);
   }
   if (A.use_d) {
     float gd = g.w - cn.w;
-    e += (gd * gd) * A.s2d;
+    e = __fmaf_rn(gd * gd, A.r2d, e);
   }
   return sw * __expf(-e);
 }
 
+// Normalised sum of one pixel; the last pass blends with the source and
+// maps to display.  Pass 0 divides as the reference does; the later passes
+// multiply by one correctly rounded reciprocal.
+template <bool EXACT>
 __device__ __forceinline__ float4 finish_pixel(const AtrousArgs& A, float ax, float ay, float az, float ws,
                                                const float4* __restrict__ src, long long c) {
   float den = fmaxf(ws, 1e-8f);
-  float fx = ax / den, fy = ay / den, fz = az / den;
+  float fx, fy, fz;
+  const float r = __frcp_rn(den);
+  if (EXACT) {
+    fx = div_by(ax, den, r), fy = div_by(ay, den, r), fz = div_by(az, den, r);
+  } else {
+    fx = ax * r, fy = ay * r, fz = az * r;
+  }
   if (A.last) {
     float4 s = __ldg(src + c);
     fx = s.x * A.keep + fx * A.amount;
@@ -184,7 +198,107 @@ __global__ void __launch_bounds__(kAtThreads) k_atrous_tiled(AtrousArgs A, int t
       }
     }
     const long long c = (long long)y * A.W + x;
-    out[c] = finish_pixel(A, ax, ay, az, ws, src, c);
+    out[c] = finish_pixel<EXACT>(A, ax, ay, az, ws, src, c);
+  }
+}
+
+// Radius 1 (the renderer's default): a tap's weight is symmetric in its two
+// pixels, bit for bit even in pass 0 ((a - b)^2 equals (b - a)^2 exactly
+// and the spatial weight depends on |dx|, |dy|), so each pair of
+// neighbours is weighed once.  A block loads a 32-column x 16-row grid of
+// the sub-lattice (tiles of outputs plus their one-pixel halo), every grid
+// pixel of rows 0-14 weighs its four forward neighbours (right, down-left,
+// down, down-right) into shared memory, and each output then gathers its
+// nine weights -- the centre's is 1 -- and sums its taps in the reference's
+// order: 4.6 weight evaluations per output instead of 9.
+// P = 1 (pass 0, step 1): one 30 x 14 output tile, lane = grid column.
+// P = 2 (step >= 2): two adjacent x residues side by side, grid column c
+// of residue plane k stored at c * 2 + k, so two neighbouring lanes read
+// and write two adjacent pixels and every 32-byte sector a warp touches is
+// used whole (one residue per block would use half of each); 2 x 14 x 14
+// outputs.
+constexpr int kA1H = 14, kA1GW = 32, kA1GH = 16, kA1Src = (kA1H + 1) * kA1GW;
+
+template <bool EXACT, int P>
+__global__ void __launch_bounds__(kAtThreads) k_atrous_r1(AtrousArgs A, int tiles_x, const float4* __restrict__ in,
+                                                          const float4* __restrict__ src,
+                                                          const float4* __restrict__ gn,
+                                                          const float4* __restrict__ ga, float4* __restrict__ out) {
+  constexpr int PW = kA1GW / P, OW = PW - 2, NOUT = P * OW * kA1H;
+  __shared__ float4 s_c[kA1GW * kA1GH], s_g[kA1GW * kA1GH], s_a[kA1GW * kA1GH];
+  __shared__ float s_w[4][kA1Src];  // forward weights: right, down-left, down, down-right
+  const int step = A.step;
+  const bool need_g = A.use_n || A.use_d;
+  const int xres = step / P;  // x residue groups
+  long long b = blockIdx.x;
+  const int rx0 = (int)(b % xres) * P;
+  b /= xres;
+  const int ry = (int)(b % step);
+  b /= step;
+  const int tx0 = (int)(b % tiles_x) * OW;
+  const int ty0 = (int)(b / tiles_x) * kA1H;
+  const int lane = threadIdx.x & 31;
+  {
+    const int col = lane / P, plane = lane % P;
+    const int gx = reflect_idx(rx0 + plane + step * (tx0 + col - 1), A.W);
+    for (int sy = threadIdx.x >> 5; sy < kA1GH; sy += kAtThreads / 32) {
+      const int gy = reflect_idx(ry + step * (ty0 + sy - 1), A.H);
+      const long long q = (long long)gy * A.W + gx;
+      const int i = sy * kA1GW + lane;
+      s_c[i] = __ldg(in + q);
+      if (need_g) s_g[i] = __ldg(gn + q);
+      if (A.use_a) s_a[i] = __ldg(ga + q);
+    }
+  }
+  __syncthreads();
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (int i = threadIdx.x; i < kA1Src; i += kAtThreads) {
+    const int c = (i & 31) / P;
+    const float4 oc = s_c[i], og = need_g ? s_g[i] : zero, oa = A.use_a ? s_a[i] : zero;
+    // right (dx 1), down-left (dx -1, dy 1), down (dy 1), down-right (1, 1)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int dx = k == 0 ? 1 : k - 2, dy = k == 0 ? 0 : 1;
+      const int tc = c + dx;
+      float w = 0.0f;
+      if (tc >= 0 && tc < PW) {
+        const int t = i + dy * kA1GW + dx * P;
+        w = tap_weight<EXACT>(A, spatial_weight(dx, dy), s_c[t], oc, need_g ? s_g[t] : zero, og,
+                              A.use_a ? s_a[t] : zero, oa);
+      }
+      s_w[k][i] = w;
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < NOUT; j += kAtThreads) {
+    const int oy = j / (P * OW), rem = j - oy * (P * OW);
+    const int plane = rem % P, ox = rem / P;
+    const int x = rx0 + plane + step * (tx0 + ox), y = ry + step * (ty0 + oy);
+    if (x >= A.W || y >= A.H) continue;
+    const int p = (oy + 1) * kA1GW + (ox + 1) * P + plane;
+    constexpr int U = kA1GW, L = P;  // one grid row up, one grid column left
+    // taps in the reference's order: dy -1..1 outer, dx -1..1 inner
+    const int tq[9] = {p - U - L, p - U, p - U + L, p - L, p, p + L, p + U - L, p + U, p + U + L};
+    const float tw[9] = {s_w[3][p - U - L], s_w[2][p - U], s_w[1][p - U + L], s_w[0][p - L], 1.0f,
+                         s_w[0][p], s_w[1][p], s_w[2][p], s_w[3][p]};
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, ws = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float4 nb = s_c[tq[k]];
+      const float w = tw[k];
+      if (EXACT) {
+        ax = ax + nb.x * w;
+        ay = ay + nb.y * w;
+        az = az + nb.z * w;
+      } else {
+        ax = __fmaf_rn(nb.x, w, ax);
+        ay = __fmaf_rn(nb.y, w, ay);
+        az = __fmaf_rn(nb.z, w, az);
+      }
+      ws = ws + w;
+    }
+    const long long c = (long long)y * A.W + x;
+    out[c] = finish_pixel<EXACT>(A, ax, ay, az, ws, src, c);
   }
 }
 
@@ -218,7 +332,7 @@ __global__ void __launch_bounds__(256) k_atrous_gather(AtrousArgs A, const float
       ws = ws + w;
     }
   }
-  out[c] = finish_pixel(A, ax, ay, az, ws, src, c);
+  out[c] = finish_pixel<EXACT>(A, ax, ay, az, ws, src, c);
 }
 
 __global__ void k_copy_display(long long n, const float4* __restrict__ in, float4* __restrict__ out, int to_display) {
@@ -249,20 +363,24 @@ static size_t atrous_smem(const AtrousArgs& A) {
 static cudaError_t atrous_passes(cudaStream_t st, AtrousArgs A, int passes, const float4* color, const float4* gn,
                                  const float4* ga, float4* out, float4* s0, float4* s1) {
   const long long P = (long long)A.H * A.W;
-  const float inv_c = 1.0f / A.s2c, inv_n = 1.0f / A.s2n, inv_a = 1.0f / A.s2a, inv_d = 1.0f / A.s2d;
-  const float s2[4] = {A.s2c, A.s2n, A.s2a, A.s2d};
+  A.r2c = 1.0f / A.s2c, A.r2n = 1.0f / A.s2n, A.r2a = 1.0f / A.s2a, A.r2d = 1.0f / A.s2d;
+  A.quot = std::max(std::max(A.s2c, A.s2n), std::max(A.s2a, A.s2d)) <= 0x1p+30f;
   const float4* in = color;
   for (int i = 0; i < passes; ++i) {
     A.step = 1 << i;
     A.last = i == passes - 1;
     const bool exact = i == 0;
-    if (exact) {
-      A.s2c = s2[0], A.s2n = s2[1], A.s2a = s2[2], A.s2d = s2[3];
-    } else {
-      A.s2c = inv_c, A.s2n = inv_n, A.s2a = inv_a, A.s2d = inv_d;
-    }
     float4* o = A.last ? out : ((i & 1) ? s1 : s0);
-    if (A.r <= kAtMaxTiledR) {
+    if (A.r == 1) {
+      const int P = A.step >= 2 ? 2 : 1, ow = kA1GW / P - 2;
+      const long long sub_w = (A.W + A.step - 1) / A.step, sub_h = (A.H + A.step - 1) / A.step;
+      const long long tiles_x = (sub_w + ow - 1) / ow, tiles_y = (sub_h + kA1H - 1) / kA1H;
+      const long long blocks = tiles_x * tiles_y * (A.step / P) * A.step;
+      if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      auto kern = P == 1 ? (exact ? k_atrous_r1<true, 1> : k_atrous_r1<false, 1>)
+                         : (exact ? k_atrous_r1<true, 2> : k_atrous_r1<false, 2>);
+      kern<<<(unsigned)blocks, kAtThreads, 0, st>>>(A, (int)tiles_x, in, color, gn, ga, o);
+    } else if (A.r <= kAtMaxTiledR) {
       const long long sub_w = (A.W + A.step - 1) / A.step, sub_h = (A.H + A.step - 1) / A.step;
       const long long tiles_x = (sub_w + kAtTW - 1) / kAtTW, tiles_y = (sub_h + kAtTH - 1) / kAtTH;
       const long long blocks = tiles_x * tiles_y * A.step * A.step;

@@ -389,6 +389,25 @@ __device__ __forceinline__ bool slab1(float3 bmin, float3 bmax, float3 o, float3
   return tx >= te && tx >= 0.001f && te <= tmax;
 }
 
+// x / d rounded to nearest, the same float as the division, given r =
+// RN(1 / d): Markstein's correction step (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): q = RN(x r), the residual x - q d is exact in one FMA,
+// and RN(q + residual * r) is the correctly rounded quotient; a zero
+// residual means q * d = x exactly, so q is the quotient (this keeps the
+// sign of a zero x).  Requires 2^-30 <= d <= 2^30; with 2^-96 <= |x| <=
+// 2^90 every intermediate is then a normal float.  For other nonzero x
+// (and non-finite x) it divides.  Used where many quotients share one
+// divisor: the running means of a frame (d = frame + 1) and the edge-aware
+// filter's range terms (d = 2 sigma^2) and normalisation.
+__device__ __forceinline__ float div_by(float x, float d, float r) {
+  const float ax = fabsf(x);
+  if (!(ax <= 0x1p+90f) || (ax < 0x1p-96f && ax != 0.0f)) return x / d;
+  const float q = x * r;
+  const float res = __fmaf_rn(-q, d, x);
+  return res == 0.0f ? q : __fmaf_rn(res, r, q);
+}
+
 // Packed child word: >= 0 internal node index; < 0 leaf with
 // ~word = (first primitive << kLeafBits) | primitive count.
 constexpr int kLeafBits = 5;
@@ -750,92 +769,6 @@ __device__ __forceinline__ int bvh4_closest(const DevScene& S, float3 o, float3 
   return hit;
 }
 
-// Closest hit on the 4-wide tree for a warp of coherent rays (the camera
-// rays of one 8 x 4 pixel tile of one sample), traversed as one packet: the
-// whole warp walks a single node sequence, every node is fetched once for
-// the warp (one broadcast load instead of up to 32 divergent ones) and
-// lanes never diverge between node and leaf work.  A child is entered when
-// any lane's ray enters it before that lane's closest hit; children are
-// visited nearest first by the packet's smallest entry distance; a stacked
-// child is skipped on pop when that distance exceeds every lane's closest
-// hit.  Each lane tests the primitives of every visited leaf with the same
-// exact triangle test, so its closest hit is the one a single-ray traversal
-// finds (only the pick among exactly equal distances can differ).  All 32
-// lanes must call it together; `active` false lanes only take part in the
-// votes.
-__device__ __forceinline__ int bvh4_closest_packet(const DevScene& S, float3 o, float3 d, bool active, float& tmax,
-                                                   float& hu, float& hv, int* err) {
-  constexpr unsigned kFull = 0xffffffffu;
-  int stk_w[kStack];
-  float stk_t[kStack];
-  int sp = 0;
-  const float3 inv = make_inv_dir(d);
-  const float3 oinv = o * inv;
-  int hit = -1;
-  float te;
-  const bool root = active && S.n_nodes4 > 0 && slab1(S.root_min, S.root_max, o, inv, tmax, te);
-  if (!__any_sync(kFull, root)) return -1;
-  int word = 0;
-  int guard = 4 * S.n_nodes4 + 64;
-  for (;;) {
-    if (--guard < 0 || word >= S.n_nodes4) {
-      if (err && (threadIdx.x & 31) == 0) atomicOr(err, ERR_BAD_NODE);
-      return hit;
-    }
-    if (word >= 0) {
-      const float4* np = S.nodes4 + 8 * (size_t)word;
-      float4 q[8];
-#pragma unroll
-      for (int k = 0; k < 7; ++k) q[k] = __ldg(np + k);
-      float t[4];
-      int w[4];
-      slab4(q, inv, oinv, active ? tmax : -INFINITY, t, w);
-      // packet entry distance of each child: the smallest over the lanes
-      // that enter it (non-negative floats order as their bit patterns)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const unsigned tb = t[k] < INFINITY ? __float_as_uint(fmaxf(t[k], 0.0f)) : __float_as_uint(INFINITY);
-        t[k] = __uint_as_float(__reduce_min_sync(kFull, tb));
-      }
-      cswap(t, w, 0, 1);
-      cswap(t, w, 2, 3);
-      cswap(t, w, 0, 2);
-      cswap(t, w, 1, 3);
-      cswap(t, w, 1, 2);
-      if (t[0] < INFINITY) {
-#pragma unroll
-        for (int k = 3; k >= 1; --k)
-          if (t[k] < INFINITY) {
-            if (sp < kStack) {
-              stk_w[sp] = w[k];
-              stk_t[sp] = t[k];
-              ++sp;
-            } else if (err && (threadIdx.x & 31) == 0) {
-              atomicOr(err, ERR_STACK_OVERFLOW);
-            }
-          }
-        word = w[0];
-        continue;
-      }
-    } else {
-      const int first = leaf_first(word), cnt = leaf_count(word);
-      if (first + cnt > S.n_prims) {
-        if (err && (threadIdx.x & 31) == 0) atomicOr(err, ERR_BAD_NODE);
-        return hit;
-      }
-      if (active) leaf_closest(S, o, d, first, cnt, tmax, hu, hv, hit);
-    }
-    // farthest closest hit over the packet: a stacked child entered later
-    // than that cannot hold a closer hit for any lane
-    const float tw = __uint_as_float(__reduce_max_sync(kFull, active ? __float_as_uint(fmaxf(tmax, 0.0f)) : 0u));
-    while (sp > 0 && stk_t[sp - 1] > tw) --sp;
-    if (sp == 0) break;
-    --sp;
-    word = stk_w[sp];
-  }
-  return hit;
-}
-
 #ifndef RX_TRAV
 #define RX_TRAV 0
 #endif
@@ -1011,40 +944,6 @@ __device__ __forceinline__ SceneHit scene_closest(const DevScene& S, float3 o, f
   h.v = 0.0f;
   float u = 0.0f, v = 0.0f;
   int p = bvh_closest<EXACT>(S, o, d, t, u, v, err);
-  if (p >= 0) {
-    h.prim = p;
-    h.slot = -1;
-    h.u = u;
-    h.v = v;
-  }
-  h.t = t;
-  return h;
-}
-
-// scene_closest for a warp of coherent rays (see bvh4_closest_packet): the
-// linear object scan per lane, then the packet traversal of the 4-wide
-// tree; trees without a 4-wide copy (the reference's) fall back to the
-// per-ray traversal.  All 32 lanes call it; inactive lanes return a miss.
-template <bool EXACT>
-__device__ __forceinline__ SceneHit scene_closest_packet(const DevScene& S, float3 o, float3 d, bool active,
-                                                         int* err) {
-  if (EXACT || !S.nodes4) {
-    SceneHit h;
-    h.t = 1e9f;
-    h.prim = h.slot = -1;
-    h.u = h.v = 0.0f;
-    if (active) h = scene_closest<EXACT>(S, o, d, err);
-    return h;
-  }
-  SceneHit h;
-  int slot = -1;
-  float t = active ? objs_closest(S, o, d, slot) : 1e9f;
-  h.slot = slot;
-  h.prim = -1;
-  h.u = 0.0f;
-  h.v = 0.0f;
-  float u = 0.0f, v = 0.0f;
-  int p = bvh4_closest_packet(S, o, d, active, t, u, v, err);
   if (p >= 0) {
     h.prim = p;
     h.slot = -1;

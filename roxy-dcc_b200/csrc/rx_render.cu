@@ -431,13 +431,11 @@ __device__ __forceinline__ int shadow_item(const Src& src, const float4* __restr
 }
 
 // 1024 resident threads per SM (64 registers): traversal is latency bound,
-// and the extra warps hide more of it than the registers they cost.  The
-// camera (packet) launch gets 80 registers (768 threads), which it needs
-// to run without spills.
+// and the extra warps hide more of it than the registers they cost.
 // CAM: the bounce-0 launch of a single render (camera items, no shadow
 // rays); the other launches are compiled without that code.
 template <bool EXACT, class Src, int BS, bool CAM = false>
-__global__ void __launch_bounds__(BS, (CAM ? 768 : 1024) / BS)
+__global__ void __launch_bounds__(BS, 1024 / BS)
     k_extend(Src src, int b, const int* __restrict__ qin, int* counters, const float4* __restrict__ ray_o,
              const float4* __restrict__ ray_d, float4* __restrict__ hits, int sb, const float4* __restrict__ shadow,
              float4* __restrict__ rad, long long shadow_cap, int* err) {
@@ -462,22 +460,6 @@ __global__ void __launch_bounds__(BS, (CAM ? 768 : 1024) / BS)
     if (base >= total) break;
     int i = base + lane;
     int job = -1, rays_here = 0;
-    if constexpr (CAM) {
-      // camera rays (a CAM launch has no other items): the warp's 32 items
-      // are an 8 x 4 pixel tile of one sample, traced together as a packet
-      // (all lanes take part)
-      const bool act = i < n;
-      float3 o = f3(0.0f, 0.0f, 0.0f), d = f3(0.0f, 0.0f, 1.0f);
-      int p = 0;
-      if (act) p = src.camera_ray(i, fb, o, d);
-      const DevScene S = src.scene(act ? src.seg(p) : 0);
-      SceneHit h = scene_closest_packet<EXACT>(S, o, d, act, err);
-      if (act) {
-        int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
-        hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
-      }
-      continue;
-    }
     if (i < n) {
       float3 o, d;
       int p;
@@ -883,10 +865,11 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
       an = g;
       aa = make_float4(al.x, al.y, al.z, 0.0f);
     } else {
-      float F = (float)frame, F1 = (float)(frame + 1);
-      a = make_float4((a.x * F + s.x) / F1, (a.y * F + s.y) / F1, (a.z * F + s.z) / F1, 0.0f);
-      an = make_float4((an.x * F + g.x) / F1, (an.y * F + g.y) / F1, (an.z * F + g.z) / F1, (an.w * F + g.w) / F1);
-      aa = make_float4((aa.x * F + al.x) / F1, (aa.y * F + al.y) / F1, (aa.z * F + al.z) / F1, 0.0f);
+      const float F = (float)frame, F1 = (float)(frame + 1), r = __frcp_rn(F1);
+      auto mean = [&](float acc, float smp) { return div_by(acc * F + smp, F1, r); };
+      a = make_float4(mean(a.x, s.x), mean(a.y, s.y), mean(a.z, s.z), 0.0f);
+      an = make_float4(mean(an.x, g.x), mean(an.y, g.y), mean(an.z, g.z), mean(an.w, g.w));
+      aa = make_float4(mean(aa.x, al.x), mean(aa.y, al.y), mean(aa.z, al.z), 0.0f);
     }
   };
   // the wave's samples are read once: streaming loads, kU frames in flight

@@ -361,9 +361,9 @@ def test_float64_reference_accumulation_and_relmse():
 
 def test_benchmark_scene_same_randoms_as_oracle():
     """The benchmark scene (327,680-triangle displaced icosphere, 64 spheres
-    in the LBVH, quad light) at 160 x 90, 2 spp, depth 12: camera rays go
-    through the packet traversal of bounce 0, later bounces through the
-    per-ray traversal.  First-hit depth and normal guides follow the oracle
+    in the LBVH, quad light) at 160 x 90, 2 spp, depth 12, traced by the
+    renderer's own launches (camera rays made in bounce 0's extend kernel,
+    the 4-wide tree).  First-hit depth and normal guides follow the oracle
     pixel by pixel; radiance as in the other same-randoms tests."""
     world = workloads.displaced_icosphere_scene(160, 90)
     W, H = 160, 90

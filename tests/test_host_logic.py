@@ -251,3 +251,33 @@ def test_rel_mse_definition():
     assert rel_mse(ref, ref) == 0.0
     with pytest.raises(ValueError):
         rel_mse(np.zeros((2, 2, 3)), np.zeros((2, 3, 3)))
+
+
+def test_running_mean_quotient_equals_ieee_division():
+    """k_accumulate divides every channel of a frame's running mean by
+    d = frame + 1 as RN(x * RN(1/d)) plus one FMA correction step
+    (Markstein's), returning RN(x * RN(1/d)) itself when the residual is
+    zero; within the range where the kernel uses it (zeros included), that
+    is the correctly rounded quotient, the same float as x / d.  Checked with the
+    same IEEE operations on the host (libm fmaf), over random floats of the
+    accumulators' magnitudes and frame counts up to 2^16."""
+    import ctypes
+    import ctypes.util
+    libm = ctypes.CDLL(ctypes.util.find_library("m"))
+    libm.fmaf.restype = ctypes.c_float
+    libm.fmaf.argtypes = [ctypes.c_float] * 3
+    rng = np.random.default_rng(12)
+    f32 = np.float32
+    d_all = np.concatenate([np.arange(2, 200), rng.integers(200, 1 << 16, 300)]).astype(np.float32)
+    mags = np.float32(10.0) ** rng.uniform(-28, 28, 40000).astype(np.float32)
+    xs = (mags * rng.choice([-1, 1], 40000)).astype(np.float32)
+    xs[:4] = [0.0, -0.0, 1.0, -0.5]
+    bad = 0
+    for k, x in enumerate(xs):
+        d = d_all[k % len(d_all)]
+        r = f32(1.0) / d
+        q = f32(x * r)
+        res = f32(libm.fmaf(-q, d, x))
+        got = q if res == 0.0 else f32(libm.fmaf(res, r, q))
+        bad += int(got.view(np.uint32) != f32(x / d).view(np.uint32))
+    assert bad == 0

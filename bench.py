@@ -336,23 +336,22 @@ def run_ours(args):
     ext_bytes = 40.0 * max(ext_rays - cam_rays, 0) + 16.0 * min(cam_rays, ext_rays)
     ext_gbs = ext_bytes / (ext_ms / 1e3) / 1e9 if ext_ms > 0 else 0.0
     # k_shade: 272 B per ray, less the 48 B of ray state a camera ray does
-    # not read at bounce 0
+    # not read at bounce 0.  64 B of it (the hit triangle's normals and
+    # palette index, the material record) come from the scene, which stays
+    # in L2; the rest is path state streamed through HBM.
     shade_bytes = 272.0 * ext_rays - 48.0 * min(cam_rays, ext_rays)
     shade_gbs = shade_bytes / (shade_ms / 1e3) / 1e9 if shade_ms > 0 else 0.0
+    shade_hbm = shade_bytes - 64.0 * ext_rays
+    shade_hbm_gbs = shade_hbm / (shade_ms / 1e3) / 1e9 if shade_ms > 0 else 0.0
     # DRAM bytes per k_extend launch: ncu's DRAM bytes per closest-hit ray
     # (committed summary: one-pass DRAM counters over the 12 extend launches
     # of this frame) times the average rays per launch here (max_depth
     # launches per wave)
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic_extend.json")
     spf = max(1, min(w["spp"], WAVE_PATHS // (W * H)))
     ext_launches = w["max_depth"] * -(-w["spp"] // spf)
-    if os.path.exists(tfile):
-        try:
-            with open(tfile) as f:
-                traffic = json.load(f)["bytes_per_ray"] * ext_rays / ext_launches
-        except (OSError, ValueError, KeyError):
-            traffic = None
+    measured = _traffic()
+    traffic = measured["k_extend"] * ext_rays / ext_launches if "k_extend" in measured else None
+    shade_dram = measured.get("k_shade")
 
     # k_accumulate: one launch folds the wave's frames; per pixel it reads
     # each frame's sample radiance and first-hit guides (3 x 16 B) and reads
@@ -422,7 +421,12 @@ def run_ours(args):
                              "extend_ms_per_step": ext_ms, "extend_rays_per_step": ext_rays,
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
                                        "algorithmic_bytes_per_ray": shade_bytes / max(ext_rays, 1),
-                                       "ms_per_step": shade_ms},
+                                       "ms_per_step": shade_ms,
+                                       "hbm_streamed": {"achieved": shade_hbm_gbs, "frac": shade_hbm_gbs / peak,
+                                                        "bytes_per_ray": shade_hbm / max(ext_rays, 1),
+                                                        "note": "algorithmic bytes less the 64 B per ray read "
+                                                                "from the L2-resident scene"},
+                                       "dram_bytes_per_ray_small_case": shade_dram},
                              "accumulate": {"achieved": acc_gbs, "frac": acc_gbs / peak, "ms_per_step": acc_ms,
                                             "algorithmic_bytes_per_step": acc_bytes,
                                             "bytes": "per pixel 48 B x spp sample reads + 112 B running means"},
@@ -444,6 +448,18 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _traffic():
+    """DRAM bytes per unit of the hot kernels, from the committed ncu
+    summaries (profiles/traffic.json: captured on the 640x360 16-spp case of
+    the benchmark scene, per closest-hit ray for k_extend, per shaded ray
+    for k_shade)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return {k: float(v["bytes_per_unit"]) for k, v in json.load(f).items()}
+    except (OSError, ValueError, KeyError, TypeError):
+        return {}
 
 
 def _atrous_roofline(nat, acc, stream, dp, W, H, peak, dev, iters=10):
@@ -807,12 +823,24 @@ def run_serve(args):
     max_req = args.max_requests or (120 if c2 else 600)
     rng = np.random.default_rng(99)
     build_ms = []
+    # scenes are built by a pool of builder threads, each on a context of its
+    # own (its own stream and lock), so extraction and BVH builds overlap one
+    # another and the server's render steps
+    import threading
+    builders = threading.local()
+
+    def builder_ctx():
+        if not hasattr(builders, "ctx"):
+            builders.ctx = nat.Context(0)
+        return builders.ctx
 
     def fresh_request(world, W, H, spp, seed):
         def prepare():
             tb = time.perf_counter()
-            ds = build_device_scene(world, method="lbvh")
+            bctx = builder_ctx()
+            ds = build_device_scene(world, method="lbvh", ctx=bctx)
             ds.use_lights(False)
+            bctx.sync()
             cam = world.active_camera
             p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
                             1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
@@ -841,14 +869,18 @@ def run_serve(args):
         n = int(min(max(rate * args.duration, 20), max_req))
         reqs = all_reqs[:n]
         row = {"rate_rps": rate, "requests": n}
-        for name, kw in (("batched", dict(max_active=1024, step_paths=1 << 23)),
-                         ("plain", dict(max_active=1, step_paths=1 << 40))):
-            srv = RenderServer(hbm_budget=150e9, wave_paths=1 << 25, preview_frames=1, ctx=ctx, **kw)
-            poisson_run(srv, all_reqs[-4:], rate=rate, seed=1)  # warm
+        # steps and waves sized to the requests: 64 M paths (a third of a
+        # 1080p 64-spp request) for full-HD requests, 8 M for the mixed sizes
+        big = 1 << 26 if c2 else 1 << 23
+        for name, kw in (("batched", dict(max_active=1024, step_paths=big, wave_paths=max(big, 1 << 25))),
+                         ("plain", dict(max_active=1, step_paths=1 << 40, wave_paths=max(big, 1 << 25)))):
+            srv = RenderServer(hbm_budget=150e9, preview_frames=1, ctx=ctx, **kw)
+            threads = args.prepare_threads if fresh else 1
+            poisson_run(srv, all_reqs[-4:], rate=rate, seed=1, prepare_threads=threads)  # warm
             st0 = srv.stats()
             build_ms.clear()
             with ClockSampler(0) as clocks:
-                r = poisson_run(srv, reqs, rate=rate, seed=2)
+                r = poisson_run(srv, reqs, rate=rate, seed=2, prepare_threads=threads)
             st = srv.stats()
             srv.close()
             row[name] = {k: r[k] for k in ("preview_p50_ms", "preview_p99_ms", "final_p50_ms", "final_p99_ms",
@@ -867,6 +899,7 @@ def run_serve(args):
             "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": desc, "world_generation_s": gen_s, "rates_rps": rates,
+                       "prepare_threads": args.prepare_threads if fresh else 1,
                        "latency_from": "arrival (scene build included)" if fresh else "submission"},
             "sweep": rows,
             "speedup_vs_plain_at_top_rate": top["batched"]["throughput_rps"] / top["plain"]["throughput_rps"],
@@ -890,6 +923,8 @@ def main():
                     help="serve workload: requests per rate at most (0: 120 for c2 sizes, 600 for mixed)")
     ap.add_argument("--serve-scenes", default="fresh", choices=["fresh", "resident"],
                     help="serve workload: build each request's scene on arrival, or reuse resident scenes")
+    ap.add_argument("--prepare-threads", type=int, default=1,
+                    help="serve workload: threads building arriving requests' scenes (fresh scenes)")
     ap.add_argument("--serve-sizes", default="c2", choices=["c2", "mixed"],
                     help="serve workload: 1920x1080 64 spp per request, or 256^2-1024^2 x 1-64 spp")
     ap.add_argument("--no-cpu", action="store_true")

@@ -85,15 +85,17 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else float("nan")
 
 
-def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0):
+def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0, prepare_threads=1):
     """Submit `requests` with exponential inter-arrival times of mean
     1/rate.  A request is (NativeScene, RenderParams, frames), or a callable
     that returns one: it runs when the request arrives (building the
     request's scene, say), and the time it takes counts toward the
     request's latencies.  A second thread plays the client that waits for
     each final image, reads it if asked and releases the request as soon as
-    it is done, while arrivals continue.  Returns latency and throughput
-    figures (latencies from arrival)."""
+    it is done, while arrivals continue.  With prepare_threads > 1 callable
+    requests are prepared and submitted by that many worker threads, so one
+    slow preparation does not hold back the arrivals behind it.  Returns
+    latency and throughput figures (latencies from arrival)."""
     import queue
     import threading
     rng = np.random.default_rng(seed)
@@ -122,6 +124,25 @@ def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0)
 
     th = threading.Thread(target=collect, daemon=True)
     th.start()
+    lock = threading.Lock()
+
+    def arrive(req, t_arrival):
+        made = req() if callable(req) else req
+        scene, params, frames = made[:3]
+        # a request's latency runs from its arrival: the time spent behind
+        # earlier arrivals' preparation counts too
+        prep = time.perf_counter() - t_arrival
+        rid = server.submit(scene, params, frames)
+        with lock:
+            prep_s[rid] = prep
+            keep[rid] = made
+        ids.put(rid)
+
+    pool = None
+    if prepare_threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        pool = ThreadPoolExecutor(prepare_threads)
+    futures = []
     t_start = time.perf_counter()
     t_next = t_start
     try:
@@ -130,19 +151,19 @@ def poisson_run(server, requests, rate, seed=0, read_final=False, timeout=300.0)
             delay = t_next - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            made = req() if callable(req) else req
-            scene, params, frames = made[:3]
-            # a request's latency runs from its arrival: the time spent
-            # behind earlier arrivals' preparation counts too
-            prep = time.perf_counter() - t_next
-            rid = server.submit(scene, params, frames)
-            prep_s[rid] = prep
-            keep[rid] = made
-            ids.put(rid)
+            if pool is not None and callable(req):
+                futures.append(pool.submit(arrive, req, t_next))
+            else:
+                arrive(req, t_next)
+        for f in futures:
+            f.result()
     except Exception:
         ids.put(None)
         th.join()
         raise
+    finally:
+        if pool is not None:
+            pool.shutdown(wait=True)
     th.join()
     if errors:
         raise errors[0]

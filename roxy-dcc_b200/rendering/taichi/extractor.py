@@ -380,18 +380,21 @@ def _upload_textures(native, builder, textures):
     return sum(im.nbytes for im in imgs)
 
 
-def build_device_scene(world, method="lbvh", leaf_size=None):
+def build_device_scene(world, method="lbvh", leaf_size=None, ctx=None):
     """Extract `world` to a device scene with a BVH.  method "lbvh" (the
     renderer's) transforms IndexedMesh geometry on the device; "morton" and
     "median" go through GPUBVHBuilder's host flattening so that the
-    reference-format tree and ordered arrays stay available."""
+    reference-format tree and ordered arrays stay available.  `ctx`: the
+    context (device stream) that builds it, by default the device's shared
+    one; a scene built on another context of the same device can be
+    rendered and served by any of them once that context is synchronised."""
     textures = TextureTable()
     if method != "lbvh":
         batches, slots = collect(world, textures)
         builder = GPUBVHBuilder()
         if leaf_size is not None:
             builder.MAX_LEAF_SIZE = leaf_size
-        native = nat.NativeScene()
+        native = nat.NativeScene(ctx)
         native.set_objects(slot_arrays(slots) if slots else None)
         builder.build(batches, method=method, native=native)
         h2d = _upload_textures(native, builder, textures)
@@ -404,7 +407,7 @@ def build_device_scene(world, method="lbvh", leaf_size=None):
                  "bvh_leaf_size": builder.MAX_LEAF_SIZE if builder.triangle_count else 0}
         return DeviceScene.from_builder(builder, slots, stats, h2d_extra=h2d)
     leaf = 4 if leaf_size is None else int(leaf_size)
-    native = nat.NativeScene()
+    native = nat.NativeScene(ctx)
     builder = GPUBVHBuilder()  # palette bookkeeping only
     slots, total, light_tris, h2d, light_index = _extract_on_device(world, native, builder, textures)
     native.set_objects(slot_arrays(slots) if slots else None)

@@ -138,7 +138,9 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
     """Each request arrives as a world: its scene is extracted and its BVH
     built when it arrives, while earlier requests are rendering; the served
     image equals a solo render of the same world bit for bit, and the
-    scenes' device memory is charged and given back with the requests."""
+    scenes' device memory is charged and given back with the requests.  The
+    scenes are built on a second context of the device, as the serving
+    benchmark builds them."""
     import math
 
     from rendering.taichi.extractor import build_device_scene
@@ -146,10 +148,13 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
     worlds = [workloads.displaced_icosphere_scene(48, 27, subdiv=5, n_spheres=8, seed=3000 + k) for k in range(3)]
     specs = [(worlds[k % 3], 48 + 16 * (k % 2), 27 + 9 * (k % 2), 1 + k % 4, 100 + k) for k in range(8)]
 
+    bctx = nat.Context(0)  # scenes built on their own stream, as the serving bench does
+
     def request(world, W, H, spp, seed):
         def prepare():
-            ds = build_device_scene(world, method="lbvh")
+            ds = build_device_scene(world, method="lbvh", ctx=bctx)
             ds.use_lights(False)
+            bctx.sync()
             cam = world.active_camera
             p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
                             1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
@@ -174,7 +179,7 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
         ids.append((srv.submit(scene, p, spp), scene, p, spp, ds))
     for rid, scene, p, spp, _ in ids:
         srv.wait(rid, final=True, timeout=60)
-        acc = nat.Accumulator(p.width, p.height)
+        acc = nat.Accumulator(p.width, p.height, bctx)  # a solo render on the scene's own context
         acc.render(scene, p, spp)
         _check_same(srv, rid, [acc.read(w) for w in BUFS])
         srv.release(rid)

@@ -933,7 +933,9 @@ struct SceneHit {
   float u, v;
 };
 
-template <bool EXACT>
+// WIDE: the caller guarantees a 4-wide tree (only that traversal is
+// compiled in, which keeps the batch kernels within their registers).
+template <bool EXACT, bool WIDE = false>
 __device__ __forceinline__ SceneHit scene_closest(const DevScene& S, float3 o, float3 d, int* err) {
   SceneHit h;
   int slot;
@@ -943,7 +945,7 @@ __device__ __forceinline__ SceneHit scene_closest(const DevScene& S, float3 o, f
   h.u = 0.0f;
   h.v = 0.0f;
   float u = 0.0f, v = 0.0f;
-  int p = bvh_closest<EXACT>(S, o, d, t, u, v, err);
+  int p = WIDE ? bvh4_closest(S, o, d, t, u, v, err) : bvh_closest<EXACT>(S, o, d, t, u, v, err);
   if (p >= 0) {
     h.prim = p;
     h.slot = -1;
@@ -954,10 +956,10 @@ __device__ __forceinline__ SceneHit scene_closest(const DevScene& S, float3 o, f
   return h;
 }
 
-template <bool EXACT>
+template <bool EXACT, bool WIDE = false>
 __device__ __forceinline__ bool scene_any(const DevScene& S, float3 o, float3 d, float max_t, int* err) {
   if (objs_any(S, o, d, max_t)) return true;
-  return bvh_any<EXACT>(S, o, d, max_t, err);
+  return WIDE ? bvh4_any(S, o, d, max_t, err) : bvh_any<EXACT>(S, o, d, max_t, err);
 }
 
 }  // namespace rx

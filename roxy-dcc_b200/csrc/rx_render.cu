@@ -274,6 +274,7 @@ __device__ __forceinline__ long long camera_path(const RenderK& K, long long t, 
 
 struct SingleSrc {
   static constexpr bool kBatch = false;
+  static constexpr bool kWide = false;  // the traversal picks the 4-wide tree when the scene has one
   DevScene S;
   RenderK K;
   __device__ __forceinline__ int seg(long long) const { return 0; }
@@ -303,6 +304,7 @@ struct SingleSrc {
 
 struct BatchSrc {
   static constexpr bool kBatch = true;
+  static constexpr bool kWide = false;
   const int* pseg;  // segment of each path
   const WaveSeg* segs;
   const DevScene* scenes;
@@ -310,9 +312,8 @@ struct BatchSrc {
   const JobAcc* accs;
   unsigned long long* job_rays;  // rays traced per job in this wave
   __device__ __forceinline__ int seg(long long p) const { return __ldg(pseg + p); }
-  // Batches traverse the binary tree: with the 4-wide traversal inlined as
-  // well, the kernels spill at 64 registers and ran 7% slower (64 scenes),
-  // and 7% slower as well at 80 registers with 768 threads per SM.
+  // This source traverses the binary tree (BatchSrc4: the 4-wide one); a
+  // kernel with both traversals inlined spills at 64 registers.
   __device__ __forceinline__ DevScene scene(int si) const {
     DevScene s = scenes[segs[si].job];
     s.nodes4 = nullptr;
@@ -330,6 +331,13 @@ struct BatchSrc {
   __device__ __forceinline__ long long camera_items(int) const { return 0; }
   __device__ __forceinline__ int frame0() const { return 0; }
   __device__ __forceinline__ int camera_ray(long long, int, float3&, float3&) const { return 0; }
+};
+
+// A batch whose scenes all have a 4-wide tree (LBVH builds): extend traverses
+// that tree only.
+struct BatchSrc4 : BatchSrc {
+  static constexpr bool kWide = true;
+  __device__ __forceinline__ DevScene scene(int si) const { return scenes[segs[si].job]; }
 };
 
 // -------------------------------------------------------------------- kernels
@@ -418,7 +426,7 @@ __device__ __forceinline__ int shadow_item(const Src& src, const float4* __restr
   bool any = false;
   for (int k = 0; k < cnt; ++k) {
     float4 s0 = sp[3 * k], s1 = sp[3 * k + 1];
-    if (!scene_any<EXACT>(S, xyz(s0), xyz(s1), s0.w, err)) {
+    if (!scene_any<EXACT, Src::kWide>(S, xyz(s0), xyz(s1), s0.w, err)) {
       sum = any ? sum + xyz(sp[3 * k + 2]) : xyz(sp[3 * k + 2]);
       any = true;
     }
@@ -476,7 +484,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
         job = src.segs[si].job;
         rays_here = 1;
       }
-      SceneHit h = scene_closest<EXACT>(S, o, d, err);
+      SceneHit h = scene_closest<EXACT, Src::kWide>(S, o, d, err);
       int code = h.prim >= 0 ? h.prim : (h.slot >= 0 ? -(h.slot + 2) : -1);
       hits[i] = make_float4(h.t, __int_as_float(code), h.u, h.v);
     } else if (i < total) {
@@ -1601,22 +1609,33 @@ static std::vector<PlannedWave> plan_waves(const Batch* b, std::vector<WaveSeg>&
 }
 
 template <int BS>
-static void launch_extend_batch(Batch* B, const BatchSrc& src, int occ, int b, const int* qin, int sb) {
-  k_extend<false, BatchSrc, BS><<<occ, BS, 0, B->ctx->stream>>>(src, b, qin, B->counters.p, B->ray_o.p, B->ray_d.p,
-                                                               B->hits.p, sb, B->shadow.p, B->rad.p, B->shadow_cap,
-                                                               B->ctx->d_err);
+static void launch_extend_batch(Batch* B, const BatchSrc& src, bool wide, int occ, int b, const int* qin, int sb) {
+  auto go = [&](auto kernel, const auto& s) {
+    kernel<<<occ, BS, 0, B->ctx->stream>>>(s, b, qin, B->counters.p, B->ray_o.p, B->ray_d.p, B->hits.p, sb,
+                                           B->shadow.p, B->rad.p, B->shadow_cap, B->ctx->d_err);
+  };
+  if (wide) go(k_extend<false, BatchSrc4, BS>, BatchSrc4{src});
+  else go(k_extend<false, BatchSrc, BS>, src);
 }
 
-static int batch_ext_blocks(Ctx* ctx, int bs) {
-  if (bs == 64) return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 64>, 64);
-  if (bs == 256) return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 256>, 256);
-  return blocks_for(ctx, (const void*)k_extend<false, BatchSrc, 128>, 128);
+template <class S>
+static int batch_ext_blocks_t(Ctx* ctx, int bs) {
+  if (bs == 64) return blocks_for(ctx, (const void*)k_extend<false, S, 64>, 64);
+  if (bs == 256) return blocks_for(ctx, (const void*)k_extend<false, S, 256>, 256);
+  return blocks_for(ctx, (const void*)k_extend<false, S, 128>, 128);
+}
+
+static int batch_ext_blocks(Ctx* ctx, int bs, bool wide) {
+  return wide ? batch_ext_blocks_t<BatchSrc4>(ctx, bs) : batch_ext_blocks_t<BatchSrc>(ctx, bs);
 }
 
 static void enqueue_batch(Batch* B, const std::vector<PlannedWave>& waves, int* n_launch) {
   Ctx* ctx = B->ctx;
   cudaStream_t st = ctx->stream;
-  int occ_ext = batch_ext_blocks(ctx, B->ext_block);
+  // the 4-wide traversal when every scene of the batch has that tree
+  bool wide = true;
+  for (const BatchJob& j : B->jobs) wide = wide && j.sc->n_nodes4 > 0 && !j.sc->exact_slab;
+  int occ_ext = batch_ext_blocks(ctx, B->ext_block, wide);
   int occ_shade = blocks_for(ctx, (const void*)k_shade<BatchSrc>, 128);
   int launches = 0;
   for (const PlannedWave& w : waves) {
@@ -1628,9 +1647,9 @@ static void enqueue_batch(Batch* B, const std::vector<PlannedWave>& waves, int* 
                                                             B->counters.p);
     ++launches;
     auto ext = [&](int b, const int* qin, int sb) {
-      if (B->ext_block == 64) launch_extend_batch<64>(B, src, occ_ext, b, qin, sb);
-      else if (B->ext_block == 256) launch_extend_batch<256>(B, src, occ_ext, b, qin, sb);
-      else launch_extend_batch<128>(B, src, occ_ext, b, qin, sb);
+      if (B->ext_block == 64) launch_extend_batch<64>(B, src, wide, occ_ext, b, qin, sb);
+      else if (B->ext_block == 256) launch_extend_batch<256>(B, src, wide, occ_ext, b, qin, sb);
+      else launch_extend_batch<128>(B, src, wide, occ_ext, b, qin, sb);
       ++launches;
     };
     for (int b = 0; b < w.max_depth; ++b) {

@@ -823,24 +823,18 @@ def run_serve(args):
     max_req = args.max_requests or (120 if c2 else 600)
     rng = np.random.default_rng(99)
     build_ms = []
-    # scenes are built by a pool of builder threads, each on a context of its
-    # own (its own stream and lock), so extraction and BVH builds overlap one
-    # another and the server's render steps
-    import threading
-    builders = threading.local()
 
-    def builder_ctx():
-        if not hasattr(builders, "ctx"):
-            builders.ctx = nat.Context(0)
-        return builders.ctx
-
+    # A request's scene is built on the server's own context while holding
+    # its lock: the build waits for the step in flight, then runs alone at
+    # full speed and the next step waits for it.  (Built on other contexts,
+    # the build's ~100 small kernels and level read-backs interleaved with
+    # the steps' long launches and each build took ~50 ms under load.)
     def fresh_request(world, W, H, spp, seed):
         def prepare():
             tb = time.perf_counter()
-            bctx = builder_ctx()
-            ds = build_device_scene(world, method="lbvh", ctx=bctx)
-            ds.use_lights(False)
-            bctx.sync()
+            with ctx.hold():
+                ds = build_device_scene(world, method="lbvh", ctx=ctx)
+                ds.use_lights(False)
             cam = world.active_camera
             p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
                             1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
@@ -869,9 +863,10 @@ def run_serve(args):
         n = int(min(max(rate * args.duration, 20), max_req))
         reqs = all_reqs[:n]
         row = {"rate_rps": rate, "requests": n}
-        # steps and waves sized to the requests: 64 M paths (a third of a
-        # 1080p 64-spp request) for full-HD requests, 8 M for the mixed sizes
-        big = 1 << 26 if c2 else 1 << 23
+        # steps and waves sized to the requests: by default 32 M paths (a
+        # quarter of a 1080p 64-spp request, ~9 ms) for full-HD requests,
+        # 8 M for the mixed sizes; a scene build waits for the step in flight
+        big = args.serve_step_paths or (1 << 25 if c2 else 1 << 23)
         for name, kw in (("batched", dict(max_active=1024, step_paths=big, wave_paths=max(big, 1 << 25))),
                          ("plain", dict(max_active=1, step_paths=1 << 40, wave_paths=max(big, 1 << 25)))):
             srv = RenderServer(hbm_budget=150e9, preview_frames=1, ctx=ctx, **kw)
@@ -900,6 +895,7 @@ def run_serve(args):
             "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": desc, "world_generation_s": gen_s, "rates_rps": rates,
                        "prepare_threads": args.prepare_threads if fresh else 1,
+                       "step_paths": args.serve_step_paths or (1 << 25 if c2 else 1 << 23),
                        "latency_from": "arrival (scene build included)" if fresh else "submission"},
             "sweep": rows,
             "speedup_vs_plain_at_top_rate": top["batched"]["throughput_rps"] / top["plain"]["throughput_rps"],
@@ -923,6 +919,8 @@ def main():
                     help="serve workload: requests per rate at most (0: 120 for c2 sizes, 600 for mixed)")
     ap.add_argument("--serve-scenes", default="fresh", choices=["fresh", "resident"],
                     help="serve workload: build each request's scene on arrival, or reuse resident scenes")
+    ap.add_argument("--serve-step-paths", type=int, default=0,
+                    help="serve workload: paths per batched step (0: 2^25 for c2 sizes, 2^23 for mixed)")
     ap.add_argument("--prepare-threads", type=int, default=1,
                     help="serve workload: threads building arriving requests' scenes (fresh scenes)")
     ap.add_argument("--serve-sizes", default="c2", choices=["c2", "mixed"],

@@ -86,6 +86,15 @@ int rx_ctx_destroy(rx_ctx* ctx);
 const char* rx_last_error(const rx_ctx* ctx);
 int rx_ctx_sync(rx_ctx* ctx);       /* waits for the device; reports kernel error flags */
 void* rx_ctx_stream(rx_ctx* ctx); /* the cudaStream_t the library launches on */
+/* Holds the context's lock across several calls made by this thread (no
+ * reference counterpart: the reference is single-threaded).  Until
+ * rx_ctx_release, calls from other threads on this context -- a serving
+ * loop's render steps among them -- wait, while the holder's own calls
+ * proceed; a scene built under the hold is built without interleaving with
+ * other threads' work.  Holds nest; every hold needs its release, from the
+ * same thread. */
+int rx_ctx_hold(rx_ctx* ctx);
+int rx_ctx_release(rx_ctx* ctx);
 
 /* Scene state.  Replaces the module-global fields written by extract_scene
  * and GPUBVHBuilder.upload (rendering/taichi/fields.py:22-79,

@@ -187,6 +187,20 @@ int rx_ctx_destroy(rx_ctx* ctx) {
   return RX_OK;
 }
 
+int rx_ctx_hold(rx_ctx* ctx) {
+  if (!ctx) return RX_ERR_ARG;
+  ctx->c.hold_waiters.fetch_add(1);
+  ctx->c.mu.lock();
+  ctx->c.hold_waiters.fetch_sub(1);
+  return RX_OK;
+}
+
+int rx_ctx_release(rx_ctx* ctx) {
+  if (!ctx) return RX_ERR_ARG;
+  ctx->c.mu.unlock();
+  return RX_OK;
+}
+
 int rx_ctx_sync(rx_ctx* ctx) {
   if (!ctx) return RX_ERR_ARG;
   LOCK(&ctx->c);

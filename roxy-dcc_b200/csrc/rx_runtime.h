@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -20,6 +21,7 @@ struct Ctx {
   int num_sms = 148;
   std::string err;
   std::recursive_mutex mu;
+  std::atomic<int> hold_waiters{0};  // threads blocked in rx_ctx_hold (the serving loop lets them go first)
   int* d_err = nullptr;  // device error bits
   int conv_impl = 0;     // 0: warp-specialised tcgen05 where it fits, 1: mma.sync only, 2: tcgen05 streaming
 };

@@ -133,7 +133,12 @@ static void serve_loop(Server* S) {
       S->cv_work.wait_for(lk, std::chrono::milliseconds(5));
       continue;
     }
-    // device work: the context lock, not the server lock, is held
+    // device work: the context lock, not the server lock, is held.  A
+    // thread waiting in rx_ctx_hold (building a request's scene, say) goes
+    // first: the mutex is not fair, and this loop would otherwise re-take
+    // it step after step (bounded: at most ~0.5 s of 50-us yields).
+    for (int k = 0; k < 10000 && S->ctx->hold_waiters.load() > 0; ++k)
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
     std::vector<int> ok(plan.size(), 1);
     int rc = RX_OK;
     double t_start = S->now();

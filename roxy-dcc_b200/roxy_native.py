@@ -4,6 +4,7 @@ Every renderer, BVH and denoise entry point of this package goes through
 here.  There is no CPU fallback: if the library or a CUDA device is missing,
 `lib()` raises `NativeUnavailable` and the caller's operation fails.
 """
+import contextlib
 import ctypes
 import os
 import subprocess
@@ -124,6 +125,8 @@ _SIGS = {
     "rx_ctx_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "rx_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
     "rx_ctx_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_ctx_hold": ([ctypes.c_void_p], ctypes.c_int),
+    "rx_ctx_release": ([ctypes.c_void_p], ctypes.c_int),
     "rx_ctx_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "rx_scene_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "rx_scene_destroy": ([ctypes.c_void_p], ctypes.c_int),
@@ -288,6 +291,17 @@ class Context:
 
     def sync(self):
         self.check(lib().rx_ctx_sync(self.h))
+
+    @contextlib.contextmanager
+    def hold(self):
+        """Holds the context's lock for a block of calls from this thread:
+        other threads' calls on the context (a serving loop's steps) wait
+        until the block ends."""
+        self.check(lib().rx_ctx_hold(self.h))
+        try:
+            yield self
+        finally:
+            lib().rx_ctx_release(self.h)
 
     def close(self):
         if getattr(self, "h", None):

@@ -139,8 +139,9 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
     built when it arrives, while earlier requests are rendering; the served
     image equals a solo render of the same world bit for bit, and the
     scenes' device memory is charged and given back with the requests.  The
-    scenes are built on a second context of the device, as the serving
-    benchmark builds them."""
+    Poisson run builds each scene on the server's context under
+    rx_ctx_hold (as the serving benchmark does); the image check builds
+    them on a second context of the device."""
     import math
 
     from rendering.taichi.extractor import build_device_scene
@@ -148,13 +149,19 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
     worlds = [workloads.displaced_icosphere_scene(48, 27, subdiv=5, n_spheres=8, seed=3000 + k) for k in range(3)]
     specs = [(worlds[k % 3], 48 + 16 * (k % 2), 27 + 9 * (k % 2), 1 + k % 4, 100 + k) for k in range(8)]
 
-    bctx = nat.Context(0)  # scenes built on their own stream, as the serving bench does
+    bctx = nat.Context(0)  # a second context of the device
 
-    def request(world, W, H, spp, seed):
+    def request(world, W, H, spp, seed, own=False):
         def prepare():
-            ds = build_device_scene(world, method="lbvh", ctx=bctx)
-            ds.use_lights(False)
-            bctx.sync()
+            if own:  # on the server's context, holding its lock (as the serving bench builds)
+                ctx = nat.context()
+                with ctx.hold():
+                    ds = build_device_scene(world, method="lbvh", ctx=ctx)
+                    ds.use_lights(False)
+            else:
+                ds = build_device_scene(world, method="lbvh", ctx=bctx)
+                ds.use_lights(False)
+                bctx.sync()
             cam = world.active_camera
             p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, 12, int(world._use_sky), 0,
                             1, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
@@ -164,7 +171,7 @@ def test_requests_with_scenes_built_on_arrival_equal_solo_renders():
 
     srv = RenderServer(hbm_budget=8e9, max_active=4, step_paths=3000, wave_paths=1 << 16)
     base = srv.stats()["bytes_in_use"]
-    r = poisson_run(srv, [request(*s) for s in specs], rate=400.0, seed=3)
+    r = poisson_run(srv, [request(*s, own=True) for s in specs], rate=400.0, seed=3)
     assert r["requests"] == len(specs) and r["prepare_p50_ms"] > 0
     st = srv.stats()
     assert st["completed"] == len(specs) and st["failed"] == 0

@@ -373,3 +373,28 @@ def test_benchmark_scene_same_randoms_as_oracle():
     assert _agree(g["normal"], o["normal"], 1e-4) > 0.995
     assert _agree(g["radiance"], o["radiance"]) > 0.97
     assert abs(g["rays"] - o["rays"]) <= 0.01 * o["rays"]
+
+
+def test_cornell_configuration_same_randoms_as_oracle():
+    """The Cornell-box configuration at its own size: 256 x 256, 16 spp,
+    depth 8, NEE at every bounce, against the oracle pixel by pixel with the
+    same random numbers (and the ray count the reference would report)."""
+    world = workloads.cornell_box()
+    g = _gpu_render(world, 256, 256, 16, 8, dlmd=8, seed=2)
+    o = _oracle_render(world, 256, 256, 16, 8, dlmd=8, seed=2)
+    assert _agree(g["radiance"], o["radiance"]) > 0.97
+    assert _agree(g["depth"], o["depth"], 1e-5) > 0.999
+    assert abs(g["rays"] - o["rays"]) <= 0.002 * o["rays"]
+    assert abs(g["radiance"].mean() - o["radiance"].mean()) < 0.002 * o["radiance"].mean()
+
+
+def test_benchmark_configuration_quarter_frame_same_randoms_as_oracle():
+    """The benchmark scene at a quarter of its frame (960 x 540), 4 spp,
+    depth 12: 2.1 M paths through the renderer's own launches against the
+    oracle with the same random numbers."""
+    world = workloads.displaced_icosphere_scene(960, 540)
+    g = _gpu_render(world, 960, 540, 4, 12, dlmd=1, seed=6)
+    o = _oracle_render(world, 960, 540, 4, 12, dlmd=1, seed=6)
+    assert _agree(g["radiance"], o["radiance"]) > 0.97
+    assert _agree(g["depth"], o["depth"], 1e-5) > 0.999
+    assert abs(g["rays"] - o["rays"]) <= 0.002 * o["rays"]

@@ -1352,7 +1352,7 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
       int ne = 2;
       ne += 2 * p->max_depth;
       if (p->max_depth > 0 && p->max_depth - 1 < p->direct_light_max_depth && nl > 0) ne += 1;
-      ne += 1;
+      ne += 2;  // after accumulate, after finish
       for (int i = 1; i < ne; ++i) {
         float ms = 0.0f;
         CUDA_TRY(ctx, cudaEventElapsedTime(&ms, a->ev[i - 1], a->ev[i]));

@@ -24,6 +24,7 @@ namespace rx {
 
 // numpy's "reflect" padding for any offset (period 2(n - 1)).
 __device__ __forceinline__ int reflect_idx(int i, int n) {
+  if ((unsigned)i < (unsigned)n) return i;  // inside the image: no reflection
   if (n == 1) return 0;
   int period = 2 * (n - 1);
   i %= period;

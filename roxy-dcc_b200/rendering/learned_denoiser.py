@@ -276,16 +276,10 @@ def render_views(scene_world, device_scene, views, size, spp, max_depth=12, seed
     cam = scene_world.active_camera
     out = {k: [] for k in ("radiance", "albedo", "normal", "depth")}
     acc = nat.Accumulator(size, size)
-    for i, (pos, at) in enumerate(views):
-        pos = np.asarray(pos, np.float64)
-        fwd = np.asarray(at, np.float64) - pos
-        fwd /= np.linalg.norm(fwd)
-        right = np.cross(fwd, [0.0, 1.0, 0.0])
-        right /= np.linalg.norm(right)
-        up = np.cross(right, fwd)
+    for i, (at_pos, at) in enumerate(views):
+        pos, fwd, right, up = _look_at(at_pos, at)
         p = make_params(size, size, math.tan(math.radians(cam.fov) / 2), 1.0, max_depth, int(scene_world._use_sky), 0,
-                        1, 10.0, list(scene_world._background_color), list(pos), list(fwd), list(right), list(up),
-                        seed=seed + i)
+                        1, 10.0, list(scene_world._background_color), pos, fwd, right, up, seed=seed + i)
         acc.reset()
         if ref:
             acc.set_f64(True)
@@ -380,10 +374,20 @@ def train(net, data, steps=3000, batch=16, crop=128, lr=2e-3, seed=0, log_every=
     return hist
 
 
-def evaluate(net, world, width=1920, height=1080, spp=4, ref_spp=4096, max_depth=12, seed=77):
+def _look_at(pos, at):
+    pos = np.asarray(pos, np.float64)
+    fwd = np.asarray(at, np.float64) - pos
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, [0.0, 1.0, 0.0])
+    right /= np.linalg.norm(right)
+    return list(pos), list(fwd), list(right), list(np.cross(right, fwd))
+
+
+def evaluate(net, world, width=1920, height=1080, spp=4, ref_spp=4096, max_depth=12, seed=77, view=None):
     """relMSE of the noisy render, the 5-pass a-trous filter and the learned
-    denoiser against a float64 `ref_spp` render of the same view; plus the
-    learned denoiser's inference time (CUDA events, mean of 10 after 3)."""
+    denoiser against a float64 `ref_spp` render of the same view (the
+    world's camera, or `view` = (position, look-at point)); plus the learned
+    denoiser's inference time (CUDA events, mean of 10 after 3)."""
     torch = _torch()
     from rendering.quality import reference_render, rel_mse
     from rendering.taichi.extractor import build_device_scene
@@ -391,9 +395,12 @@ def evaluate(net, world, width=1920, height=1080, spp=4, ref_spp=4096, max_depth
     cam = world.active_camera
     ds = build_device_scene(world)
     ds.use_lights(False)
+    if view is None:
+        pos, fwd, right, up = list(cam.position), list(cam.forward), list(cam.right), list(cam.up)
+    else:
+        pos, fwd, right, up = _look_at(*view)
     p = make_params(width, height, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, max_depth,
-                    int(world._use_sky), 0, 1, 10.0, list(world._background_color), list(cam.position),
-                    list(cam.forward), list(cam.right), list(cam.up), seed=seed)
+                    int(world._use_sky), 0, 1, 10.0, list(world._background_color), pos, fwd, right, up, seed=seed)
     ref = reference_render(ds.native, p, ref_spp)
     acc = nat.Accumulator(width, height)
     acc.render(ds.native, p, spp)
@@ -421,14 +428,34 @@ def evaluate(net, world, width=1920, height=1080, spp=4, ref_spp=4096, max_depth
             "infer_tflops": flops / (ms / 1e3) / 1e12, "flops_per_frame": flops}
 
 
+HELD_OUT_SEEDS = tuple(range(4001, 4009))  # scene seeds never rendered for training
+
+
+def evaluate_held_out(net, seeds=HELD_OUT_SEEDS, spp=4, ref_spp=4096):
+    """`evaluate` on one orbit view of each held-out scene of the large-mesh
+    generator at 1920x1080: per-view relMSE of the noisy render, the a-trous
+    filter and the learned denoiser, and their means."""
+    import workloads
+    rows = []
+    for k, s in enumerate(seeds):
+        view = orbit_views(1, 9000 + s)[0]
+        r = evaluate(net, workloads.displaced_icosphere_scene(seed=s), spp=spp, ref_spp=ref_spp, seed=500 + k,
+                     view=view)
+        rows.append({"seed": s, **{m: r[m] for m in ("relmse_noisy", "relmse_atrous", "relmse_learned")}})
+    mean = {m: float(np.mean([r[m] for r in rows])) for m in ("relmse_noisy", "relmse_atrous", "relmse_learned")}
+    return {"views": rows, "mean": mean, "spp": spp, "ref_spp": ref_spp}
+
+
 def main():
     """Train on renderer-generated pairs and write the weights file."""
     import argparse
     import json
     import time
     ap = argparse.ArgumentParser()
-    ap.add_argument("--steps", type=int, default=3000)
-    ap.add_argument("--views", type=int, default=48)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--scenes", type=int, default=16, help="training scenes (seeds 3001, 3002, ...)")
+    ap.add_argument("--views", type=int, default=128, help="orbit views per training scene")
+    ap.add_argument("--spp-ref", type=int, default=1024, help="spp of the training targets")
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--eval", action="store_true")
     ap.add_argument("--infer", default=None, metavar="WxH",
@@ -450,18 +477,21 @@ def main():
         print(json.dumps({"infer": [w, h], "repeat": args.repeat}))
         return
     t0 = time.time()
-    data = make_training_set(views_per_scene=args.views)
+    data = make_training_set(scene_seeds=tuple(range(3001, 3001 + args.scenes)), views_per_scene=args.views,
+                             spp_ref=args.spp_ref)
     t_data = time.time() - t0
     net = Denoiser(seed=0)
     t0 = time.time()
     hist = train(net, data, steps=args.steps)
     t_train = time.time() - t0
     save_weights(net, args.out)
-    res = {"pairs": int(data["radiance"].shape[0]), "data_s": t_data, "train_s": t_train, "loss": hist}
+    res = {"pairs": int(data["radiance"].shape[0]), "spp_ref": args.spp_ref, "data_s": t_data, "train_s": t_train,
+           "loss": hist}
     if args.eval:
         import workloads
         net2 = Denoiser(weights=load_weights(args.out))
         res["eval"] = evaluate(net2, workloads.displaced_icosphere_scene())
+        res["held_out"] = evaluate_held_out(net2)
     print(json.dumps(res))
 
 

@@ -525,17 +525,54 @@ __global__ void k_lbvh_bottom_up(int n, const int* __restrict__ order, const int
   }
 }
 
+// Breadth-first level walks run without a host round trip per level: the
+// walk's state lives on the device -- lv[0] nodes of the level being laid
+// out, lv[1] output index of its first node, lv[2] nodes queued for the next
+// level, lv[3] blocks of the current launch that have finished, lv[4] levels
+// laid out -- and the last block of each level launch advances it for the
+// next launch.  Every block reads lv[0] and lv[1] before it counts itself
+// finished, so the advance never races with a reader.  A launch that finds
+// lv[0] == 0 (the walk is over) returns at once; the host enqueues levels in
+// batches and reads lv back once per batch.
+enum { LV_NCUR = 0, LV_BASE = 1, LV_NEXT = 2, LV_DONE = 3, LV_LEVELS = 4, LV_N = 8 };
+
+__device__ __forceinline__ void level_advance(int* lv) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&lv[LV_DONE], 1) == (int)gridDim.x - 1) {
+      const int ncur = lv[LV_NCUR];
+      lv[LV_BASE] += ncur;
+      lv[LV_NCUR] = atomicAdd(&lv[LV_NEXT], 0);
+      lv[LV_NEXT] = 0;
+      lv[LV_DONE] = 0;
+      lv[LV_LEVELS] += 1;
+      __threadfence();
+    }
+  }
+}
+
 // One breadth-first level of the collapsed tree.  `cur` holds Karras node
-// ids; their output indices are out_base + position.  Kept internal children
+// ids; their output indices are base + position.  Kept internal children
 // are appended to `next` and receive indices in the following level.
-__global__ void k_lbvh_layout_level(const int* __restrict__ cur, int ncur, int out_base, int* __restrict__ next,
-                                    int* __restrict__ next_count, int next_base, int next_cap,
-                                    const int* __restrict__ kl,
+__global__ void k_lbvh_layout_level(const int* __restrict__ cur, int* __restrict__ next, int* __restrict__ lv,
+                                    int n_total, int* __restrict__ err, const int* __restrict__ kl,
                                     const int* __restrict__ kr, const int* __restrict__ first,
                                     const int* __restrict__ last, const int* __restrict__ collapse,
                                     const int* __restrict__ order, const float3* __restrict__ pmin,
                                     const float3* __restrict__ pmax, const float3* __restrict__ imin,
                                     const float3* __restrict__ imax, float4* __restrict__ out) {
+  const int ncur = lv[LV_NCUR], out_base = lv[LV_BASE];
+  if (ncur <= 0) return;
+  if (out_base + ncur > n_total) {  // cannot happen for a tree of n_total nodes
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      atomicOr(err, ERR_BAD_NODE);
+      lv[LV_NCUR] = 0;
+    }
+    return;
+  }
+  const int next_base = out_base + ncur, next_cap = n_total - next_base;
+  int* next_count = &lv[LV_NEXT];
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ncur; q += gridDim.x * blockDim.x) {
     int node = cur[q];
     int words[2], counts[2];
@@ -567,6 +604,7 @@ __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int ncur, int o
     o[3] = make_float4(__int_as_float(words[0]), __int_as_float(words[1]), __int_as_float(counts[0]),
                        __int_as_float(counts[1]));
   }
+  level_advance(lv);
 }
 
 // 4-wide nodes from the laid-out binary tree, one level per launch.  The
@@ -578,10 +616,19 @@ __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int ncur, int o
 // icosphere).  Leaf children stay leaves; internal children that remain
 // become 4-wide nodes of the next level.  Empty binary slots (count 0
 // leaves) are dropped; unused slots get a box at 1e30 and count 0.
-__global__ void k_bvh4_level(const int* __restrict__ cur, int ncur, int* __restrict__ next,
-                             int* __restrict__ next_count, int next_base, int next_cap,
-                             const float4* __restrict__ bin, int n_bin, float4* __restrict__ out4, int out_base,
-                             int* err) {
+__global__ void k_bvh4_level(const int* __restrict__ cur, int* __restrict__ next, int* __restrict__ lv,
+                             const float4* __restrict__ bin, int n_bin, float4* __restrict__ out4, int* err) {
+  const int ncur = lv[LV_NCUR], out_base = lv[LV_BASE];
+  if (ncur <= 0) return;
+  if (out_base + ncur > n_bin) {  // a 4-wide tree has at most as many nodes as the binary one
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      atomicOr(err, ERR_BAD_NODE);
+      lv[LV_NCUR] = 0;
+    }
+    return;
+  }
+  const int next_base = out_base + ncur, next_cap = n_bin - next_base;
+  int* next_count = &lv[LV_NEXT];
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ncur; q += gridDim.x * blockDim.x) {
     float mn[4][3], mx[4][3];
     int wd[4], ct[4];
@@ -667,6 +714,7 @@ __global__ void k_bvh4_level(const int* __restrict__ cur, int ncur, int* __restr
     o[6] = make_float4(__int_as_float(wd[0]), __int_as_float(wd[1]), __int_as_float(wd[2]), __int_as_float(wd[3]));
     o[7] = make_float4(__int_as_float(ct[0]), __int_as_float(ct[1]), __int_as_float(ct[2]), __int_as_float(ct[3]));
   }
+  level_advance(lv);
 }
 
 // Root record for a tree that is a single leaf of `cnt` primitives.
@@ -840,6 +888,44 @@ int set_reference_nodes(Ctx* ctx, Scene* sc, int n_nodes, const float* node_min,
   return RX_OK;
 }
 
+// Runs a device-driven level walk: `launch(level, cur, next, lv)` enqueues
+// one level (cur / next alternate between a and b); levels are enqueued in
+// batches of kLevelBatch and the state is read back once per batch.  The
+// root (node 0) is the only node of level 0.  Returns the total nodes laid
+// out through *n_out and the number of levels through *levels.
+constexpr int kLevelBatch = 16, kMaxLevels = 1024;
+template <class F>
+static int level_walk(Ctx* ctx, int* a, int* b, int* lv, int* n_out, int* levels, F launch) {
+  cudaStream_t st = ctx->stream;
+  const int init[LV_N] = {1, 0, 0, 0, 0, 0, 0, 0};
+  CUDA_TRY(ctx, cudaMemsetAsync(a, 0, sizeof(int), st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(lv, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  int h[LV_N] = {0};
+  int derr = 0;
+  for (int level = 0;;) {
+    for (int k = 0; k < kLevelBatch; ++k, ++level) launch(level, (level & 1) ? b : a, (level & 1) ? a : b, lv);
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaMemcpyAsync(h, lv, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&derr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (derr & ERR_BAD_NODE) return set_error(ctx, "BVH level walk: a level overflowed the tree"), RX_ERR_DEVICE;
+    if (h[LV_NCUR] == 0) break;
+    if (level >= kMaxLevels) return set_error(ctx, "BVH level walk did not terminate"), RX_ERR_DEVICE;
+  }
+  *n_out = h[LV_BASE];
+  *levels = h[LV_LEVELS];
+  return RX_OK;
+}
+
+// Blocks for level `level` of a tree whose nodes have up to `fan` children:
+// at most fan^level nodes, and never more than the whole tree's n.
+static int level_grid(Ctx* ctx, int level, int fan_log2, long long n) {
+  const long long bound = level * fan_log2 >= 40 ? n : std::min<long long>(n, 1LL << (level * fan_log2));
+  long long g = (bound + 255) / 256;
+  const long long cap = (long long)ctx->num_sms * 32;
+  return (int)std::max<long long>(1, std::min(g, cap));
+}
+
 // The 4-wide copy of the laid-out binary tree (k_bvh4_level, level by
 // level from the root, breadth first).
 static int build_wide(Ctx* ctx, Scene* sc) {
@@ -848,24 +934,14 @@ static int build_wide(Ctx* ctx, Scene* sc) {
   sc->n_nodes4 = 0;
   if (nb <= 0) return RX_OK;
   if (!sc->d_nodes4.alloc(ctx, (size_t)8 * nb)) return set_error(ctx, "out of device memory for the 4-wide BVH"), RX_ERR_CAPACITY;
-  DevBuf<int> la(ctx, nb), lb(ctx, nb), cnt(ctx, 1);
-  if (!la.p || !lb.p || !cnt.p) return set_error(ctx, "out of device memory"), RX_ERR_CAPACITY;
-  CUDA_TRY(ctx, cudaMemsetAsync(la.p, 0, sizeof(int), st));  // level 0: binary root 0
-  int ncur = 1, base = 0;
-  int* cur = la.p;
-  int* nxt = lb.p;
-  while (ncur > 0) {
-    if (base + ncur > nb) return set_error(ctx, "4-wide BVH: level walk did not terminate"), RX_ERR_DEVICE;
-    CUDA_TRY(ctx, cudaMemsetAsync(cnt.p, 0, sizeof(int), st));
-    k_bvh4_level<<<grid_for(ctx, ncur), 256, 0, st>>>(cur, ncur, nxt, cnt.p, base + ncur, nb - base - ncur,
-                                                       sc->d_nodes.p, nb, sc->d_nodes4.p, base, ctx->d_err);
-    int h = 0;
-    CUDA_TRY(ctx, cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    base += ncur;
-    ncur = h;
-    std::swap(cur, nxt);
-  }
+  DevBuf<int> la(ctx, nb), lb(ctx, nb), lv(ctx, LV_N);
+  if (!all_ok(la, lb, lv)) return set_error(ctx, "out of device memory"), RX_ERR_CAPACITY;
+  int base = 0, levels = 0;
+  int rc = level_walk(ctx, la.p, lb.p, lv.p, &base, &levels, [&](int level, int* cur, int* nxt, int* st_lv) {
+    k_bvh4_level<<<level_grid(ctx, level, 2, nb), 256, 0, st>>>(cur, nxt, st_lv, sc->d_nodes.p, nb, sc->d_nodes4.p,
+                                                              ctx->d_err);
+  });
+  if (rc) return rc;
   sc->n_nodes4 = base;
   return RX_OK;
 }
@@ -971,31 +1047,22 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
       sc->n_nodes = 1;
     } else {
       sc->d_nodes.alloc(ctx, (size_t)4 * n_int);
-      DevBuf<int> la(ctx, n_int), lb(ctx, n_int), cnt(ctx, 1);
-      if (!all_ok(sc->d_nodes, la, lb, cnt)) {
+      DevBuf<int> la(ctx, n_int), lb(ctx, n_int), lv(ctx, LV_N);
+      if (!all_ok(sc->d_nodes, la, lb, lv)) {
         sc->clear_bvh();
         return set_error(ctx, "LBVH: out of device memory"), RX_ERR_CAPACITY;
       }
-      int zero = 0;
-      cudaMemcpyAsync(la.p, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
-      int ncur = 1, base = 0;
-      int* cur = la.p;
-      int* nxt = lb.p;
-      while (ncur > 0) {
-        if (sc->depth > 1024 || base + ncur > n_int)
-          return set_error(ctx, "LBVH layout: level walk did not terminate"), RX_ERR_DEVICE;
-        cudaMemsetAsync(cnt.p, 0, sizeof(int), st);
-        k_lbvh_layout_level<<<grid_for(ctx, ncur), 256, 0, st>>>(cur, ncur, base, nxt, cnt.p, base + ncur, n_int, kl.p,
-                                                                  kr.p, first.p, last.p, collapse.p, order.p,
-                                                                  pmin.p, pmax.p, imin.p, imax.p, sc->d_nodes.p);
-        int h = 0;
-        cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st);
-        CUDA_TRY(ctx, cudaStreamSynchronize(st));
-        base += ncur;
-        ncur = h;
-        std::swap(cur, nxt);
-        sc->depth++;
+      int base = 0, levels = 0;
+      int rc = level_walk(ctx, la.p, lb.p, lv.p, &base, &levels, [&](int level, int* cur, int* nxt, int* st_lv) {
+        k_lbvh_layout_level<<<level_grid(ctx, level, 1, n_int), 256, 0, st>>>(
+            cur, nxt, st_lv, n_int, ctx->d_err, kl.p, kr.p, first.p, last.p, collapse.p, order.p, pmin.p, pmax.p,
+            imin.p, imax.p, sc->d_nodes.p);
+      });
+      if (rc) {
+        sc->clear_bvh();
+        return rc;
       }
+      sc->depth = levels;
       sc->n_nodes = base;
     }
   }

@@ -218,7 +218,10 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
             "config": {"workload": w["desc"], "impl_note": "CPU restatement of the reference Taichi path "
-                                                           "(oracle, C++/OpenMP); Taichi is not installable"},
+                                                           "(oracle, C++/OpenMP); Taichi is not installable"
+                                                           + ("; times the trace only: the reference has no "
+                                                              "multi-pass a-trous filter" if w.get("denoise_passes")
+                                                              else "")},
             "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": vals[0]["cores"], "kind": "port",
                              "sample": vals[0]["sample"]},
             "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -1,5 +1,24 @@
 """Scene graph node: shapes, a TRS transform and children."""
+import math
+
 from core import Color, RotationOrder, Transform, Vec3
+
+
+def _point(r, px, py, pz):
+    """Mat4x4.transform_point on rows `r`: the same operations, as a list."""
+    x = px * r[0][0] + py * r[0][1] + pz * r[0][2] + r[0][3]
+    y = px * r[1][0] + py * r[1][1] + pz * r[1][2] + r[1][3]
+    z = px * r[2][0] + py * r[2][1] + pz * r[2][2] + r[2][3]
+    w = px * r[3][0] + py * r[3][1] + pz * r[3][2] + r[3][3]
+    return [x / w, y / w, z / w] if w != 0 else [x, y, z]
+
+
+def _vec_len(r, vx, vy, vz):
+    """Mat4x4.transform_vector(...).length() on rows `r`, the same operations."""
+    x = vx * r[0][0] + vy * r[0][1] + vz * r[0][2]
+    y = vx * r[1][0] + vy * r[1][1] + vz * r[1][2]
+    z = vx * r[2][0] + vy * r[2][1] + vz * r[2][2]
+    return math.sqrt(x * x + y * y + z * z)
 
 
 class SceneObject:
@@ -105,17 +124,19 @@ class SceneObject:
         if shape is None:
             return []
         M = self.world_matrix
-        inv = self.world_inverse_matrix
         mat = self.material or Diffuse(Color(0.8, 0.8, 0.8))
         rec = self.material_record(mat)
         zero = [0.0, 0.0, 0.0]
         if isinstance(shape, Sphere):
-            c = list(M.transform_point(Vec3(0, 0, 0)))
-            s = max(M.transform_vector(Vec3(1, 0, 0)).length(), M.transform_vector(Vec3(0, 1, 0)).length(),
-                    M.transform_vector(Vec3(0, 0, 1)).length())
+            # M.transform_point(Vec3(0, 0, 0)) and the lengths of M applied to
+            # the unit axes, in the same arithmetic without the Vec3 objects
+            r = M.rows
+            c = _point(r, 0, 0, 0)
+            s = max(_vec_len(r, 1, 0, 0), _vec_len(r, 0, 1, 0), _vec_len(r, 0, 0, 1))
             return {"type": 0, "center": c, "radius": shape._radius * s, "normal": [0.0, 1.0, 0.0], "offset": 0.0,
                     "extra": zero, **rec}
         if isinstance(shape, Plane):
+            inv = self.world_inverse_matrix
             n = inv.transpose().transform_vector(shape._normal).normalize()
             d = shape._distance
             p = M.transform_point(Vec3(shape._normal.x * -d, shape._normal.y * -d, shape._normal.z * -d))

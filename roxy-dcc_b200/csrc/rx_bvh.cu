@@ -529,12 +529,13 @@ __global__ void k_lbvh_bottom_up(int n, const int* __restrict__ order, const int
 // walk's state lives on the device -- lv[0] nodes of the level being laid
 // out, lv[1] output index of its first node, lv[2] nodes queued for the next
 // level, lv[3] blocks of the current launch that have finished, lv[4] levels
-// laid out -- and the last block of each level launch advances it for the
+// laid out, lv[5] set when a level would overflow the tree -- and the last
+// block of each level launch advances it for the
 // next launch.  Every block reads lv[0] and lv[1] before it counts itself
 // finished, so the advance never races with a reader.  A launch that finds
 // lv[0] == 0 (the walk is over) returns at once; the host enqueues levels in
 // batches and reads lv back once per batch.
-enum { LV_NCUR = 0, LV_BASE = 1, LV_NEXT = 2, LV_DONE = 3, LV_LEVELS = 4, LV_N = 8 };
+enum { LV_NCUR = 0, LV_BASE = 1, LV_NEXT = 2, LV_DONE = 3, LV_LEVELS = 4, LV_OVERFLOW = 5, LV_N = 8 };
 
 __device__ __forceinline__ void level_advance(int* lv) {
   __syncthreads();
@@ -556,7 +557,7 @@ __device__ __forceinline__ void level_advance(int* lv) {
 // ids; their output indices are base + position.  Kept internal children
 // are appended to `next` and receive indices in the following level.
 __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int* __restrict__ next, int* __restrict__ lv,
-                                    int n_total, int* __restrict__ err, const int* __restrict__ kl,
+                                    int n_total, const int* __restrict__ kl,
                                     const int* __restrict__ kr, const int* __restrict__ first,
                                     const int* __restrict__ last, const int* __restrict__ collapse,
                                     const int* __restrict__ order, const float3* __restrict__ pmin,
@@ -566,7 +567,7 @@ __global__ void k_lbvh_layout_level(const int* __restrict__ cur, int* __restrict
   if (ncur <= 0) return;
   if (out_base + ncur > n_total) {  // cannot happen for a tree of n_total nodes
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      atomicOr(err, ERR_BAD_NODE);
+      lv[LV_OVERFLOW] = 1;
       lv[LV_NCUR] = 0;
     }
     return;
@@ -622,7 +623,7 @@ __global__ void k_bvh4_level(const int* __restrict__ cur, int* __restrict__ next
   if (ncur <= 0) return;
   if (out_base + ncur > n_bin) {  // a 4-wide tree has at most as many nodes as the binary one
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      atomicOr(err, ERR_BAD_NODE);
+      lv[LV_OVERFLOW] = 1;
       lv[LV_NCUR] = 0;
     }
     return;
@@ -901,14 +902,12 @@ static int level_walk(Ctx* ctx, int* a, int* b, int* lv, int* n_out, int* levels
   CUDA_TRY(ctx, cudaMemsetAsync(a, 0, sizeof(int), st));
   CUDA_TRY(ctx, cudaMemcpyAsync(lv, init, sizeof(init), cudaMemcpyHostToDevice, st));
   int h[LV_N] = {0};
-  int derr = 0;
   for (int level = 0;;) {
     for (int k = 0; k < kLevelBatch; ++k, ++level) launch(level, (level & 1) ? b : a, (level & 1) ? a : b, lv);
     CUDA_TRY(ctx, cudaGetLastError());
     CUDA_TRY(ctx, cudaMemcpyAsync(h, lv, sizeof(h), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(ctx, cudaMemcpyAsync(&derr, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    if (derr & ERR_BAD_NODE) return set_error(ctx, "BVH level walk: a level overflowed the tree"), RX_ERR_DEVICE;
+    if (h[LV_OVERFLOW]) return set_error(ctx, "BVH level walk: a level overflowed the tree"), RX_ERR_DEVICE;
     if (h[LV_NCUR] == 0) break;
     if (level >= kMaxLevels) return set_error(ctx, "BVH level walk did not terminate"), RX_ERR_DEVICE;
   }
@@ -1055,7 +1054,7 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
       int base = 0, levels = 0;
       int rc = level_walk(ctx, la.p, lb.p, lv.p, &base, &levels, [&](int level, int* cur, int* nxt, int* st_lv) {
         k_lbvh_layout_level<<<level_grid(ctx, level, 1, n_int), 256, 0, st>>>(
-            cur, nxt, st_lv, n_int, ctx->d_err, kl.p, kr.p, first.p, last.p, collapse.p, order.p, pmin.p, pmax.p,
+            cur, nxt, st_lv, n_int, kl.p, kr.p, first.p, last.p, collapse.p, order.p, pmin.p, pmax.p,
             imin.p, imax.p, sc->d_nodes.p);
       });
       if (rc) {

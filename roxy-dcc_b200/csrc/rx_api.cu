@@ -181,6 +181,7 @@ int rx_ctx_destroy(rx_ctx* ctx) {
   if (!ctx) return RX_OK;
   cudaSetDevice(ctx->c.device);
   cudaStreamSynchronize(ctx->c.stream);
+  host_stage_free(&ctx->c);
   cudaFree(ctx->c.d_err);
   cudaStreamDestroy(ctx->c.stream);
   delete ctx;

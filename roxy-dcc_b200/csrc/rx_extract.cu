@@ -162,15 +162,13 @@ int scene_put_triangles(Ctx* c, Scene* s, int offset, int n, const float* const*
            RX_ERR_ARG;
   if (n == 0) return RX_OK;
   float* dst[6] = {s->d_v0, s->d_v1, s->d_v2, s->d_n0, s->d_n1, s->d_n2};
-  for (int k = 0; k < 6; ++k) {
-    const float* src = rows[k] ? rows[k] : rows[0];
-    CUDA_TRY(c, cudaMemcpyAsync(dst[k] + (size_t)3 * offset, src, sizeof(float) * 3 * n, cudaMemcpyHostToDevice,
-                                c->stream));
-  }
-  if (mat_idx)
-    CUDA_TRY(c, cudaMemcpyAsync(s->d_tri_mat + offset, mat_idx, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
-  else
-    CUDA_TRY(c, cudaMemsetAsync(s->d_tri_mat + offset, 0, sizeof(int) * n, c->stream));
+  HostPiece up[7];
+  for (int k = 0; k < 6; ++k)
+    up[k] = {dst[k] + (size_t)3 * offset, rows[k] ? rows[k] : rows[0], sizeof(float) * 3 * (size_t)n};
+  if (mat_idx) up[6] = {s->d_tri_mat + offset, mat_idx, sizeof(int) * (size_t)n};
+  int rc = upload_staged(c, up, mat_idx ? 7 : 6);
+  if (rc) return rc;
+  if (!mat_idx) CUDA_TRY(c, cudaMemsetAsync(s->d_tri_mat + offset, 0, sizeof(int) * n, c->stream));
   ++s->version;
   return RX_OK;
 }
@@ -203,22 +201,37 @@ int scene_put_indexed(Ctx* c, Scene* s, int offset, int n_tris, int n_pos, const
   }
   DevBuf<double> d_pos, d_nrm;
   DevBuf<int> d_tri_pos, d_tri_nrm, d_group, d_group_mat, d_err;
-  int rc;
-  if ((rc = upload_tmp(c, d_pos, positions, (size_t)3 * n_pos)) ||
-      (rc = upload_tmp(c, d_tri_pos, tri_pos_idx, (size_t)3 * n_tris)) ||
-      (rc = upload_tmp(c, d_group_mat, group_mat, (size_t)n_groups)) || (rc = upload_tmp(c, d_err, (int*)nullptr, 1)))
-    return rc;
-  if (A.n_nrm > 0) {
-    if ((rc = upload_tmp(c, d_nrm, normals, (size_t)3 * n_nrm)) ||
-        (rc = upload_tmp(c, d_tri_nrm, tri_nrm_idx, (size_t)3 * n_tris)))
-      return rc;
+  const bool has_n = A.n_nrm > 0;
+  d_pos.alloc(c, (size_t)3 * std::max(n_pos, 1));
+  d_tri_pos.alloc(c, (size_t)3 * n_tris);
+  d_group_mat.alloc(c, (size_t)n_groups);
+  d_err.alloc(c, 1);
+  if (has_n) {
+    d_nrm.alloc(c, (size_t)3 * n_nrm);
+    d_tri_nrm.alloc(c, (size_t)3 * n_tris);
+  }
+  if (tri_group_idx) d_group.alloc(c, (size_t)n_tris);
+  if (!all_ok(d_pos, d_tri_pos, d_group_mat, d_err, d_nrm, d_tri_nrm, d_group))
+    return set_error(c, "put_indexed: out of device memory for %d triangles", n_tris), RX_ERR_CAPACITY;
+  // one staged upload of every host array (about 52 B per triangle with
+  // normals and groups, plus 24 B per position and normal)
+  HostPiece up[6];
+  int nu = 0;
+  up[nu++] = {d_pos.p, positions, sizeof(double) * 3 * (size_t)n_pos};
+  up[nu++] = {d_tri_pos.p, tri_pos_idx, sizeof(int) * 3 * (size_t)n_tris};
+  up[nu++] = {d_group_mat.p, group_mat, sizeof(int) * (size_t)n_groups};
+  if (has_n) {
+    up[nu++] = {d_nrm.p, normals, sizeof(double) * 3 * (size_t)n_nrm};
+    up[nu++] = {d_tri_nrm.p, tri_nrm_idx, sizeof(int) * 3 * (size_t)n_tris};
     A.nrm = d_nrm.p;
     A.tri_nrm = d_tri_nrm.p;
   }
   if (tri_group_idx) {
-    if ((rc = upload_tmp(c, d_group, tri_group_idx, (size_t)n_tris))) return rc;
+    up[nu++] = {d_group.p, tri_group_idx, sizeof(int) * (size_t)n_tris};
     A.tri_group = d_group.p;
   }
+  int rc = upload_staged(c, up, nu);
+  if (rc) return rc;
   A.pos = d_pos.p;
   A.tri_pos = d_tri_pos.p;
   A.group_mat = d_group_mat.p;
@@ -265,13 +278,16 @@ int scene_put_uvs(Ctx* c, Scene* s, int offset, int n, const float* uv0, const f
     CUDA_TRY(c, cudaMemsetAsync(s->uvb.p, 0, s->uvb.bytes(), c->stream));
   }
   if (n == 0) return RX_OK;
-  DevBuf<float> d0, d1, d2;
+  DevBuf<float> d0(c, (size_t)2 * n), d1(c, (size_t)2 * n), d2(c, (size_t)2 * n);
   DevBuf<int> dh;
-  int rc;
-  if ((rc = upload_tmp(c, d0, uv0, (size_t)2 * n)) || (rc = upload_tmp(c, d1, uv1, (size_t)2 * n)) ||
-      (rc = upload_tmp(c, d2, uv2, (size_t)2 * n)))
-    return rc;
-  if (has_uv && (rc = upload_tmp(c, dh, has_uv, (size_t)n))) return rc;
+  if (has_uv) dh.alloc(c, (size_t)n);
+  if (!all_ok(d0, d1, d2, dh)) return set_error(c, "put_uvs: out of device memory"), RX_ERR_CAPACITY;
+  HostPiece up[4] = {{d0.p, uv0, sizeof(float) * 2 * (size_t)n},
+                     {d1.p, uv1, sizeof(float) * 2 * (size_t)n},
+                     {d2.p, uv2, sizeof(float) * 2 * (size_t)n},
+                     {dh.p, has_uv, sizeof(int) * (size_t)n}};
+  int rc = upload_staged(c, up, has_uv ? 4 : 3);
+  if (rc) return rc;
   int blocks = (int)std::min<long long>((n + 255) / 256, (long long)c->num_sms * 8);
   k_pack_uvs<<<blocks, 256, 0, c->stream>>>(n, d0.p, d1.p, d2.p, has_uv ? dh.p : nullptr, s->uvb.p + 2 * (size_t)offset);
   CUDA_TRY(c, cudaGetLastError());
@@ -323,13 +339,11 @@ int scene_get_triangles(Ctx* c, Scene* s, int offset, int n, float* const* rows,
            RX_ERR_ARG;
   if (n == 0) return RX_OK;
   const float* src[6] = {s->d_v0, s->d_v1, s->d_v2, s->d_n0, s->d_n1, s->d_n2};
+  int rc;
   for (int k = 0; k < 6; ++k)
-    if (rows[k])
-      CUDA_TRY(c, cudaMemcpyAsync(rows[k], src[k] + (size_t)3 * offset, sizeof(float) * 3 * n,
-                                  cudaMemcpyDeviceToHost, c->stream));
-  if (mat_idx)
-    CUDA_TRY(c, cudaMemcpyAsync(mat_idx, s->d_tri_mat + offset, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (rows[k] && (rc = download_staged(c, rows[k], src[k] + (size_t)3 * offset, sizeof(float) * 3 * (size_t)n)))
+      return rc;
+  if (mat_idx && (rc = download_staged(c, mat_idx, s->d_tri_mat + offset, sizeof(int) * (size_t)n))) return rc;
   return RX_OK;
 }
 

@@ -21,7 +21,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <thread>
 #include <vector>
 
 #include "rx_internal.cuh"
@@ -999,9 +998,6 @@ struct Accum {
   // denoise scratch
   DevBuf<float4> dn0, dn1, dn_out;
   int occ_ext = 0, occ_shade = 0;
-  // pinned staging for reads to the host (kept for the accumulator's life)
-  void* stage = nullptr;
-  size_t stage_bytes = 0;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -1010,50 +1006,13 @@ struct Accum {
   ~Accum() {
     drop_graph();
     for (auto e : ev) cudaEventDestroy(e);
-    if (stage) cudaFreeHost(stage);
   }
 };
 
-// Device buffer -> caller's host memory through the accumulator's pinned
-// staging buffer: one DMA at full PCIe rate, then a copy out on a few host
-// threads (a pageable destination would be staged by the driver in small
-// synchronous chunks instead).
+// Device buffer -> caller's host memory through the context's pinned buffer,
+// the DMA of later pieces overlapping the threaded copy-out of earlier ones.
 static int read_to_host(Accum* a, void* host_out, const void* dev, size_t bytes) {
-  Ctx* ctx = a->ctx;
-  if (bytes > a->stage_bytes) {
-    if (a->stage) cudaFreeHost(a->stage);
-    a->stage = nullptr;
-    a->stage_bytes = 0;
-    if (cudaHostAlloc(&a->stage, bytes, cudaHostAllocDefault) != cudaSuccess) {
-      cudaGetLastError();
-      a->stage = nullptr;
-    } else {
-      a->stage_bytes = bytes;
-    }
-  }
-  if (!a->stage) {  // no pinned memory to be had: the driver's pageable path
-    CUDA_TRY(ctx, cudaMemcpyAsync(host_out, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    return RX_OK;
-  }
-  CUDA_TRY(ctx, cudaMemcpyAsync(a->stage, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  const size_t kPart = 4 << 20;
-  const int parts = (int)std::min<size_t>(8, (bytes + kPart - 1) / kPart);
-  if (parts <= 1) {
-    std::memcpy(host_out, a->stage, bytes);
-    return RX_OK;
-  }
-  const size_t chunk = (bytes + parts - 1) / parts;
-  std::vector<std::thread> th;
-  for (int i = 0; i < parts; ++i) {
-    const size_t off = (size_t)i * chunk;
-    if (off >= bytes) break;
-    const size_t n = std::min(chunk, bytes - off);
-    th.emplace_back([=] { std::memcpy(static_cast<char*>(host_out) + off, static_cast<const char*>(a->stage) + off, n); });
-  }
-  for (auto& t : th) t.join();
-  return RX_OK;
+  return download_staged(a->ctx, host_out, dev, bytes);
 }
 
 Accum* accum_new(Ctx* ctx, int w, int h) {

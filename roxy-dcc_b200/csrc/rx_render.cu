@@ -29,9 +29,13 @@
 namespace rx {
 
 constexpr int kMaxBounce = 64;
+// Default queue length at or below which k_tail runs a wave's remaining
+// bounces path by path (tuned on the 1080p benchmark frame).
+constexpr int kTailPaths = 1 << 16;
 // counters, 64 per kind (one per bounce): queue lengths, extend fetch,
-// shade fetch, shadow record counts
-enum { C_Q = 0, C_FE = 64, C_FS = 128, C_S = 192, C_N = 256 };
+// shade fetch, shadow record counts; then the bounce + 1 at which k_tail
+// took the wave over (0: not taken) and k_tail's fetch counter
+enum { C_Q = 0, C_FE = 64, C_FS = 128, C_S = 192, C_TAIL = 256, C_FT = 257, C_N = 260 };
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kTwoPi = 6.283185307179586f;
 
@@ -451,6 +455,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
   // they share this launch instead of paying for a small one of their own.
   // Camera items (bounce 0 without k_generate): item i is camera path i of
   // the wave, its ray made here; this launch also sets the bounce-0 count.
+  // Nothing to do once k_tail has taken the wave over.
+  if (*(volatile int*)&counters[C_TAIL]) return;
   const long long cam_n = CAM ? src.camera_items(b) : 0;
   const int fb = cam_n ? src.frame0() : 0;
   if (cam_n && blockIdx.x == 0 && threadIdx.x == 0) counters[C_Q + 0] = (int)cam_n;
@@ -527,6 +533,242 @@ __device__ __forceinline__ int warp_append_n(int cnt, int* counter) {
   return base + x - cnt;
 }
 
+// Next-event estimation at a vertex (trace.py:23-93), shared by k_shade
+// (which writes shadow records) and k_tail (which traces them at once).
+// direct_light_mode "one": one light, picked uniformly in compat mode, by
+// the alias table otherwise.  nee_p: the point lights are sampled from.
+__device__ __forceinline__ bool nee_one(const DevScene& S, const RenderK& K, bool mis, PathRng& rng, float3 nee_p,
+                                        float3 nrm, float3 alb, float nee_scale, float3& dir, float& max_t,
+                                        float3& val) {
+  int li;
+  float w;
+  if (K.compat) {
+    int cnt = S.n_lights;
+    li = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)cnt), cnt - 1);
+    w = (float)cnt;
+  } else {
+    int nl = S.n_lights;
+    int col = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)nl), nl - 1);
+    li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
+    w = 1.0f / S.lights[li].pick_pdf;
+  }
+  float pdf;
+  bool ok = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir, max_t,
+                         val, pdf);
+  // MIS: this light sample against the BSDF lobe that NEE stands in for
+  // (density nee_scale * cos / pi)
+  if (ok && mis) val = val * mis_power(pdf * S.lights[li].pick_pdf, nee_scale * dot(nrm, dir) / kPi);
+  return ok;
+}
+
+// direct_light_mode "all": light li with its own random slots
+__device__ __forceinline__ bool nee_light(const DevScene& S, bool mis, PathRng& rng, int li, float3 nee_p, float3 nrm,
+                                          float3 alb, float nee_scale, float3& dir, float& max_t, float3& val) {
+  int s1 = SLOT_ALL_LIGHTS + 4 * li;
+  float pdf;
+  bool ok = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val, pdf);
+  if (ok && mis) val = val * mis_power(pdf, nee_scale * dot(nrm, dir) / kPi);
+  return ok;
+}
+
+// Radiance a visible shadow ray adds: the throughput before this vertex's
+// albedo times the light sample's value (times the glossy lobe's weight).
+__device__ __forceinline__ float3 nee_contribution(float3 thr_nee, float3 val, float nee_scale) {
+  float3 c = thr_nee * val;
+  if (nee_scale != 1.0f) c = c * nee_scale;
+  return c;
+}
+
+// One path vertex (trace.py:139-236): the ray (o, d) with throughput thr
+// and current index of refraction cur_ior met the hit record h = (t, code,
+// u, v); prev_w is the previous vertex's NEE weight (0: no NEE there, else
+// its BSDF density for MIS).  Returns the radiance to add, the next ray when
+// the path goes on, and what next-event estimation at this vertex needs.
+// k_shade runs it once per launch over a queue of paths, k_tail bounce after
+// bounce for one path; the arithmetic is the same for both.
+// `out` receives the first-hit guides (out.guides(normal + depth, albedo),
+// on a surface hit) and the next ray (out.next(origin, ior, direction, NEE
+// weight, throughput), when the path goes on) where they are formed, so
+// k_shade stores them at once instead of keeping them in registers.
+struct Vertex {
+  float3 add = {0.0f, 0.0f, 0.0f};
+  bool has_add = false;
+  bool hit = false;  // a surface was hit
+  bool alive = false;
+  bool do_nee = false;
+  float nee_scale = 1.0f;
+  float3 hit_p = {0.0f, 0.0f, 0.0f}, nrm = {0.0f, 0.0f, 1.0f}, alb = {0.0f, 0.0f, 0.0f}, thr_nee = {0.0f, 0.0f, 0.0f};
+};
+
+template <class Out>
+__device__ __forceinline__ void shade_vertex(const DevScene& S, const RenderK& K, bool mis, int b, bool last_bounce,
+                                             float3 o, float3 d, float3 thr, float cur_ior, float prev_w, float4 h,
+                                             PathRng& rng, Vertex& v, Out& out) {
+  const bool prev_nee = prev_w != 0.0f;
+  const int code = __float_as_int(h.y);
+  if (code == -1) {
+    // trace.py:154-159
+    float3 sky;
+    if (K.use_sky) {
+      float t = 0.5f * (d.y + 1.0f);
+      sky = f3(1.0f, 1.0f, 1.0f) * (1.0f - t) + f3(0.5f, 0.7f, 1.0f) * t;
+    } else {
+      sky = K.bg;
+    }
+    v.add = thr * sky;
+    v.has_add = true;
+    return;
+  }
+  float t = h.x;
+  float3 nn;
+  int m;
+  int src_tri = -1;
+  bool listed;
+  if (code >= 0) {
+    const float4* sp = S.shade + 3 * (size_t)code;
+    float4 pa = __ldg(S.prims + 3 * (size_t)code);
+    float4 s0 = __ldg(sp);
+    m = __float_as_int(s0.w);
+    if (__float_as_int(pa.w) == PRIM_TRI) {
+      float w = 1.0f - h.z - h.w;
+      float4 s1 = __ldg(sp + 1);
+      src_tri = __float_as_int(s1.w);
+      nn = normalized((xyz(s0) * w + xyz(s1) * h.z) + xyz(__ldg(sp + 2)) * h.w);
+    } else {
+      nn = analytic_normal(o + d * t, pa, __ldg(S.prims + 3 * (size_t)code + 1));
+    }
+    // triangles and spheres can be lights; cubes are not in the light list
+    listed = __float_as_int(pa.w) != PRIM_CUBE;
+  } else {
+    const ObjSlot& ob = S.objs[-code - 2];
+    m = ob.mat;
+    if (ob.type == 0) nn = normalized((o + d * t) - ob.center);
+    else if (ob.type == 1) nn = ob.normal;
+    else if (ob.type == 2) nn = cube_normal(o + d * t, ob.center, ob.extra);
+    else nn = normalized(cross(ob.v1 - ob.v0, ob.v2 - ob.v0));
+    listed = ob.type == 0;
+  }
+  bool front = dot(nn, d) < 0.0f;
+  if (!front) nn = -nn;
+  const float3 hit_p = o + d * t;
+  v.hit_p = hit_p;
+  float4 ma = __ldg(S.mat_a + m), mb = __ldg(S.mat_b + m);
+  int mt = __float_as_int(ma.w);
+  float3 albedo = xyz(ma);
+  float rough = mb.x, ior = mb.y, em = mb.z;
+  int tex = __float_as_int(mb.w);
+  if (src_tri >= 0 && tex >= 0) albedo = textured_albedo(S, src_tri, tex, h.z, h.w, albedo);
+  // textured emitters are left out of the light list (their radiance
+  // varies over the surface), so BSDF hits always count them
+  listed = listed && mt == 3 && em > 0.0f && !(src_tri >= 0 && tex >= 0);
+  v.hit = true;
+  out.guides(make_float4(nn.x, nn.y, nn.z, t), make_float4(albedo.x, albedo.y, albedo.z, 0.0f));
+  if (mt == 3) {
+    // trace.py:194-196; with NEE on the previous diffuse vertex the
+    // default estimator already counted this emitter, unless MIS
+    // shares it between the two samples
+    if (!(!K.compat && prev_nee && listed)) {
+      v.add = (thr * albedo) * em;
+      v.has_add = true;
+    } else if (mis) {
+      int li = -1;
+      if (code >= 0)
+        li = src_tri >= 0 ? __ldg(S.light_of_tri + src_tri)
+                          : __ldg(S.light_of_obj + __float_as_int(__ldg(S.shade + 3 * (size_t)code + 1).w));
+      else
+        li = __ldg(S.light_of_lin + (-code - 2));
+      if (li >= 0) {
+        // prev_w: density of this direction under the previous vertex's BSDF
+        const Light& L = S.lights[li];
+        float pl = light_dir_pdf(L, o, d, t) * (K.mode == 0 ? L.pick_pdf : 1.0f);
+        v.add = ((thr * albedo) * em) * mis_power(prev_w, pl);
+        v.has_add = true;
+      }
+    }
+    return;
+  }
+  bool nee_here = false;
+  bool can_nee = b < K.dlmd && S.n_lights > 0;
+  float3 nd = d;
+  if (mt == 0) {
+    if (can_nee) {
+      v.do_nee = true;
+      nee_here = true;
+    }
+    nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
+  } else if (mt == 1) {
+    float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
+    nd = normalized(reflect(d, nn) + ru * rough);
+  } else if (mt == 4) {
+    if (can_nee) {
+      v.do_nee = true;
+      v.nee_scale = rough;
+    }
+    if (rng.get(SLOT_LOBE) < rough) {
+      nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
+      nee_here = v.do_nee;
+    } else {
+      float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
+      nd = normalized(reflect(d, nn) + ru * rough);
+    }
+  } else if (mt == 2) {
+    float eta;
+    if (front) {
+      eta = cur_ior / ior;
+      cur_ior = ior;
+    } else {
+      eta = cur_ior / 1.0f;
+      cur_ior = 1.0f;
+    }
+    float c = fminf(-dot(d, nn), 1.0f);
+    float s = sqrtf(1.0f - c * c);
+    bool refl = eta * s > 1.0f;
+    if (!refl) refl = schlick(c, eta) > rng.get(SLOT_LOBE);
+    nd = refl ? reflect(d, nn) : refract(d, nn, eta);
+  }
+  v.thr_nee = thr;
+  thr = thr * albedo;
+  v.alb = albedo;
+  v.nrm = nn;
+  bool alive = true;
+  if (b > 2) {
+    float rr = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+    if (rng.get(SLOT_RR) > rr) alive = false;
+    else thr = thr / rr;
+  }
+  if (last_bounce) alive = false;
+  v.alive = alive;
+  if (alive) {
+    // w: 0 = no NEE here; with MIS the BSDF density of nd through the lobe
+    // NEE stands in for (nee_scale * cos / pi), else 1
+    float nee_w = 0.0f;
+    if (nee_here) nee_w = mis ? fmaxf(v.nee_scale * dot(nn, nd) / kPi, 1e-30f) : 1.0f;
+    out.next(hit_p + nn * 1e-4f, cur_ior, nd, nee_w, thr);
+  }
+}
+
+// k_shade's vertex output: guides of bounce 0 and the next ray go to the
+// path's state at once
+struct PathStateOut {
+  float4* gn;
+  float4* ga;
+  float4* ray_o;
+  float4* ray_d;
+  float4* thr;
+  int p, b;
+  __device__ __forceinline__ void guides(float4 n, float4 a) {
+    if (b == 0) {
+      gn[p] = n;
+      ga[p] = a;
+    }
+  }
+  __device__ __forceinline__ void next(float3 o, float ior, float3 d, float w, float3 t) {
+    ray_o[p] = make_float4(o.x, o.y, o.z, ior);
+    ray_d[p] = make_float4(d.x, d.y, d.z, w);
+    thr[p] = make_float4(t.x, t.y, t.z, 0.0f);
+  }
+};
+
 template <class Src>
 __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int b, const int* __restrict__ qin,
                                                int* __restrict__ qout, int* counters,
@@ -536,7 +778,9 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
                                                float4* __restrict__ ga, const float4* __restrict__ hits,
                                                float4* __restrict__ shadow, int* err) {
   // camera items: bounce 0 without k_generate (see k_extend); the path's
-  // state is the camera ray, unit throughput and no radiance yet
+  // state is the camera ray, unit throughput and no radiance yet.  Nothing
+  // to do once k_tail has taken the wave over.
+  if (*(volatile int*)&counters[C_TAIL]) return;
   const long long cam_n = src.camera_items(b);
   const int n = cam_n ? (int)cam_n : *(volatile int*)&counters[C_Q + b];
   const int fb = frame_base ? *frame_base : 0;
@@ -575,167 +819,29 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
         d4 = ray_d[p];
         t4 = thr_b[p];
       }
-      float4 h = hits[i];
-      float3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
-      float cur_ior = o4.w;
-      bool prev_nee = d4.w != 0.0f;
-      int code = __float_as_int(h.y);
+      const float4 h = hits[i];
       uint32_t pix_id, smp;
       src.locate(si, p, fb, pix_id, smp);
       rng.init(pix_id, smp, (uint32_t)b, K.seed);
-      float3 add = f3(0.0f, 0.0f, 0.0f);
-      bool has_add = false;
-      if (code == -1) {
-        // trace.py:154-159
-        float3 sky;
-        if (K.use_sky) {
-          float t = 0.5f * (d.y + 1.0f);
-          sky = f3(1.0f, 1.0f, 1.0f) * (1.0f - t) + f3(0.5f, 0.7f, 1.0f) * t;
-        } else {
-          sky = K.bg;
-        }
-        add = thr * sky;
-        has_add = true;
-        if (cam_n) {  // no first hit: empty guides
-          gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-      } else {
-        float t = h.x;
-        float3 nn;
-        int m;
-        int src_tri = -1;
-        bool listed;
-        if (code >= 0) {
-          const float4* sp = S.shade + 3 * (size_t)code;
-          float4 pa = __ldg(S.prims + 3 * (size_t)code);
-          float4 s0 = __ldg(sp);
-          m = __float_as_int(s0.w);
-          if (__float_as_int(pa.w) == PRIM_TRI) {
-            float w = 1.0f - h.z - h.w;
-            float4 s1 = __ldg(sp + 1);
-            src_tri = __float_as_int(s1.w);
-            nn = normalized((xyz(s0) * w + xyz(s1) * h.z) + xyz(__ldg(sp + 2)) * h.w);
-          } else {
-            nn = analytic_normal(o + d * t, pa, __ldg(S.prims + 3 * (size_t)code + 1));
-          }
-          // triangles and spheres can be lights; cubes are not in the light list
-          listed = __float_as_int(pa.w) != PRIM_CUBE;
-        } else {
-          const ObjSlot& ob = S.objs[-code - 2];
-          m = ob.mat;
-          if (ob.type == 0) nn = normalized((o + d * t) - ob.center);
-          else if (ob.type == 1) nn = ob.normal;
-          else if (ob.type == 2) nn = cube_normal(o + d * t, ob.center, ob.extra);
-          else nn = normalized(cross(ob.v1 - ob.v0, ob.v2 - ob.v0));
-          listed = ob.type == 0;
-        }
-        bool front = dot(nn, d) < 0.0f;
-        if (!front) nn = -nn;
-        hit_p = o + d * t;
-        float4 ma = __ldg(S.mat_a + m), mb = __ldg(S.mat_b + m);
-        int mt = __float_as_int(ma.w);
-        float3 albedo = xyz(ma);
-        float rough = mb.x, ior = mb.y, em = mb.z;
-        int tex = __float_as_int(mb.w);
-        if (src_tri >= 0 && tex >= 0) albedo = textured_albedo(S, src_tri, tex, h.z, h.w, albedo);
-        // textured emitters are left out of the light list (their radiance
-        // varies over the surface), so BSDF hits always count them
-        listed = listed && mt == 3 && em > 0.0f && !(src_tri >= 0 && tex >= 0);
-        if (b == 0) {
-          gn[p] = make_float4(nn.x, nn.y, nn.z, t);
-          ga[p] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
-        }
-        if (mt == 3) {
-          // trace.py:194-196; with NEE on the previous diffuse vertex the
-          // default estimator already counted this emitter, unless MIS
-          // shares it between the two samples
-          if (!( !K.compat && prev_nee && listed)) {
-            add = (thr * albedo) * em;
-            has_add = true;
-          } else if (mis) {
-            int li = -1;
-            if (code >= 0)
-              li = src_tri >= 0 ? __ldg(S.light_of_tri + src_tri)
-                                : __ldg(S.light_of_obj + __float_as_int(__ldg(S.shade + 3 * (size_t)code + 1).w));
-            else
-              li = __ldg(S.light_of_lin + (-code - 2));
-            if (li >= 0) {
-              // d4.w: density of this direction under the previous vertex's BSDF
-              const Light& L = S.lights[li];
-              float pl = light_dir_pdf(L, o, d, t) * (K.mode == 0 ? L.pick_pdf : 1.0f);
-              add = ((thr * albedo) * em) * mis_power(d4.w, pl);
-              has_add = true;
-            }
-          }
-        } else {
-          bool nee_here = false;
-          bool can_nee = b < K.dlmd && S.n_lights > 0;
-          float3 nd = d;
-          if (mt == 0) {
-            if (can_nee) {
-              do_nee = true;
-              nee_here = true;
-            }
-            nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
-          } else if (mt == 1) {
-            float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
-            nd = normalized(reflect(d, nn) + ru * rough);
-          } else if (mt == 4) {
-            if (can_nee) {
-              do_nee = true;
-              nee_scale = rough;
-            }
-            if (rng.get(SLOT_LOBE) < rough) {
-              nd = diffuse_scatter(nn, rng.get(SLOT_BSDF_U1), rng.get(SLOT_BSDF_U2));
-              nee_here = do_nee;
-            } else {
-              float3 ru = random_unit_vector(rng.get(SLOT_FUZZ_U1), rng.get(SLOT_FUZZ_U2));
-              nd = normalized(reflect(d, nn) + ru * rough);
-            }
-          } else if (mt == 2) {
-            float eta;
-            if (front) {
-              eta = cur_ior / ior;
-              cur_ior = ior;
-            } else {
-              eta = cur_ior / 1.0f;
-              cur_ior = 1.0f;
-            }
-            float c = fminf(-dot(d, nn), 1.0f);
-            float s = sqrtf(1.0f - c * c);
-            bool refl = eta * s > 1.0f;
-            if (!refl) refl = schlick(c, eta) > rng.get(SLOT_LOBE);
-            nd = refl ? reflect(d, nn) : refract(d, nn, eta);
-          }
-          thr_nee = thr;
-          thr = thr * albedo;
-          alb = albedo;
-          nrm = nn;
-          alive = true;
-          if (b > 2) {
-            float rr = fmaxf(thr.x, fmaxf(thr.y, thr.z));
-            if (rng.get(SLOT_RR) > rr) alive = false;
-            else thr = thr / rr;
-          }
-          if (last_bounce) alive = false;
-          if (alive) {
-            float3 no = hit_p + nn * 1e-4f;
-            ray_o[p] = make_float4(no.x, no.y, no.z, cur_ior);
-            // w: 0 = no NEE here; with MIS the BSDF density of nd through
-            // the lobe NEE stands in for (nee_scale * cos / pi), else 1
-            float nee_w = 0.0f;
-            if (nee_here) nee_w = mis ? fmaxf(nee_scale * dot(nn, nd) / kPi, 1e-30f) : 1.0f;
-            ray_d[p] = make_float4(nd.x, nd.y, nd.z, nee_w);
-            thr_b[p] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-          }
-        }
+      Vertex v;
+      PathStateOut out{gn, ga, ray_o, ray_d, thr_b, p, b};
+      shade_vertex(S, K, mis, b, last_bounce, xyz(o4), xyz(d4), xyz(t4), o4.w, d4.w, h, rng, v, out);
+      if (!v.hit && cam_n) {  // no first hit: empty guides
+        gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       }
+      alive = v.alive;
+      do_nee = v.do_nee;
+      nee_scale = v.nee_scale;
+      hit_p = v.hit_p;
+      nrm = v.nrm;
+      alb = v.alb;
+      thr_nee = v.thr_nee;
       if (cam_n) {
-        rad_b[p] = make_float4(add.x, add.y, add.z, 0.0f);  // the path's first radiance
-      } else if (has_add) {
+        rad_b[p] = make_float4(v.add.x, v.add.y, v.add.z, 0.0f);  // the path's first radiance
+      } else if (v.has_add) {
         float4 r = rad_b[p];
-        rad_b[p] = make_float4(r.x + add.x, r.y + add.y, r.z + add.z, 0.0f);
+        rad_b[p] = make_float4(r.x + v.add.x, r.y + v.add.y, r.z + v.add.z, 0.0f);
       }
     }
     // next-event estimation: shadow records for connect.  The default
@@ -748,8 +854,7 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
     // count = number of this path's records starting here (0 on followers)
     auto write_rec = [&](long long slot, float3 dir, float max_t, float3 val, int count) {
       float3 so = hit_p + nrm * 1e-4f;
-      float3 c = thr_nee * val;
-      if (nee_scale != 1.0f) c = c * nee_scale;
+      float3 c = nee_contribution(thr_nee, val, nee_scale);
       float4* sp = shadow + 3 * (size_t)slot;
       sp[0] = make_float4(so.x, so.y, so.z, max_t);
       sp[1] = make_float4(dir.x, dir.y, dir.z, __int_as_float(p));
@@ -758,33 +863,11 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
     // direct_light_mode "one": one light picked (uniformly in compat mode,
     // by the alias table otherwise)
     auto sample_one = [&](float3& dir, float& max_t, float3& val) {
-      int li;
-      float w;
-      if (K.compat) {
-        int cnt = S.n_lights;
-        li = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)cnt), cnt - 1);
-        w = (float)cnt;
-      } else {
-        int nl = S.n_lights;
-        int col = min((int)(rng.get(SLOT_LIGHT_PICK) * (float)nl), nl - 1);
-        li = rng.get(SLOT_LIGHT_ACCEPT) < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_idx + col);
-        w = 1.0f / S.lights[li].pick_pdf;
-      }
-      float pdf;
-      bool ok = light_sample(S.lights[li], rng.get(SLOT_LIGHT_U1), rng.get(SLOT_LIGHT_U2), nee_p, nrm, alb, w, dir,
-                             max_t, val, pdf);
-      // MIS: this light sample against the BSDF lobe that NEE stands in for
-      // (density nee_scale * cos / pi)
-      if (ok && mis) val = val * mis_power(pdf * S.lights[li].pick_pdf, nee_scale * dot(nrm, dir) / kPi);
-      return ok;
+      return nee_one(S, K, mis, rng, nee_p, nrm, alb, nee_scale, dir, max_t, val);
     };
     // direct_light_mode "all": light li with its own random slots
     auto sample_li = [&](int li, float3& dir, float& max_t, float3& val) {
-      int s1 = SLOT_ALL_LIGHTS + 4 * li;
-      float pdf;
-      bool ok = light_sample(S.lights[li], rng.get(s1), rng.get(s1 + 1), nee_p, nrm, alb, 1.0f, dir, max_t, val, pdf);
-      if (ok && mis) val = val * mis_power(pdf, nee_scale * dot(nrm, dir) / kPi);
-      return ok;
+      return nee_light(S, mis, rng, li, nee_p, nrm, alb, nee_scale, dir, max_t, val);
     };
     bool one_light = false;  // warp-uniform: one scene, mode "one"
     if constexpr (!Src::kBatch) one_light = K.mode == 0;
@@ -842,6 +925,124 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
       if (q < K.queue_cap) qout[q] = p;
       else atomicOr(err, ERR_QUEUE_OVERFLOW);
     }
+  }
+}
+
+// k_tail's vertex output: the next ray stays in registers (no guides: the
+// tail starts at bounce 1 or later)
+struct RegisterOut {
+  float3 o, d, t;
+  float ior, w;
+  __device__ __forceinline__ void guides(float4, float4) {}
+  __device__ __forceinline__ void next(float3 o_, float ior_, float3 d_, float w_, float3 t_) {
+    o = o_;
+    ior = ior_;
+    d = d_;
+    w = w_;
+    t = t_;
+  }
+};
+
+// The tail of a wave.  Launched after bounce b's k_extend (b >= 1): when that
+// bounce's queue holds at most `max_paths` paths, one thread per path shades
+// bounce b from the hit record k_extend wrote, then traces, shades and runs
+// next-event estimation for each of the path's remaining bounces itself,
+// tracing its shadow rays at once.  Late bounces hold few, incoherent rays,
+// and a one-bounce launch lasts as long as its slowest ray; this launch lasts
+// as long as its slowest path.  Radiance is added in the order of the
+// one-bounce launches (a bounce's emission, then its shadow rays, then the
+// next bounce's), with the same random numbers and arithmetic
+// (shade_vertex, nee_one / nee_light), so images and ray counts are the same
+// bit for bit.  The launch that takes over sets counters[C_TAIL] = b + 1;
+// the wave's later k_extend, k_shade and k_tail launches then return at once.
+template <bool EXACT, class Src>
+__global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restrict__ qin, int* counters,
+                                              int max_paths, const int* __restrict__ frame_base,
+                                              const float4* __restrict__ ray_o, const float4* __restrict__ ray_d,
+                                              const float4* __restrict__ thr_b, float4* __restrict__ rad_b,
+                                              const float4* __restrict__ hits, int* err) {
+  const int taken = *(volatile int*)&counters[C_TAIL];
+  if (taken != 0 && taken != b + 1) return;  // an earlier bounce's launch took over
+  const int n = *(volatile int*)&counters[C_Q + b];
+  if (n > max_paths) return;  // the one-bounce launches go on
+  // every block of this launch reads the same queue length and flag (0 or
+  // b + 1), so all of them take over
+  if (threadIdx.x == 0) counters[C_TAIL] = b + 1;
+  const int fb = frame_base ? *frame_base : 0;
+  const int lane = threadIdx.x & 31;
+  int n_closest = 0, n_shadow = 0;  // rays traced here, counted as the one-bounce launches count them
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&counters[C_FT], 32);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      const int p = qin[i];
+      const int si = src.seg(p);
+      const DevScene S = src.scene(si);
+      const RenderK K = src.params(si);
+      const bool mis = K.mis && S.light_of_lin != nullptr;
+      const float4 o4 = ray_o[p], d4 = ray_d[p], t4 = thr_b[p];
+      float3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
+      float ior = o4.w, w = d4.w;
+      float4 h = hits[i];
+      float4 r = rad_b[p];
+      uint32_t pix_id, smp;
+      src.locate(si, p, fb, pix_id, smp);
+      for (int bb = b;; ++bb) {
+        PathRng rng;
+        rng.init(pix_id, smp, (uint32_t)bb, K.seed);
+        Vertex v;
+        RegisterOut out;
+        shade_vertex(S, K, mis, bb, (bb + 1) >= K.max_depth, o, d, thr, ior, w, h, rng, v, out);
+        if (v.has_add) r = make_float4(r.x + v.add.x, r.y + v.add.y, r.z + v.add.z, 0.0f);
+        if (v.do_nee) {
+          // the shadow rays this vertex would have written as records, traced
+          // in record order and summed as the next extend launch sums them
+          const float3 nee_p = K.compat ? v.hit_p : v.hit_p + v.nrm * 1e-4f;
+          const float3 so = v.hit_p + v.nrm * 1e-4f;
+          float3 sum = f3(0.0f, 0.0f, 0.0f);
+          bool any = false;
+          auto shadow_ray = [&](float3 dir, float max_t, float3 val) {
+            ++n_shadow;
+            if (!scene_any<EXACT, Src::kWide>(S, so, dir, max_t, err)) {
+              const float3 c = nee_contribution(v.thr_nee, val, v.nee_scale);
+              sum = any ? sum + c : c;
+              any = true;
+            }
+          };
+          float3 dir, val;
+          float max_t;
+          if (K.mode == 0) {
+            if (nee_one(S, K, mis, rng, nee_p, v.nrm, v.alb, v.nee_scale, dir, max_t, val)) shadow_ray(dir, max_t, val);
+          } else {
+            for (int li = 0; li < S.n_lights; ++li)
+              if (nee_light(S, mis, rng, li, nee_p, v.nrm, v.alb, v.nee_scale, dir, max_t, val))
+                shadow_ray(dir, max_t, val);
+          }
+          if (any) r = make_float4(r.x + sum.x, r.y + sum.y, r.z + sum.z, r.w);
+        }
+        if (!v.alive) break;
+        ++n_closest;
+        o = out.o;
+        d = out.d;
+        thr = out.t;
+        ior = out.ior;
+        w = out.w;
+        const SceneHit hh = scene_closest<EXACT, Src::kWide>(S, o, d, err);
+        const int code = hh.prim >= 0 ? hh.prim : (hh.slot >= 0 ? -(hh.slot + 2) : -1);
+        h = make_float4(hh.t, __int_as_float(code), hh.u, hh.v);
+      }
+      rad_b[p] = r;
+    }
+  }
+  // every lane leaves the fetch loop together
+  n_closest = __reduce_add_sync(0xffffffffu, n_closest);
+  n_shadow = __reduce_add_sync(0xffffffffu, n_shadow);
+  if (lane == 0) {
+    if (n_closest) atomicAdd(&counters[C_Q + b + 1], n_closest);
+    if (n_shadow) atomicAdd(&counters[C_S + b], n_shadow);
   }
 }
 
@@ -986,6 +1187,7 @@ struct Accum {
   rx_render_params g_params;
   int g_spf = 0;
   int g_launches = 0;
+  int g_events = 0;  // timing events the captured wave records
   // reset / render return once queued (errors surface at rx_ctx_sync)
   bool async = false;
   // timing
@@ -997,7 +1199,10 @@ struct Accum {
   int last_launches = 0;
   // denoise scratch
   DevBuf<float4> dn0, dn1, dn_out;
-  int occ_ext = 0, occ_shade = 0;
+  int occ_ext = 0, occ_shade = 0, occ_tail = 0;
+  // k_tail takes a wave over at the first bounce (>= 1) whose queue holds at
+  // most this many paths; 0: never
+  int tail_paths = kTailPaths;
 
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -1103,9 +1308,20 @@ static void launch_extend(Accum* a, const DevScene& S, const RenderK& K, int b, 
   }
 }
 
+static void launch_tail(Accum* a, const DevScene& S, const RenderK& K, int b, const int* qin) {
+  Ctx* ctx = a->ctx;
+  SingleSrc src{S, K, a->frame_base.p};
+  auto go = [&](auto kernel) {
+    kernel<<<a->occ_tail, 128, 0, ctx->stream>>>(src, b, qin, a->counters.p, a->tail_paths, a->frame_base.p,
+                                                  a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p, a->hits.p, ctx->d_err);
+  };
+  if (S.exact_slab) go(k_tail<true, SingleSrc>);
+  else go(k_tail<false, SingleSrc>);
+}
+
 // Records the launch sequence of one wave on the context stream.  With
 // `timed`, an event is recorded after every kernel (class in ev_class).
-static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int* n_launch) {
+static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int* n_launch, int* n_events) {
   Ctx* ctx = a->ctx;
   cudaStream_t st = ctx->stream;
   DevScene S = sc->view();
@@ -1137,6 +1353,13 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
     launch_extend(a, S, K, b, qin, sb);
     ++launches;
     mark(K_EXTEND);
+    if (b >= 1 && a->tail_paths > 0) {
+      // takes the wave over once the queue is short (then the launches
+      // below return at once); its time counts as extend time
+      launch_tail(a, S, K, b, qin);
+      ++launches;
+      mark(K_EXTEND);
+    }
     k_shade<SingleSrc><<<a->occ_shade, 128, 0, st>>>(SingleSrc{S, K, a->frame_base.p}, b, qin, qout, a->counters.p,
                                                       a->frame_base.p, a->ray_o.p, a->ray_d.p, a->thr.p, a->rad.p,
                                                       a->gn.p, a->ga.p, a->hits.p, a->shadow.p, ctx->d_err);
@@ -1157,6 +1380,7 @@ static void enqueue_wave(Accum* a, Scene* sc, const RenderK& K, bool timed, int*
   launches += 2;
   mark(K_OTHER);
   *n_launch = launches;
+  *n_events = ev_i;
 }
 
 static int ensure_wave_buffers(Accum* a, long long cap, long long shadow_cap) {
@@ -1185,6 +1409,7 @@ static int ensure_wave_buffers(Accum* a, long long cap, long long shadow_cap) {
   if (!a->occ_ext) {
     a->occ_ext = blocks_for(ctx, (const void*)k_extend<false, SingleSrc, 128>, 128);
     a->occ_shade = blocks_for(ctx, (const void*)k_shade<SingleSrc>, 128);
+    a->occ_tail = blocks_for(ctx, (const void*)k_tail<false, SingleSrc>, 128);
   }
   return RX_OK;
 }
@@ -1263,14 +1488,14 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
   while (remaining > 0) {
     int k = std::min(spf, remaining);
     RenderK K = make_k(p, a, k, shadow_cap);
-    int nlaunch = 0;
+    int nlaunch = 0, nevent = 0;
     if (k == spf) {
       bool cached = a->gexec && a->g_scene == sc && a->g_ver == sc->version && a->g_spf == spf &&
                     a->g_timed == timed && std::memcmp(&a->g_params, p, sizeof(*p)) == 0;
       if (!cached) {
         cudaGraph_t g;
         CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        enqueue_wave(a, sc, K, timed, &nlaunch);
+        enqueue_wave(a, sc, K, timed, &nlaunch, &nevent);
         CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
         // same launch sequence with new arguments (another scene, other
         // parameters): update the executable graph in place, else rebuild it
@@ -1298,21 +1523,21 @@ int render(Scene* sc, Accum* a, const rx_render_params* p, int frames) {
         a->g_timed = timed;
         a->g_params = *p;
         a->g_launches = nlaunch;
+        a->g_events = nevent;
       }
       nlaunch = a->g_launches;
+      nevent = a->g_events;
       CUDA_TRY(ctx, cudaGraphLaunch(a->gexec, st));
     } else {
-      enqueue_wave(a, sc, K, timed, &nlaunch);
+      enqueue_wave(a, sc, K, timed, &nlaunch, &nevent);
     }
     launches_total += nlaunch;
     if (timed) {
       CUDA_TRY(ctx, cudaStreamSynchronize(st));
-      // events: start, after generate, after each bounce kernel, after accumulate
-      int ne = 2;
-      ne += 2 * p->max_depth;
-      if (p->max_depth > 0 && p->max_depth - 1 < p->direct_light_max_depth && nl > 0) ne += 1;
-      ne += 2;  // after accumulate, after finish
-      for (int i = 1; i < ne; ++i) {
+      // events: start, after generate, after each bounce kernel (extend,
+      // tail, shade), after the last shadow rays, accumulate and finish;
+      // interval i - 1 -> i counts for the class of the kernel ending at i
+      for (int i = 1; i < nevent; ++i) {
         float ms = 0.0f;
         CUDA_TRY(ctx, cudaEventElapsedTime(&ms, a->ev[i - 1], a->ev[i]));
         k_ms[a->ev_class[i]] += ms;
@@ -1405,6 +1630,13 @@ int accum_set_timing(Accum* a, int on) {
 
 int accum_set_async(Accum* a, int on) {
   a->async = on != 0;
+  return RX_OK;
+}
+
+int accum_set_tail(Accum* a, int max_paths) {
+  if (max_paths < 0) return set_error(a->ctx, "accum_set_tail: max_paths must be >= 0"), RX_ERR_ARG;
+  if (max_paths != a->tail_paths) a->drop_graph();  // the graph holds the launches
+  a->tail_paths = max_paths;
   return RX_OK;
 }
 

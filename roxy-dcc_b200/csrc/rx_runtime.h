@@ -259,6 +259,7 @@ int accum_info(Accum* a, int* w, int* h, int* frames, long long* rays);
 int accum_denoise(Accum* a, const rx_denoise_params* dp, float* host_out);
 int accum_set_timing(Accum* a, int on);
 int accum_set_async(Accum* a, int on);
+int accum_set_tail(Accum* a, int max_paths);
 int accum_last_timing(Accum* a, float* ms_total, float* ms_kernels, int n_kernels, int* launches);
 int accum_set_f64(Accum* a, int on);
 int accum_read_f64(Accum* a, double* host_out);

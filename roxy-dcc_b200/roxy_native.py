@@ -165,6 +165,7 @@ _SIGS = {
     "rx_accum_denoise": ([ctypes.c_void_p, ctypes.POINTER(DenoiseParams), _f32p], ctypes.c_int),
     "rx_accum_set_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_accum_set_async": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rx_accum_set_tail": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_accum_last_timing": ([ctypes.c_void_p, _f32p, _f32p, ctypes.c_int, _i32p], ctypes.c_int),
     "rx_accum_set_f64": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_batch_create": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
@@ -623,6 +624,11 @@ class Accumulator:
     def set_async(self, on):
         """reset()/render() return once queued; errors surface at ctx.sync()."""
         self.ctx.check(lib().rx_accum_set_async(self.h, int(bool(on))))
+
+    def set_tail(self, max_paths):
+        """Queue length at or below which one launch runs a wave's remaining
+        bounces path by path (0: one launch pair per bounce throughout)."""
+        self.ctx.check(lib().rx_accum_set_tail(self.h, int(max_paths)))
 
     def last_timing(self):
         tot = ctypes.c_float()

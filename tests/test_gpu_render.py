@@ -147,6 +147,64 @@ def test_converges_to_reference_estimator_3sigma(scene_name):
     assert zm < 4, (zm, ma.mean(), mr.mean())
 
 
+def _renders_with_tail(world, W, H, spp, max_depth, dlmd, tails, mode=0, compat=False, mis=False, method="lbvh",
+                       wave_paths=0):
+    ds = build_device_scene(world, method=method)
+    ds.use_lights(compat)
+    cam = world.active_camera
+    p = make_params(W, H, math.tan(math.radians(cam.fov) / 2), cam.aspect_ratio, max_depth, world._use_sky, mode,
+                    dlmd, 10.0, list(world._background_color), list(cam.position), list(cam.forward),
+                    list(cam.right), list(cam.up), reference_compat=compat, seed=11, wave_paths=wave_paths)
+    if mis:
+        p.mis = 1
+    outs = []
+    for t in tails:
+        acc = nat.Accumulator(W, H)
+        acc.set_tail(t)
+        acc.render(ds.native, p, spp)
+        acc.render(ds.native, p, 2)  # a second call continues the running means
+        out = [acc.read(w) for w in (nat.RX_ACC_RADIANCE, nat.RX_ACC_NORMAL, nat.RX_ACC_ALBEDO, nat.RX_ACC_DEPTH,
+                                     nat.RX_ACC_DISPLAY)]
+        outs.append((out, acc.info()["rays"]))
+    return outs
+
+
+@pytest.mark.parametrize("case", ["trace-one", "trace-all", "trace-compat", "trace-reference-tree", "cornell",
+                                  "cornell-mis", "cornell-waves", "texture", "icosphere"])
+def test_wave_tail_equals_one_launch_per_bounce(case):
+    """k_tail (a wave's remaining bounces run path by path in one launch, the
+    shadow rays traced at once) gives the same radiance, guides, display and
+    ray count bit for bit as one extend and one shade launch per bounce,
+    whether it takes over at bounce 1 (threshold above every queue) or part
+    way through the wave (threshold between the queue lengths)."""
+    W, H, spp = 40, 30, 6
+    paths = W * H * spp
+    tails = (0, 1 << 30, paths // 9)
+    kw = {}
+    if case.startswith("trace"):
+        world = gs.build_trace_scene(_ns())
+        kw = {"trace-one": dict(mode=0), "trace-all": dict(mode=1), "trace-compat": dict(compat=True),
+              "trace-reference-tree": dict(method="morton")}[case]
+        max_depth, dlmd = 8, 8
+    elif case.startswith("cornell"):
+        world = workloads.cornell_box(W, H)
+        kw = {"cornell": {}, "cornell-mis": dict(mis=True), "cornell-waves": dict(wave_paths=2 * W * H)}[case]
+        max_depth, dlmd = 8, 8
+    elif case == "texture":
+        world = gs.build_texture_scene(_ns())
+        max_depth, dlmd = 6, 6
+    else:
+        world = workloads.displaced_icosphere_scene(W, H, subdiv=4)
+        max_depth, dlmd = 12, 1
+    outs = _renders_with_tail(world, W, H, spp, max_depth, dlmd, tails, **kw)
+    (ref, rays) = outs[0]
+    assert rays > paths
+    for t, (out, r) in zip(tails[1:], outs[1:]):
+        assert r == rays, (t, r, rays)
+        for k, (a, b) in enumerate(zip(out, ref)):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (t, k, float(np.abs(a - b).max()))
+
+
 def _block_z(A, B):
     n = len(A)
     H, W = A.shape[1:3]

@@ -269,6 +269,11 @@ int rx_batch_clear(rx_batch* batch);
 int rx_batch_add(rx_batch* batch, rx_scene* scene, rx_accum* acc, const rx_render_params* params, int frames,
                  int* job);
 int rx_batch_set_config(rx_batch* batch, long long wave_paths, int extend_block);
+/* The batch counterpart of rx_accum_set_tail: from the first bounce >= 1
+ * whose wave queue holds at most max_paths paths, of every scene of the
+ * wave, one launch runs the remaining bounces a thread per path.  0 turns it
+ * off; the default is 65536. */
+int rx_batch_set_tail(rx_batch* batch, int max_paths);
 int rx_batch_render(rx_batch* batch);
 int rx_batch_last_stats(rx_batch* batch, float* ms, int* waves, int* launches);
 

@@ -823,6 +823,12 @@ int rx_batch_set_config(rx_batch* b, long long wave_paths, int extend_block) {
   return batch_set_config(b->b, wave_paths, extend_block);
 }
 
+int rx_batch_set_tail(rx_batch* b, int max_paths) {
+  if (!b) return RX_ERR_ARG;
+  LOCK(b->ctx);
+  return batch_set_tail(b->b, max_paths);
+}
+
 int rx_batch_render(rx_batch* b) {
   if (!b) return RX_ERR_ARG;
   LOCK(b->ctx);

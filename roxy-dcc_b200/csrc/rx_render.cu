@@ -977,11 +977,14 @@ __global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restr
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
     const int i = base + lane;
+    int job = -1, rays_here = 0;  // batches: the rays this lane traced, counted for its job
     if (i < n) {
       const int p = qin[i];
       const int si = src.seg(p);
       const DevScene S = src.scene(si);
       const RenderK K = src.params(si);
+      if constexpr (Src::kBatch) job = src.segs[si].job;
+      const int closest0 = n_closest, shadow0 = n_shadow;
       const bool mis = K.mis && S.light_of_lin != nullptr;
       const float4 o4 = ray_o[p], d4 = ray_d[p], t4 = thr_b[p];
       float3 o = xyz(o4), d = xyz(d4), thr = xyz(t4);
@@ -1035,14 +1038,23 @@ __global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restr
         h = make_float4(hh.t, __int_as_float(code), hh.u, hh.v);
       }
       rad_b[p] = r;
+      rays_here = (n_closest - closest0) + (n_shadow - shadow0);
+    }
+    if constexpr (Src::kBatch) {
+      // rays traced, counted per job as k_extend counts them
+      unsigned m = __match_any_sync(0xffffffffu, job);
+      int tot = __reduce_add_sync(m, rays_here);
+      if (job >= 0 && tot && lane == __ffs(m) - 1) atomicAdd(src.job_rays + job, (unsigned long long)tot);
     }
   }
-  // every lane leaves the fetch loop together
-  n_closest = __reduce_add_sync(0xffffffffu, n_closest);
-  n_shadow = __reduce_add_sync(0xffffffffu, n_shadow);
-  if (lane == 0) {
-    if (n_closest) atomicAdd(&counters[C_Q + b + 1], n_closest);
-    if (n_shadow) atomicAdd(&counters[C_S + b], n_shadow);
+  if constexpr (!Src::kBatch) {
+    // every lane leaves the fetch loop together
+    n_closest = __reduce_add_sync(0xffffffffu, n_closest);
+    n_shadow = __reduce_add_sync(0xffffffffu, n_shadow);
+    if (lane == 0) {
+      if (n_closest) atomicAdd(&counters[C_Q + b + 1], n_closest);
+      if (n_shadow) atomicAdd(&counters[C_S + b], n_shadow);
+    }
   }
 }
 
@@ -1693,6 +1705,7 @@ struct Batch {
   std::vector<BatchJob> jobs;
   long long wave_paths = 1LL << 25;
   int ext_block = 128;
+  int tail_paths = kTailPaths;  // k_tail's threshold (0: never)
   bool use_graph = true;
   long long cap = 0, shadow_cap = 0;
   DevBuf<float4> ray_o, ray_d, thr, rad, gn, ga, hits, shadow;
@@ -1766,6 +1779,13 @@ int batch_set_config(Batch* b, long long wave_paths, int ext_block) {
   return RX_OK;
 }
 
+int batch_set_tail(Batch* b, int max_paths) {
+  if (max_paths < 0) return set_error(b->ctx, "batch_set_tail: max_paths must be >= 0"), RX_ERR_ARG;
+  if (max_paths != b->tail_paths) b->drop_graph();
+  b->tail_paths = max_paths;
+  return RX_OK;
+}
+
 static std::vector<PlannedWave> plan_waves(const Batch* b, std::vector<WaveSeg>& segs) {
   std::vector<PlannedWave> waves;
   std::vector<int> rem(b->jobs.size());
@@ -1828,6 +1848,8 @@ static void enqueue_batch(Batch* B, const std::vector<PlannedWave>& waves, int* 
   for (const BatchJob& j : B->jobs) wide = wide && j.sc->n_nodes4 > 0 && !j.sc->exact_slab;
   int occ_ext = batch_ext_blocks(ctx, B->ext_block, wide);
   int occ_shade = blocks_for(ctx, (const void*)k_shade<BatchSrc>, 128);
+  int occ_tail = wide ? blocks_for(ctx, (const void*)k_tail<false, BatchSrc4>, 128)
+                      : blocks_for(ctx, (const void*)k_tail<false, BatchSrc>, 128);
   int launches = 0;
   for (const PlannedWave& w : waves) {
     BatchSrc src{B->pseg.p, B->d_segs.p + w.seg0, B->d_scenes.p, B->d_ks.p, B->d_accs.p, B->d_job_rays.p};
@@ -1847,6 +1869,15 @@ static void enqueue_batch(Batch* B, const std::vector<PlannedWave>& waves, int* 
       const int* qin = (b & 1) ? B->q1.p : B->q0.p;
       int* qout = (b & 1) ? B->q0.p : B->q1.p;
       ext(b, qin, b >= 1 ? b - 1 : -1);
+      if (b >= 1 && B->tail_paths > 0) {
+        auto tail = [&](auto kernel, const auto& s) {
+          kernel<<<occ_tail, 128, 0, st>>>(s, b, qin, B->counters.p, B->tail_paths, nullptr, B->ray_o.p, B->ray_d.p,
+                                           B->thr.p, B->rad.p, B->hits.p, ctx->d_err);
+        };
+        if (wide) tail(k_tail<false, BatchSrc4>, BatchSrc4{src});
+        else tail(k_tail<false, BatchSrc>, src);
+        ++launches;
+      }
       k_shade<BatchSrc><<<occ_shade, 128, 0, st>>>(src, b, qin, qout, B->counters.p, nullptr, B->ray_o.p,
                                                     B->ray_d.p, B->thr.p, B->rad.p, B->gn.p, B->ga.p, B->hits.p,
                                                     B->shadow.p, ctx->d_err);

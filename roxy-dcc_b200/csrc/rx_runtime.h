@@ -271,6 +271,7 @@ void batch_delete(Batch* b);
 int batch_clear(Batch* b);
 int batch_add(Batch* b, Scene* sc, Accum* acc, const rx_render_params* p, int frames, int* job);
 int batch_set_config(Batch* b, long long wave_paths, int ext_block);
+int batch_set_tail(Batch* b, int max_paths);
 int batch_render(Batch* b);
 int batch_last_stats(Batch* b, float* ms, int* waves, int* launches);
 void batch_use_graph(Batch* b, bool on);

@@ -174,6 +174,7 @@ _SIGS = {
     "rx_batch_add": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(RenderParams), ctypes.c_int,
                       _i32p], ctypes.c_int),
     "rx_batch_set_config": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int], ctypes.c_int),
+    "rx_batch_set_tail": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rx_batch_render": ([ctypes.c_void_p], ctypes.c_int),
     "rx_batch_last_stats": ([ctypes.c_void_p, _f32p, _i32p, _i32p], ctypes.c_int),
     "rx_accum_read_f64": ([ctypes.c_void_p, _f64p], ctypes.c_int),
@@ -555,6 +556,11 @@ class Batch:
 
     def set_config(self, wave_paths, extend_block=128):
         self.ctx.check(lib().rx_batch_set_config(self.h, int(wave_paths), int(extend_block)))
+
+    def set_tail(self, max_paths):
+        """Wave queue length at or below which one launch runs the remaining
+        bounces path by path (0: one launch pair per bounce throughout)."""
+        self.ctx.check(lib().rx_batch_set_tail(self.h, int(max_paths)))
 
     def render(self):
         self.ctx.check(lib().rx_batch_render(self.h))

@@ -53,6 +53,26 @@ def test_batch_equals_solo_renders(wave_paths, block):
         _same(j.acc, s)
 
 
+@pytest.mark.parametrize("tail", [0, 1 << 30, 400])
+def test_batch_tail_equals_solo_renders_without_tail(tail):
+    """k_tail in a batch (a wave's remaining bounces run path by path for
+    every scene of the wave, each path's rays counted for its job) leaves
+    every job's accumulators, frames and ray count equal to a solo render
+    with one launch pair per bounce, whether it is off, takes over at bounce
+    1 or takes over part way."""
+    br = BatchRenderer(_jobs(), BatchConfig(wave_paths=9000, extend_block=128))
+    br.batch.set_tail(tail)
+    solo = []
+    for j in br.jobs:
+        acc = nat.Accumulator(j.width, j.height)
+        acc.set_tail(0)
+        acc.render(j.scene.native, j.params, j.spp)
+        solo.append(acc)
+    br.render()
+    for j, s in zip(br.jobs, solo):
+        _same(j.acc, s)
+
+
 def test_batch_graph_replay_continues_accumulation():
     br = BatchRenderer(_jobs()[:3], BatchConfig(wave_paths=5000, extend_block=128))
     br.render()

@@ -416,11 +416,13 @@ def run_ours(args):
                            "bvh": "LBVH + SAH collapse, leaf 4", "bvh_build_s_host_incl": build_s,
                            "l2": "wavefront state > L2 each wave; BVH + triangles L2-resident by design"},
                 "gpu_launches": launches,
-                "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
+                "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal) + k_tail",
                              "achieved": ext_gbs, "peak": peak, "unit": "GB/s", "frac": ext_gbs / peak,
                              "traffic": traffic, "peak_source": peak_kind,
                              "algorithmic_bytes_per_ray": ext_bytes / max(ext_rays, 1),
-                             "note": f"traversal is latency/L2 bound; frac is of the {peak_kind} HBM copy bandwidth",
+                             "note": f"traversal is latency/L2 bound; frac is of the {peak_kind} HBM copy bandwidth; "
+                                     "extend time includes k_tail, which runs the last bounces of each wave "
+                                     "(their traversal and shading) once the queue is short",
                              "extend_ms_per_step": ext_ms, "extend_rays_per_step": ext_rays,
                              "shade": {"achieved": shade_gbs, "frac": shade_gbs / peak,
                                        "algorithmic_bytes_per_ray": shade_bytes / max(ext_rays, 1),

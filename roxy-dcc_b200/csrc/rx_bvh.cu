@@ -96,6 +96,37 @@ __global__ void k_reduce_bounds(int n, const float3* __restrict__ p, float3* __r
   }
 }
 
+// Second stage: one block of kBoundsThreads reduces the parts' boxes --
+// the minimum over mins[] and the maximum over maxs[] -- into out[0],
+// out[1].  Min and max are exact, so the result does not depend on the
+// order.
+constexpr int kBoundsThreads = 1024;
+__global__ void __launch_bounds__(kBoundsThreads) k_bounds_final(int parts, const float3* __restrict__ mins,
+                                                                 const float3* __restrict__ maxs,
+                                                                 float3* __restrict__ out) {
+  __shared__ float3 slo[kBoundsThreads], shi[kBoundsThreads];
+  float3 lo = f3(INFINITY, INFINITY, INFINITY), hi = f3(-INFINITY, -INFINITY, -INFINITY);
+  for (int k = threadIdx.x; k < parts; k += kBoundsThreads) {
+    lo = vmin(lo, mins[k]);
+    hi = vmax(hi, maxs[k]);
+  }
+  const int t = threadIdx.x;
+  slo[t] = lo;
+  shi[t] = hi;
+  __syncthreads();
+  for (int s = kBoundsThreads / 2; s > 0; s >>= 1) {
+    if (t < s) {
+      slo[t] = vmin(slo[t], slo[t + s]);
+      shi[t] = vmax(shi[t], shi[t + s]);
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[0] = slo[0];
+    out[1] = shi[0];
+  }
+}
+
 __device__ __forceinline__ uint32_t expand10(uint32_t v) {
   v &= 0x000003ffu;
   v = (v | (v << 16)) & 0x030000ffu;
@@ -110,16 +141,12 @@ __device__ __forceinline__ uint32_t expand10(uint32_t v) {
 // cubic != 0 (the LBVH): all three axes are normalised by the largest
 // extent, so the grid's cells are cubes rather than the bounds' shape; on the
 // benchmark scene's rays that tree visits 1.5-5 % fewer nodes.
-__global__ void k_morton(int n, const float3* __restrict__ cen, const float3* __restrict__ part_min,
-                         const float3* __restrict__ part_max, int nparts, int cubic, uint32_t* __restrict__ codes,
-                         int* __restrict__ idx) {
+// `bounds`: the centroid bounds (k_bounds_final).
+__global__ void k_morton(int n, const float3* __restrict__ cen, const float3* __restrict__ bounds, int cubic,
+                         uint32_t* __restrict__ codes, int* __restrict__ idx) {
   __shared__ float3 s_lo, s_ext;
   if (threadIdx.x == 0) {
-    float3 lo = f3(INFINITY, INFINITY, INFINITY), hi = f3(-INFINITY, -INFINITY, -INFINITY);
-    for (int i = 0; i < nparts; ++i) {
-      lo = vmin(lo, part_min[i]);
-      hi = vmax(hi, part_max[i]);
-    }
+    const float3 lo = bounds[0], hi = bounds[1];
     float3 e = hi - lo;
     if (e.x <= 1e-12f) e.x = 1.0f;
     if (e.y <= 1e-12f) e.y = 1.0f;
@@ -741,18 +768,6 @@ __global__ void k_single_leaf_root(const float3* __restrict__ bmin, const float3
   out[3] = make_float4(__int_as_float(pack_leaf(0, cnt)), __int_as_float(pack_leaf(0, 0)), __int_as_float(cnt), __int_as_float(0));
 }
 
-// Folds the per-block partial minima / maxima into out[0] (min), out[1] (max).
-__global__ void k_box_finish(int parts, const float3* __restrict__ part_min, const float3* __restrict__ part_max,
-                             float3* __restrict__ out) {
-  float3 lo = f3(INFINITY, INFINITY, INFINITY), hi = f3(-INFINITY, -INFINITY, -INFINITY);
-  for (int k = 0; k < parts; ++k) {
-    lo = vmin(lo, part_min[k]);
-    hi = vmax(hi, part_max[k]);
-  }
-  out[0] = lo;
-  out[1] = hi;
-}
-
 static int grid_for(Ctx* ctx, long long n, int block = 256) {
   long long g = (n + block - 1) / block;
   long long cap = (long long)ctx->num_sms * 32;
@@ -772,12 +787,14 @@ static int front_end(Ctx* ctx, Scene* sc, int n_obj, const float4* d_obj_a, cons
   const int parts = std::min(grid_for(ctx, n), 1024);
   DevBuf<float3> part_min(ctx, parts), part_max(ctx, parts);
   DevBuf<uint32_t> codes(ctx, n);
-  if (!all_ok(pmin, pmax, order, cen, part_min, part_max, codes))
+  DevBuf<float3> cbox(ctx, 2);
+  if (!all_ok(pmin, pmax, order, cen, part_min, part_max, codes, cbox))
     return set_error(ctx, "BVH build: out of device memory"), RX_ERR_CAPACITY;
   k_prim_bounds<<<grid_for(ctx, n), 256, 0, st>>>(sc->n_tris, sc->d_v0, sc->d_v1, sc->d_v2, n_obj, d_obj_a, d_obj_b,
                                                    lbvh_keys, pmin.p, pmax.p, cen.p);
   k_reduce_bounds<<<parts, 256, 0, st>>>(n, cen.p, part_min.p, part_max.p);
-  k_morton<<<grid_for(ctx, n), 256, 0, st>>>(n, cen.p, part_min.p, part_max.p, parts, lbvh_keys, codes.p, order.p);
+  k_bounds_final<<<1, kBoundsThreads, 0, st>>>(parts, part_min.p, part_max.p, cbox.p);
+  k_morton<<<grid_for(ctx, n), 256, 0, st>>>(n, cen.p, cbox.p, lbvh_keys, codes.p, order.p);
   if (int rc = radix_sort(ctx, n, codes.p, order.p, 30)) return rc;
   sc->tmp_codes.swap(codes);
   return RX_OK;
@@ -1020,7 +1037,7 @@ int build_lbvh(Ctx* ctx, Scene* sc, int max_leaf, int spheres_in_bvh, float c_t,
     }
     k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmin.p, lo_min.p, lo_max.p);
     k_reduce_bounds<<<parts, 256, 0, st>>>(n, pmax.p, hi_min.p, hi_max.p);
-    k_box_finish<<<1, 1, 0, st>>>(parts, lo_min.p, hi_max.p, rb.p);
+    k_bounds_final<<<1, kBoundsThreads, 0, st>>>(parts, lo_min.p, hi_max.p, rb.p);
   }
   float3 hb[2];
   cudaMemcpyAsync(hb, rb.p, sizeof(hb), cudaMemcpyDeviceToHost, st);

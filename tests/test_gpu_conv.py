@@ -197,7 +197,7 @@ def test_tcgen05_and_mma_sync_convolutions_agree():
     g = torch.Generator(device="cuda").manual_seed(21)
     for (Cin, Cout, H, W) in ((16, 32, 33, 257), (96, 32, 20, 128), (64, 128, 9, 200), (32, 16, 5, 130),
                               (64, 64, 70, 300), (192, 64, 6, 129), (32, 32, 128, 512), (96, 32, 600, 256),
-                              (96, 64, 20, 140)):
+                              (96, 64, 20, 140), (128, 128, 12, 140)):
         x = torch.randn((2, H, W, Cin), generator=g, device="cuda").to(torch.bfloat16)
         w = (torch.randn((Cout, 9, Cin), generator=g, device="cuda") / np.sqrt(9 * Cin)).to(torch.bfloat16)
         b = torch.randn(Cout, generator=g, device="cuda")

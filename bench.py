@@ -693,9 +693,10 @@ def run_denoiser(args):
             "config": {"workload": "learned denoiser, 3-level U-Net 32/64/128, 1920x1080 4-spp render of the "
                                    "displaced-icosphere scene", "flops_per_frame": r["flops_per_frame"]},
             "roofline": {"bound": "tensor",
-                         "kernel": "whole inference: k_conv_fwd_ws (tcgen05, 9 layers) + k_conv_fwd (mma.sync, the "
-                                   "2 layers whose weights do not fit beside the row ring) + pool / upsample / "
-                                   "feature / output kernels; network FLOPs over the inference time",
+                         "kernel": "whole inference: k_conv_fwd_ws (tcgen05; 9 layers in one launch, e3b and d2a, "
+                                   "whose weights do not fit beside the row ring in one, as two launches over "
+                                   "the halves of their input channels) + pool / upsample / feature / output "
+                                   "kernels; network FLOPs over the inference time",
                          "achieved": r["infer_tflops"], "peak": peak, "unit": "TFLOP/s",
                          "frac": r["infer_tflops"] / peak,
                          "peak_source": "measured" if "bf16_tflops" in peaks else "fallback", "traffic": None},

@@ -460,11 +460,15 @@ __device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity, vo
   }
 }
 
+// acc_in (may be null): fp32 partial sums [pixel][Cout] of the other input
+// channels, added before the bias (a layer split over its input channels,
+// conv_fwd); y (may be null): bf16 output.
 template <int NG>
 __global__ void __launch_bounds__(224, 1) k_conv_fwd_ws(rx_conv_desc d, const bf16* __restrict__ x,
                                                         const bf16* __restrict__ w, const float* __restrict__ bias,
-                                                        bf16* __restrict__ y, float* __restrict__ y32, int relu,
-                                                        int S, int G, long long per_cta, int* err) {
+                                                        bf16* __restrict__ y, float* __restrict__ y32,
+                                                        const float* __restrict__ acc_in, int relu, int S, int G,
+                                                        long long per_cta, int* err) {
   constexpr int TCOLS = 2 * NG < 32 ? 32 : 2 * NG;  // two accumulators
   constexpr int kProducers = 64;                     // warps 5 and 6
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -674,21 +678,36 @@ __global__ void __launch_bounds__(224, 1) k_conv_fwd_ws(rx_conv_desc d, const bf
           if (xx < d.W) {
             float v[16];
 #pragma unroll
+            for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+            if (acc_in) {
+              const float4* a4 = reinterpret_cast<const float4*>(acc_in + m * d.Cout + grp * NG + c0);
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const float4 a = a4[k];
+                v[4 * k] += a.x;
+                v[4 * k + 1] += a.y;
+                v[4 * k + 2] += a.z;
+                v[4 * k + 3] += a.w;
+              }
+            }
+#pragma unroll
             for (int k = 0; k < 16; ++k) {
-              v[k] = __uint_as_float(r[k]) + sbias[c0 + k];
+              v[k] = v[k] + sbias[c0 + k];
               if (relu) v[k] = fmaxf(v[k], 0.0f);
             }
-            uint4 pk[2];
-            uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-              pw[k] = *reinterpret_cast<uint32_t*>(&h);
-            }
             const long long o = m * d.y_cstride + d.y_coff + grp * NG + c0;
-            uint4* dst = reinterpret_cast<uint4*>(y + o);
-            dst[0] = pk[0];
-            dst[1] = pk[1];
+            if (y) {
+              uint4 pk[2];
+              uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+                pw[k] = *reinterpret_cast<uint32_t*>(&h);
+              }
+              uint4* dst = reinterpret_cast<uint4*>(y + o);
+              dst[0] = pk[0];
+              dst[1] = pk[1];
+            }
             if (y32) {
               float4* d32 = reinterpret_cast<float4*>(y32 + o);
 #pragma unroll
@@ -1085,7 +1104,7 @@ static int launch_tc(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16*
 
 template <int NG>
 static int launch_ws_ng(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
-                        float* y32, int relu, int S, int smem, cudaStream_t st, int* rc) {
+                        float* y32, const float* acc_in, int relu, int S, int smem, cudaStream_t st, int* rc) {
   const int limit = 232448 - 1024;  // opt-in shared memory per block, less the static part
   static int attr_dev = -1;
   if (attr_dev != ctx->device) {
@@ -1111,8 +1130,8 @@ static int launch_ws_ng(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf
   const long long strips_want = std::max<long long>(1, (long long)ctx->num_sms * per_sm / G);
   const long long per_cta = (total + std::min(total, strips_want) - 1) / std::min(total, strips_want);
   const long long strips = (total + per_cta - 1) / per_cta;
-  k_conv_fwd_ws<NG><<<(unsigned)(strips * G), 224, smem, st>>>(*d, x, w, bias, y, y32, relu, S, G, per_cta,
-                                                                 ctx->d_err);
+  k_conv_fwd_ws<NG><<<(unsigned)(strips * G), 224, smem, st>>>(*d, x, w, bias, y, y32, acc_in, relu, S, G,
+                                                                 per_cta, ctx->d_err);
   cudaError_t e = cudaGetLastError();
   *rc = e == cudaSuccess ? RX_OK : (set_error(ctx, "conv_bf16_fwd: %s", cudaGetErrorString(e)), RX_ERR_CUDA);
   return 1;
@@ -1122,28 +1141,100 @@ static int launch_ws_ng(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf
 // 64, 32 or 16, dividing Cout) whose weights fit in shared memory beside a
 // ring of at least 4 input rows (6 where they fit).  Returns 1 if it
 // launched, 0 if the shape or the pointers do not suit it.
-static int launch_ws(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
-                     float* y32, int relu, cudaStream_t st, int* rc) {
+// Output-channel group for the warp-specialised kernel at this Cin / Cout,
+// and the ring's row slots; 0 when the weights do not fit.
+static int ws_group(int Cin, int Cout, int* S_out, int* smem_out) {
   const int limit = 232448 - 1024;
-  if (((uintptr_t)x & 15) || ((uintptr_t)y & 15) || (y32 && ((uintptr_t)y32 & 15))) return 0;
-  const int SB = tc::slot_bytes(d->Cin);
+  const int SB = tc::slot_bytes(Cin);
   int NG = 0;
   // at most two groups: every group re-reads the input rows, and a UMMA's
   // cost is mostly its A (pixel) operand read, so narrow groups do not pay
   for (int ng = 128; ng >= 16; ng >>= 1)
-    if (d->Cout % ng == 0 && d->Cout / ng <= 2 && tc::weights_bytes(d->Cin, ng) + 4 * SB + 128 <= limit) {
+    if (Cout % ng == 0 && Cout / ng <= 2 && tc::weights_bytes(Cin, ng) + 4 * SB + 128 <= limit) {
       NG = ng;
       break;
     }
   if (!NG) return 0;
-  const int S = std::min(6, (limit - 128 - tc::weights_bytes(d->Cin, NG)) / SB);
-  const int smem = tc::weights_bytes(d->Cin, NG) + S * SB + 128;
+  *S_out = std::min(6, (limit - 128 - tc::weights_bytes(Cin, NG)) / SB);
+  *smem_out = tc::weights_bytes(Cin, NG) + *S_out * SB + 128;
+  return NG;
+}
+
+static int launch_ws(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                     float* y32, const float* acc_in, int relu, cudaStream_t st, int* rc) {
+  if (((uintptr_t)x & 15) || ((uintptr_t)w & 15) || ((uintptr_t)y & 15) || ((uintptr_t)y32 & 15) ||
+      ((uintptr_t)acc_in & 15))
+    return 0;
+  int S = 0, smem = 0;
+  const int NG = ws_group(d->Cin, d->Cout, &S, &smem);
   switch (NG) {
-    case 128: return launch_ws_ng<128>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
-    case 64: return launch_ws_ng<64>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
-    case 32: return launch_ws_ng<32>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
-    default: return launch_ws_ng<16>(ctx, d, x, w, bias, y, y32, relu, S, smem, st, rc);
+    case 128: return launch_ws_ng<128>(ctx, d, x, w, bias, y, y32, acc_in, relu, S, smem, st, rc);
+    case 64: return launch_ws_ng<64>(ctx, d, x, w, bias, y, y32, acc_in, relu, S, smem, st, rc);
+    case 32: return launch_ws_ng<32>(ctx, d, x, w, bias, y, y32, acc_in, relu, S, smem, st, rc);
+    case 16: return launch_ws_ng<16>(ctx, d, x, w, bias, y, y32, acc_in, relu, S, smem, st, rc);
+    default: return 0;
   }
+}
+
+// Input channels [p * cp, (p + 1) * cp) of weights [Cout][9][Cin] as
+// contiguous [Cout][9][cp], for p = 0, 1 (16-byte chunks).
+__global__ void k_weight_halves(int Cout, int Cin, const uint4* __restrict__ w, uint4* __restrict__ out) {
+  const int cp8 = Cin / 16, c8 = Cin / 8;  // chunks per half row, per row
+  const long long n = (long long)Cout * 9 * c8;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long row = i / c8;
+    const int k = (int)(i - row * c8), half = k / cp8;
+    out[(long long)half * Cout * 9 * cp8 + row * cp8 + (k - half * cp8)] = w[i];
+  }
+}
+
+// A layer whose weights do not fit beside the row ring in one launch, run
+// as two launches over the halves of its input channels: the first writes
+// fp32 partial sums, the second adds them before the bias and activation
+// (sum over channels [0, Cin/2), then [Cin/2, Cin), then + bias).  Returns
+// 1 if it launched.
+static int launch_ws_split(Ctx* ctx, const rx_conv_desc* d, const bf16* x, const bf16* w, const float* bias, bf16* y,
+                           float* y32, int relu, cudaStream_t st, int* rc) {
+  const int cp = d->Cin / 2;
+  int S = 0, smem = 0;
+  if (d->Cin % 32 || !ws_group(cp, d->Cout, &S, &smem)) return 0;
+  if (((uintptr_t)x & 15) || ((uintptr_t)w & 15) || ((uintptr_t)y & 15) || ((uintptr_t)y32 & 15)) return 0;
+  const long long P = (long long)d->N * d->H * d->W;
+  const size_t wbytes = sizeof(bf16) * (size_t)d->Cout * 9 * d->Cin;
+  void* halves = nullptr;
+  float* part = nullptr;
+  // stream-ordered on the caller's stream, which runs the launches
+  if (cudaMallocAsync(&halves, wbytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  if (cudaMallocAsync((void**)&part, sizeof(float) * (size_t)P * d->Cout, st) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeAsync(halves, st);
+    return 0;
+  }
+  const long long chunks = (long long)d->Cout * 9 * (d->Cin / 8);
+  k_weight_halves<<<(int)std::min<long long>((chunks + 255) / 256, (long long)ctx->num_sms * 8), 256, 0, st>>>(
+      d->Cout, d->Cin, reinterpret_cast<const uint4*>(w), static_cast<uint4*>(halves));
+  const bf16* w0 = static_cast<const bf16*>(halves);
+  const bf16* w1 = w0 + (size_t)d->Cout * 9 * cp;
+  rx_conv_desc d0 = *d, d1 = *d;
+  d0.Cin = d1.Cin = cp;
+  d1.x_coff = d->x_coff + cp;
+  d0.y_cstride = d->Cout;  // the partial sums: [pixel][Cout]
+  d0.y_coff = 0;
+  const int first = launch_ws(ctx, &d0, x, w0, nullptr, nullptr, part, nullptr, 0, st, rc);
+  int second = 0;
+  if (first && *rc == RX_OK) second = launch_ws(ctx, &d1, x, w1, bias, y, y32, part, relu, st, rc);
+  cudaFreeAsync(part, st);
+  cudaFreeAsync(halves, st);
+  if (!first) return 0;  // the kernel is not available: the caller falls back
+  if (*rc == RX_OK && !second) {
+    // same kernel and shape as the first launch, so this does not happen
+    set_error(ctx, "conv_bf16_fwd: second half of a split layer did not launch");
+    *rc = RX_ERR_CUDA;
+  }
+  return 1;
 }
 
 int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, const float* bias, void* y, float* y32,
@@ -1153,7 +1244,9 @@ int conv_fwd(Ctx* ctx, const rx_conv_desc* d, const void* x, const void* w, cons
   if (ctx->conv_impl == 0) {
     int rc = RX_OK;
     if (launch_ws(ctx, d, static_cast<const bf16*>(x), static_cast<const bf16*>(w), bias, static_cast<bf16*>(y), y32,
-                  relu, st, &rc))
+                  nullptr, relu, st, &rc) ||
+        launch_ws_split(ctx, d, static_cast<const bf16*>(x), static_cast<const bf16*>(w), bias,
+                        static_cast<bf16*>(y), y32, relu, st, &rc))
       return rc;
   } else if (ctx->conv_impl == 2 && d->H <= 65535 && d->N <= 65535) {
     const bf16* xb = static_cast<const bf16*>(x);

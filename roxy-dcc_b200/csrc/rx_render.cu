@@ -257,22 +257,41 @@ struct JobAcc {
   unsigned long long* rays;
 };
 
-// Queue position s of a frame -> pixel: 4-row strips walked column by
-// column, so a warp covers an 8 x 4 tile.
+// Strip index s of a frame -> pixel: 4-row strips walked column by column,
+// so 32 consecutive indices cover an 8 x 4 tile (32-bit: a frame holds
+// fewer than 2^31 pixels).
 __device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& px, int& py) {
-  long long strip = s / (4LL * K.W);
-  long long r = s - strip * 4LL * K.W;
-  int hs = min(4, K.H - (int)(4 * strip));
-  px = (int)(r / hs);
-  py = (int)(4 * strip + r % hs);
+  const int si = (int)s, w4 = 4 * K.W;
+  const int strip = si / w4, r = si - strip * w4;
+  const int hs = min(4, K.H - 4 * strip);
+  const int c = r / hs;
+  px = c;
+  py = 4 * strip + (r - c * hs);
 }
 
-// Bounce-0 queue position t of a wave -> path index, pixel and frame of the
-// wave: frames outer, then strip order inside a frame.
+// Single renders store path state at index f * P + s: frame f of the wave,
+// s the pixel's strip index.  Camera item t of a wave: frames go in groups
+// of kCamFrames (fewer when the wave's frame count is not a multiple);
+// within a group consecutive items are one pixel's samples and pixels
+// follow the strips, so a warp traces 4 pixels (a strip column) x 8
+// samples, rays that differ only by their sub-pixel jitter, and stores
+// their state as eight runs of 4 consecutive paths.  Any order gives the same image: a path's
+// random numbers depend on its pixel, sample and bounce.
+constexpr int kCamFrames = 8;
+__device__ __forceinline__ int camera_group(const RenderK& K) {
+  int g = kCamFrames;  // the largest power of two up to kCamFrames that divides the wave's frames
+  while (K.spf % g) g >>= 1;
+  return g;
+}
 __device__ __forceinline__ long long camera_path(const RenderK& K, long long t, int& px, int& py, int& f) {
-  f = (int)(t / K.P);
-  strip_pixel(K, t - (long long)f * K.P, px, py);
-  return (long long)f * K.P + (long long)py * K.W + px;
+  const int g = camera_group(K);
+  const long long span = (long long)g * K.P;
+  const long long c = t / span;
+  const int r = (int)(t - c * span);
+  const int s = r / g;
+  f = (int)(c * g) + (r - s * g);
+  strip_pixel(K, s, px, py);
+  return (long long)f * K.P + s;
 }
 
 struct SingleSrc {
@@ -283,10 +302,14 @@ struct SingleSrc {
   __device__ __forceinline__ int seg(long long) const { return 0; }
   __device__ __forceinline__ DevScene scene(int) const { return S; }
   __device__ __forceinline__ RenderK params(int) const { return K; }
-  // pixel and sample index of path p (fb: the accumulator's frame base)
+  // pixel (row major) and sample index of path p = f * P + strip index
+  // (fb: the accumulator's frame base)
   __device__ __forceinline__ void locate(int, long long p, int fb, uint32_t& pix, uint32_t& smp) const {
-    pix = (uint32_t)(p % K.P);
-    smp = (uint32_t)(fb + (int)(p / K.P));
+    const int f = (int)(p / K.P);
+    int px, py;
+    strip_pixel(K, p - (long long)f * K.P, px, py);
+    pix = (uint32_t)(py * K.W + px);
+    smp = (uint32_t)(fb + f);
   }
   // With K.camera0, bounce 0 has no queue: its items are the wave's camera
   // paths in k_generate's order, and k_extend / k_shade make each camera ray
@@ -1062,8 +1085,10 @@ __global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restr
 // display = sqrt(min(acc, 1)).  Frames of the wave are folded in order.
 // One pixel: fold `spf` frames (paths path0 + f * P + pix) into the running
 // means, starting at frame index fb.
+// src: the pixel's path index within a frame (path path0 + f * P + src);
+// pix: its accumulator index.
 __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, long long P, long long path0,
-                                                 long long pix, const float4* __restrict__ rad,
+                                                 long long src, long long pix, const float4* __restrict__ rad,
                                                  const float4* __restrict__ gn, const float4* __restrict__ ga,
                                                  const JobAcc& A) {
   float4 a = A.acc_r[pix], an = A.acc_n[pix], aa = A.acc_a[pix];
@@ -1100,7 +1125,7 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
     float4 s[kU], g[kU], al[kU];
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
-      const long long p = path0 + (long long)(f + u) * P + pix;
+      const long long p = path0 + (long long)(f + u) * P + src;
       s[u] = __ldcs(rad + p);
       g[u] = __ldcs(gn + p);
       al[u] = __ldcs(ga + p);
@@ -1109,7 +1134,7 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
     for (int u = 0; u < kU; ++u) fold(s[u], g[u], al[u], fb + f + u);
   }
   for (; f < spf; ++f) {
-    const long long p = path0 + (long long)f * P + pix;
+    const long long p = path0 + (long long)f * P + src;
     fold(__ldcs(rad + p), __ldcs(gn + p), __ldcs(ga + p), fb + f);
   }
   A.acc_r[pix] = a;
@@ -1127,9 +1152,13 @@ __device__ __forceinline__ void accumulate_pixel(float clamp, int spf, int fb, l
 __global__ void k_accumulate(RenderK K, JobAcc A, const float4* __restrict__ rad, const float4* __restrict__ gn,
                              const float4* __restrict__ ga) {
   int fb = *A.frame_base;
-  for (long long pix = blockIdx.x * (long long)blockDim.x + threadIdx.x; pix < K.P;
-       pix += (long long)gridDim.x * blockDim.x)
-    accumulate_pixel(K.clamp, K.spf, fb, K.P, 0, pix, rad, gn, ga, A);
+  // pixels in strip order: a frame's samples are read contiguously
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < K.P;
+       s += (long long)gridDim.x * blockDim.x) {
+    int px, py;
+    strip_pixel(K, s, px, py);
+    accumulate_pixel(K.clamp, K.spf, fb, K.P, 0, s, (long long)py * K.W + px, rad, gn, ga, A);
+  }
 }
 
 __global__ void k_accumulate_batch(BatchSrc src, int n_segs, long long total, const float4* __restrict__ rad,
@@ -1139,7 +1168,8 @@ __global__ void k_accumulate_batch(BatchSrc src, int n_segs, long long total, co
     int si = find_seg<true>(src.segs, n_segs, t);
     WaveSeg g = src.segs[si];
     JobAcc A = src.accs[g.job];
-    accumulate_pixel(src.ks[g.job].clamp, g.frames, *A.frame_base, g.P, g.path0, t - g.acc0, rad, gn, ga, A);
+    accumulate_pixel(src.ks[g.job].clamp, g.frames, *A.frame_base, g.P, g.path0, t - g.acc0, t - g.acc0, rad, gn, ga,
+                     A);
   }
 }
 

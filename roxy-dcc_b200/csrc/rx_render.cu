@@ -264,6 +264,11 @@ __device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& 
   const int si = (int)s, w4 = 4 * K.W;
   const int strip = si / w4, r = si - strip * w4;
   const int hs = min(4, K.H - 4 * strip);
+  if (hs == 4) {  // every strip but a short last one
+    px = r >> 2;
+    py = 4 * strip + (r & 3);
+    return;
+  }
   const int c = r / hs;
   px = c;
   py = 4 * strip + (r - c * hs);
@@ -278,11 +283,13 @@ __device__ __forceinline__ void strip_pixel(const RenderK& K, long long s, int& 
 // their state as eight runs of 4 consecutive paths.  Any order gives the same image: a path's
 // random numbers depend on its pixel, sample and bounce.
 constexpr int kCamFrames = 8;
-__device__ __forceinline__ int camera_group(const RenderK& K) {
-  int g = kCamFrames;  // the largest power of two up to kCamFrames that divides the wave's frames
-  while (K.spf % g) g >>= 1;
+// the largest power of two up to kCamFrames that divides `frames`
+__device__ __forceinline__ int group_of(int frames) {
+  int g = kCamFrames;
+  while (frames % g) g >>= 1;
   return g;
 }
+__device__ __forceinline__ int camera_group(const RenderK& K) { return group_of(K.spf); }
 __device__ __forceinline__ long long camera_path(const RenderK& K, long long t, int& px, int& py, int& f) {
   const int g = camera_group(K);
   const long long span = (long long)g * K.P;
@@ -350,8 +357,12 @@ struct BatchSrc {
     WaveSeg g = segs[si];
     long long l = p - g.path0;
     int fb = *accs[g.job].frame_base;
-    pix = (uint32_t)(l % g.P);
-    smp = (uint32_t)(fb + (int)(l / g.P));
+    const int f = (int)(l / g.P);
+    const RenderK& K = ks[g.job];
+    int px, py;
+    strip_pixel(K, l - (long long)f * g.P, px, py);
+    pix = (uint32_t)(py * K.W + px);
+    smp = (uint32_t)(fb + f);
   }
   // batches keep k_generate_batch's queue and path state at bounce 0
   __device__ __forceinline__ long long camera_items(int) const { return 0; }
@@ -420,11 +431,18 @@ __global__ void k_generate_batch(BatchSrc src, int n_segs, long long total, floa
     WaveSeg g = src.segs[si];
     RenderK K = src.ks[g.job];
     int fb = *src.accs[g.job].frame_base;
-    long long l = t - g.path0;
-    int f = (int)(l / g.P);
+    // the single-render order and layout per segment: samples of a pixel
+    // on consecutive items, path state at path0 + f * P + strip index
+    const long long l = t - g.path0;
+    const int gs = group_of(g.frames);
+    const long long span = (long long)gs * g.P;
+    const long long c = l / span;
+    const int r = (int)(l - c * span);
+    const int si2 = r / gs;
+    const int f = (int)(c * gs) + (r - si2 * gs);
     int px, py;
-    strip_pixel(K, l - (long long)f * g.P, px, py);
-    long long p = g.path0 + (long long)f * g.P + (long long)py * K.W + px;
+    strip_pixel(K, si2, px, py);
+    long long p = g.path0 + (long long)f * g.P + si2;
     init_path(K, px, py, fb + f, p, ray_o, ray_d, thr, rad, gn, ga);
     pseg[p] = si;
     q0[t] = (int)p;
@@ -1083,7 +1101,7 @@ __global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restr
 
 // trace.py:262-283: clamp, running mean of radiance and first-hit guides,
 // display = sqrt(min(acc, 1)).  Frames of the wave are folded in order.
-// One pixel: fold `spf` frames (paths path0 + f * P + pix) into the running
+// One pixel: fold `spf` frames (paths path0 + f * P + src) into the running
 // means, starting at frame index fb.
 // src: the pixel's path index within a frame (path path0 + f * P + src);
 // pix: its accumulator index.
@@ -1168,8 +1186,12 @@ __global__ void k_accumulate_batch(BatchSrc src, int n_segs, long long total, co
     int si = find_seg<true>(src.segs, n_segs, t);
     WaveSeg g = src.segs[si];
     JobAcc A = src.accs[g.job];
-    accumulate_pixel(src.ks[g.job].clamp, g.frames, *A.frame_base, g.P, g.path0, t - g.acc0, t - g.acc0, rad, gn, ga,
-                     A);
+    // pixels in strip order, as the segment's path state is laid out
+    const RenderK& K = src.ks[g.job];
+    int px, py;
+    strip_pixel(K, t - g.acc0, px, py);
+    accumulate_pixel(K.clamp, g.frames, *A.frame_base, g.P, g.path0, t - g.acc0, (long long)py * K.W + px, rad, gn,
+                     ga, A);
   }
 }
 

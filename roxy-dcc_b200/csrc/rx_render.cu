@@ -326,11 +326,16 @@ struct SingleSrc {
     return b == 0 && K.camera0 ? (long long)K.spf * K.P : 0;
   }
   __device__ __forceinline__ int frame0() const { return *fbase; }
-  __device__ __forceinline__ int camera_ray(long long t, int fb, float3& o, float3& d) const {
+  // camera ray of item t; pix / smp: its pixel (row major) and sample, as
+  // locate() gives them
+  __device__ __forceinline__ int camera_ray(long long t, int fb, float3& o, float3& d, uint32_t& pix,
+                                            uint32_t& smp) const {
     int px, py, f;
     const long long p = camera_path(K, t, px, py, f);
     o = K.cam_pos;
     d = camera_dir(K, px, py, fb + f);
+    pix = (uint32_t)(py * K.W + px);
+    smp = (uint32_t)(fb + f);
     return (int)p;
   }
 };
@@ -367,7 +372,9 @@ struct BatchSrc {
   // batches keep k_generate_batch's queue and path state at bounce 0
   __device__ __forceinline__ long long camera_items(int) const { return 0; }
   __device__ __forceinline__ int frame0() const { return 0; }
-  __device__ __forceinline__ int camera_ray(long long, int, float3&, float3&) const { return 0; }
+  __device__ __forceinline__ int camera_ray(long long, int, float3&, float3&, uint32_t&, uint32_t&) const {
+    return 0;
+  }
 };
 
 // A batch whose scenes all have a 4-wide tree (LBVH builds): extend traverses
@@ -518,7 +525,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS)
       float3 o, d;
       int p;
       if (cam_n) {
-        p = src.camera_ray(i, fb, o, d);
+        uint32_t pix_unused, smp_unused;
+        p = src.camera_ray(i, fb, o, d, pix_unused, smp_unused);
       } else {
         p = qin[i];
         o = xyz(ray_o[p]);
@@ -848,9 +856,10 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
     PathRng rng;
     if (valid) {
       float4 o4, d4, t4;
+      uint32_t pix_id, smp;
       if (cam_n) {
         float3 co, cd;
-        p = src.camera_ray(i, fb, co, cd);
+        p = src.camera_ray(i, fb, co, cd, pix_id, smp);
         o4 = make_float4(co.x, co.y, co.z, 1.0f);
         d4 = make_float4(cd.x, cd.y, cd.z, 0.0f);
         t4 = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -859,10 +868,9 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
         o4 = ray_o[p];
         d4 = ray_d[p];
         t4 = thr_b[p];
+        src.locate(si, p, fb, pix_id, smp);
       }
       const float4 h = hits[i];
-      uint32_t pix_id, smp;
-      src.locate(si, p, fb, pix_id, smp);
       rng.init(pix_id, smp, (uint32_t)b, K.seed);
       Vertex v;
       PathStateOut out{gn, ga, ray_o, ray_d, thr_b, p, b};

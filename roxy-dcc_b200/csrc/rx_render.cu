@@ -309,14 +309,10 @@ struct SingleSrc {
   __device__ __forceinline__ int seg(long long) const { return 0; }
   __device__ __forceinline__ DevScene scene(int) const { return S; }
   __device__ __forceinline__ RenderK params(int) const { return K; }
-  // pixel (row major) and sample index of path p = f * P + strip index
-  // (fb: the accumulator's frame base)
-  __device__ __forceinline__ void locate(int, long long p, int fb, uint32_t& pix, uint32_t& smp) const {
-    const int f = (int)(p / K.P);
-    int px, py;
-    strip_pixel(K, p - (long long)f * K.P, px, py);
-    pix = (uint32_t)(py * K.W + px);
-    smp = (uint32_t)(fb + f);
+  // sample index of path p = f * P + strip index (fb: the accumulator's
+  // frame base); the path's pixel travels in its throughput's w
+  __device__ __forceinline__ uint32_t sample(int, long long p, int fb) const {
+    return (uint32_t)(fb + (int)(p / K.P));
   }
   // With K.camera0, bounce 0 has no queue: its items are the wave's camera
   // paths in k_generate's order, and k_extend / k_shade make each camera ray
@@ -326,8 +322,7 @@ struct SingleSrc {
     return b == 0 && K.camera0 ? (long long)K.spf * K.P : 0;
   }
   __device__ __forceinline__ int frame0() const { return *fbase; }
-  // camera ray of item t; pix / smp: its pixel (row major) and sample, as
-  // locate() gives them
+  // camera ray of item t; pix / smp: its pixel (row major) and sample
   __device__ __forceinline__ int camera_ray(long long t, int fb, float3& o, float3& d, uint32_t& pix,
                                             uint32_t& smp) const {
     int px, py, f;
@@ -358,16 +353,10 @@ struct BatchSrc {
     return s;
   }
   __device__ __forceinline__ RenderK params(int si) const { return ks[segs[si].job]; }
-  __device__ __forceinline__ void locate(int si, long long p, int, uint32_t& pix, uint32_t& smp) const {
-    WaveSeg g = segs[si];
-    long long l = p - g.path0;
-    int fb = *accs[g.job].frame_base;
-    const int f = (int)(l / g.P);
-    const RenderK& K = ks[g.job];
-    int px, py;
-    strip_pixel(K, l - (long long)f * g.P, px, py);
-    pix = (uint32_t)(py * K.W + px);
-    smp = (uint32_t)(fb + f);
+  // sample index of path p (the path's pixel travels in its throughput's w)
+  __device__ __forceinline__ uint32_t sample(int si, long long p, int) const {
+    const WaveSeg g = segs[si];
+    return (uint32_t)(*accs[g.job].frame_base + (int)((p - g.path0) / g.P));
   }
   // batches keep k_generate_batch's queue and path state at bounce 0
   __device__ __forceinline__ long long camera_items(int) const { return 0; }
@@ -393,7 +382,7 @@ __device__ __forceinline__ void init_path(const RenderK& K, int px, int py, int 
   float3 d = camera_dir(K, px, py, frame);
   ray_o[p] = make_float4(K.cam_pos.x, K.cam_pos.y, K.cam_pos.z, 1.0f);
   ray_d[p] = make_float4(d.x, d.y, d.z, 0.0f);
-  thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float((uint32_t)(py * K.W + px)));  // w: the pixel
   rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   ga[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -805,6 +794,7 @@ struct PathStateOut {
   float4* ray_d;
   float4* thr;
   int p, b;
+  uint32_t pix;  // the path's pixel, kept in thr.w for the later bounces
   __device__ __forceinline__ void guides(float4 n, float4 a) {
     if (b == 0) {
       gn[p] = n;
@@ -814,7 +804,7 @@ struct PathStateOut {
   __device__ __forceinline__ void next(float3 o, float ior, float3 d, float w, float3 t) {
     ray_o[p] = make_float4(o.x, o.y, o.z, ior);
     ray_d[p] = make_float4(d.x, d.y, d.z, w);
-    thr[p] = make_float4(t.x, t.y, t.z, 0.0f);
+    thr[p] = make_float4(t.x, t.y, t.z, __uint_as_float(pix));
   }
 };
 
@@ -868,12 +858,13 @@ __global__ void __launch_bounds__(128, Src::kBatch ? 5 : 1) k_shade(Src src, int
         o4 = ray_o[p];
         d4 = ray_d[p];
         t4 = thr_b[p];
-        src.locate(si, p, fb, pix_id, smp);
+        pix_id = __float_as_uint(t4.w);
+        smp = src.sample(si, p, fb);
       }
       const float4 h = hits[i];
       rng.init(pix_id, smp, (uint32_t)b, K.seed);
       Vertex v;
-      PathStateOut out{gn, ga, ray_o, ray_d, thr_b, p, b};
+      PathStateOut out{gn, ga, ray_o, ray_d, thr_b, p, b, pix_id};
       shade_vertex(S, K, mis, b, last_bounce, xyz(o4), xyz(d4), xyz(t4), o4.w, d4.w, h, rng, v, out);
       if (!v.hit && cam_n) {  // no first hit: empty guides
         gn[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1040,8 +1031,7 @@ __global__ void __launch_bounds__(128) k_tail(Src src, int b, const int* __restr
       float ior = o4.w, w = d4.w;
       float4 h = hits[i];
       float4 r = rad_b[p];
-      uint32_t pix_id, smp;
-      src.locate(si, p, fb, pix_id, smp);
+      const uint32_t pix_id = __float_as_uint(t4.w), smp = src.sample(si, p, fb);
       for (int bb = b;; ++bb) {
         PathRng rng;
         rng.init(pix_id, smp, (uint32_t)bb, K.seed);
